@@ -1,0 +1,422 @@
+"""Benchmark of the uniform-grid hot path (voxel centroid downsample + radius
+normals) on B200.
+
+Workload (one step): the 2,000,000-point georeferenced scan-like point_xyzi
+cloud (60% ground, 30% box faces, 10% clutter; offset (450000, 3900000, 50) m,
+fed as f32(world - origin)), voxel-downsampled at leaf 0.1 m and at leaf 0.5 m,
+each followed by radius normals (r = 0.5 m, viewpoint origin + (0, 0, 100)) on
+the centroids -- the MvpPipeline chain.  value = input points per second
+through the whole step (2M points / step time), inputs resident in HBM, L2
+flushed (256 MB write) between timed steps.  e2e = the same through the C ABI
+with pinned host buffers (H2D of the inputs and D2H of all results inside the
+timed region).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU (torchrun, one process per GPU): replicas -- every rank runs the
+full workload on its own GPU (weak scaling); the step time is the max over
+ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_POINTS = 2_000_000
+LEAVES = (0.1, 0.5)
+RADIUS = 0.5
+VIEWPOINT = (0.0, 0.0, 100.0)  # origin + (0, 0, 100) in the cloud's local frame
+WORKLOAD = "georef_scan_2M_xyzi: voxel leaf 0.1 + leaf 0.5, each -> radius normals r 0.5 on centroids"
+METRIC = "M points/s voxel+normals (2M georeferenced point_xyzi, leaf 0.1 & 0.5, r 0.5)"
+UNIT = "Mpoints/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-all", action="store_true",
+                    help="print the per-kernel-group timing table to stderr")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload_cloud():
+    from spatialrust_b200 import synthetic
+    return synthetic.georef_scan(N_POINTS, seed=1)
+
+
+# ---- CPU (reference restatement) -------------------------------------------
+
+def cpu_crop(cloud, side=None):
+    """The whole cloud (side None) or the x, y < side tile at full density."""
+    if side is None:
+        return cloud.x, cloud.y, cloud.z, cloud.intensity
+    m = (cloud.x < side) & (cloud.y < side)
+    return (np.ascontiguousarray(cloud.x[m]), np.ascontiguousarray(cloud.y[m]),
+            np.ascontiguousarray(cloud.z[m]), np.ascontiguousarray(cloud.intensity[m]))
+
+
+def cpu_step(crop):
+    import oracle
+    x, y, z, i = crop
+    for leaf in LEAVES:
+        v = oracle.voxel_centroid(x, y, z, [i], leaf=leaf)
+        oracle.radius_normals_ref(v.x, v.y, v.z, RADIUS, 3, VIEWPOINT, threads=0)
+
+
+def cpu_threads(n_centroids: int) -> int:
+    import oracle
+    return oracle.parallel_worker_count(n_centroids, os.cpu_count() or 1)
+
+
+CROP_SIDE = None  # the CPU runs the whole 2M-point step (about 2-3 s on 8 cores)
+CPU_BUDGET_S = 12.0
+
+
+def cpu_baseline(cloud):
+    """Reference CPU path (C restatement: single-threaded hash voxel, KD-tree
+    radius normals threaded as staging.rs does), whole steps repeated for
+    about CPU_BUDGET_S seconds."""
+    import oracle
+    oracle.build()
+    crop = cpu_crop(cloud, CROP_SIDE)
+    times = []
+    t_start = time.perf_counter()
+    while not times or (time.perf_counter() - t_start < CPU_BUDGET_S and len(times) < 8):
+        t0 = time.perf_counter()
+        cpu_step(crop)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    v = oracle.voxel_centroid(*crop[:3], [crop[3]], leaf=LEAVES[0])
+    return dict(value=len(crop[0]) / t / 1e6, unit=UNIT, cores=cpu_threads(len(v.x)),
+                kind="port", seconds_per_step=t,
+                sample=(f"the full step on all {len(crop[0])} points, {len(times)} step(s), "
+                        f"median {t:.2f} s; voxel single-threaded (voxel.rs:502-520), normals on "
+                        f"{cpu_threads(len(v.x))} threads (staging.rs:11-41); C restatement of "
+                        "the reference's CPU path (Rust is not buildable here)"))
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    cloud = workload_cloud()
+    import oracle
+    oracle.build()
+    crop = cpu_crop(cloud, CROP_SIDE)
+    for _ in range(max(args.warmup, 1)):
+        cpu_step(crop)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_step(crop)
+    t = (time.perf_counter() - t0) / args.steps
+    v = oracle.voxel_centroid(*crop[:3], [crop[3]], leaf=LEAVES[0])
+    value = len(crop[0]) / t / 1e6
+    line = dict(
+        impl="reference", metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus,
+        steps=args.steps, warmup=args.warmup, ms_per_step=t * 1e3, higher_is_better=True,
+        scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
+        config=dict(workload=WORKLOAD, points=len(crop[0]), sample_of=N_POINTS),
+        cpu_baseline=dict(value=value, unit=UNIT, cores=cpu_threads(len(v.x)), kind="port",
+                          sample=(f"the full step on all {len(crop[0])} points each step; the "
+                                  "reference is Rust and cannot be built here, so its CPU path "
+                                  "runs as the C restatement in oracle/")),
+        e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+    )
+    print(json.dumps(line), flush=True)
+
+
+# ---- GPU --------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return dict(sm_mhz=statistics.median(sm) if sm else None,
+                    sm_max_mhz=max(smax) if smax else None, reasons=sorted(reasons),
+                    samples=len(sm))
+
+
+def algorithmic_bytes(group: str, info: dict, n_attrs: int = 1) -> float:
+    """Compulsory bytes of one launch group, per the per-unit figures of the
+    path's byte model: voxel 16 B/point read + 28 B/voxel written (sort and
+    segment groups at their implementation minimum), normals 12 B/point read +
+    20 B/point written."""
+    n, v, u = info["points"], info["voxels"], info["cells"]
+    cols = 3 + n_attrs
+    if group == "voxel_sort":
+        return n * 12.0 + max(info["voxel_sort_passes"], 1) * n * 24.0
+    if group == "cell_sort":
+        return v * 12.0 + max(info["cell_sort_passes"], 1) * v * 24.0
+    if group == "voxel_segments":
+        return n * 12.0 + n * 4.0 * cols + v * (4.0 * cols + 12.0)
+    if group == "cells":
+        return v * 12.0 + v * 12.0 + v * 16.0 + u * 12.0
+    if group == "normals":
+        return v * 12.0 + v * 20.0
+    if group in ("voxel_hist", "bounds"):
+        return n * 12.0
+    if group == "cell_hist":
+        return v * 12.0
+    if group == "ranges":
+        return u * 9 * 8.0 + u * 12.0
+    if group == "hash":
+        return u * 16.0
+    return 0.0
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    from spatialrust_b200 import _native
+
+    world, rank, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    cloud = workload_cloud()
+    stream = torch.cuda.current_stream(dev)
+    # one context per leaf so both chains' results stay resident
+    ctxs = [_native.Context(local) for _ in LEAVES]
+    for c in ctxs:
+        c.set_stream(stream.cuda_stream)
+    cols = [torch.from_numpy(a).to(dev) for a in (cloud.x, cloud.y, cloud.z, cloud.intensity)]
+    keep = _native._Keep()
+    dcloud = _native.make_cloud(cols[0], cols[1], cols[2], [cols[3]], keep)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        for c, leaf in zip(ctxs, LEAVES):
+            c.voxel_normals_enqueue(dcloud, leaf, None, RADIUS, 3, VIEWPOINT)
+
+    # warm-up (also sizes every buffer)
+    for _ in range(max(args.warmup, 3)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    infos = []
+    for c in ctxs:
+        c.frame_check()
+        infos.append(c.chain_info())
+
+    # untimed profile pass: which kernel group dominates
+    for c in ctxs:
+        c.profile_read(reset=True)
+        c.profile_enable(_native.KERNEL_IDS)
+    for _ in range(3):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    prof = [c.profile_read(reset=True) for c in ctxs]
+    group_ms = {g: sum(p[g]["total_ms"] for p in prof) for g in _native.KERNEL_IDS}
+    dominant = max(group_ms, key=group_ms.get)
+    if args.profile_all and rank == 0:
+        tot = sum(group_ms.values())
+        for g, ms in sorted(group_ms.items(), key=lambda kv: -kv[1]):
+            print(f"  {g:16s} {ms / 3:9.4f} ms/step  {100 * ms / tot:5.1f}%", file=sys.stderr)
+    for c in ctxs:
+        c.profile_enable([dominant])
+
+    # timed region
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for s in range(args.steps):
+        flush.zero_()  # outside the timed events
+        ev[s][0].record(stream)
+        step()
+        ev[s][1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clock = clocks.stop()
+    ms_steps = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(ms_steps)
+    prof = [c.profile_read(reset=True) for c in ctxs]
+    for c in ctxs:
+        c.profile_enable([])
+        c.frame_check()  # device status of the last chain: raises on any failure
+    launches = sum(p[g]["launches"] for p in prof for g in _native.KERNEL_IDS)
+    dom_ms = sum(p[dominant]["total_ms"] for p in prof)
+    dom_regions = sum(p[dominant]["timed_regions"] for p in prof)
+    dom_bytes = sum(algorithmic_bytes(dominant, info) for info in infos) / len(infos)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    ms_per_step = max_ms / args.steps
+    value = world * N_POINTS / (ms_per_step / 1e3) / 1e6
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = run_e2e(ctxs[0], cloud, args, torch, dev, stream)
+
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    avg_launch_ms = dom_ms / max(dom_regions, 1)
+    achieved = dom_bytes / (avg_launch_ms / 1e3) / 1e9 if dom_regions else 0.0
+    roofline = dict(bound="hbm", kernel=dominant, achieved=achieved, peak=hbm, unit="GB/s",
+                    frac=achieved / hbm, traffic=None,
+                    peak_source="MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
+                    else "fallback 6650 GB/s",
+                    algorithmic_bytes_per_launch=dom_bytes, avg_launch_ms=avg_launch_ms,
+                    step_share=group_ms[dominant] / max(sum(group_ms.values()), 1e-9))
+    line = dict(
+        metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
+        warmup=args.warmup, ms_per_step=ms_per_step, higher_is_better=True, scaling="weak",
+        vs_baseline=None, dtype="f32", data="synthetic",
+        config=dict(workload=WORKLOAD, points=N_POINTS, leaves=list(LEAVES), radius=RADIUS,
+                    voxels=[i["voxels"] for i in infos], cells=[i["cells"] for i in infos],
+                    l2="flushed by a 256 MB write before every timed step (outside the events)",
+                    parallelism=f"replicas x{world}"),
+        e2e=e2e, roofline=roofline, clocks=clock, gpu_launches=int(launches),
+    )
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cloud)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for c in ctxs:
+        c.close()
+
+
+def run_e2e(ctx, cloud, args, torch, dev, stream):
+    """Synchronous srcu_voxel_normals calls with pinned host inputs and outputs."""
+    from spatialrust_b200 import _native
+    lib = _native.load()
+    n = cloud.n
+    pin = [torch.from_numpy(a).pin_memory() for a in (cloud.x, cloud.y, cloud.z, cloud.intensity)]
+    keep = _native._Keep()
+    attr_in = keep.add((ctypes.c_void_p * 1)(pin[3].data_ptr()))
+    hcloud = _native.SrcuCloud(pin[0].data_ptr(), pin[1].data_ptr(), pin[2].data_ptr(),
+                               ctypes.cast(attr_in, ctypes.c_void_p), 1, 0, n)
+    outs = []
+    for _ in LEAVES:
+        vcols = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(4)]
+        counts = torch.empty(n, dtype=torch.int32).pin_memory()
+        ncols = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(4)]
+        ncount = torch.empty(n, dtype=torch.int32).pin_memory()
+        attr_out = keep.add((ctypes.c_void_p * 1)(vcols[3].data_ptr()))
+        vout = _native.SrcuVoxelOut(vcols[0].data_ptr(), vcols[1].data_ptr(), vcols[2].data_ptr(),
+                                    ctypes.cast(attr_out, ctypes.c_void_p), 0, counts.data_ptr(), 0)
+        nout = _native.SrcuNormalOut(*[c.data_ptr() for c in ncols], ncount.data_ptr(), 0)
+        outs.append((vcols, counts, ncols, ncount, vout, nout))
+    params = [(_native._voxel_params(leaf, None), _native._normal_params(RADIUS, 3, VIEWPOINT, False))
+              for leaf in LEAVES]
+    nv = ctypes.c_uint64(0)
+    stats = _native.SrcuNormalStats()
+    voxels = [0] * len(LEAVES)
+
+    def step():
+        for k, (vp, np_) in enumerate(params):
+            st = lib.srcu_voxel_normals(ctx.handle, ctypes.byref(hcloud), ctypes.byref(vp),
+                                        ctypes.byref(np_), ctypes.byref(outs[k][4]),
+                                        ctypes.byref(outs[k][5]), ctypes.byref(nv),
+                                        ctypes.byref(stats))
+            if st != 0:
+                ctx._check(st)
+            voxels[k] = int(nv.value)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    steps = max(args.steps // 2, 3)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        step()
+    end.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / steps
+    h2d = len(LEAVES) * n * 16
+    d2h = sum(v * (16 + 4 + 16 + 4) for v in voxels)
+    return dict(value=N_POINTS / (ms / 1e3) / 1e6, unit=UNIT, ms_per_step=ms,
+                h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
+                api="srcu_voxel_normals (include/srcuda.h), pinned host buffers, one call per leaf")
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,257 @@
+/*
+ * srcuda.h -- C ABI of the B200 (sm_100a) uniform-grid hot path of SpatialRust:
+ * VoxelGrid centroid downsample and radius-mode normal estimation.
+ *
+ * Plain C: pointers, sizes and POD structs only.  Every entry point returns an
+ * srcu_status; a message for the last failure on a context is available from
+ * srcu_last_error().  Nothing here aborts the process or traps the GPU: device
+ * side failures (a bounded wait that gave up, a key that does not fit) are
+ * written to a device status word and surfaced as a status code.
+ *
+ * Threading: a context is NOT thread-safe.  Use one context per host thread,
+ * or let one thread own it (the serving loop in this library does so).
+ *
+ * Reference interfaces replaced (SpatialRust, Rust):
+ *   - ExecutionPolicy::Gpu(DeviceKind::Cuda) arm of
+ *     VoxelGridDownsample::filter_internal
+ *     (crates/spatialrust-filtering/src/voxel.rs:278-308, today rejected at
+ *     voxel.rs:336-339),
+ *   - ExecutionPolicy::Gpu(DeviceKind::Cuda) arm of
+ *     NormalEstimator::estimate_policy_output / resolve_policy
+ *     (crates/spatialrust-features/src/normal.rs:208-230, 276-297, today
+ *     rejected at normal.rs:292-294),
+ *   - GpuNormalEstimator::estimate radius mode
+ *     (crates/spatialrust-features/src/normal_gpu.rs:33-83 ->
+ *     crates/spatialrust-gpu/src/kernels/normals_grid.rs:208-350),
+ *   - the device-resident voxel -> radius-grid -> normals frame chain
+ *     (crates/spatialrust-gpu/src/gpu_frame.rs:344-365).
+ */
+#ifndef SRCUDA_H
+#define SRCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SRCU_ABI_VERSION 1
+
+/* Status codes.  The first four map 1:1 onto SpatialError
+ * (crates/spatialrust-core/src/error.rs:8-37); the rest surface as
+ * SpatialError::InvalidArgument(text) on the Rust side. */
+typedef enum srcu_status {
+  SRCU_OK = 0,
+  SRCU_ERR_INVALID_ARGUMENT = 1, /* SpatialError::InvalidArgument */
+  SRCU_ERR_LENGTH_MISMATCH = 2,  /* SpatialError::BufferLengthMismatch */
+  SRCU_ERR_UNSUPPORTED_DTYPE = 3,/* SpatialError::UnsupportedDType */
+  SRCU_ERR_MISSING_FIELD = 4,    /* SpatialError::MissingField */
+  SRCU_ERR_OUT_OF_BUDGET = 5,    /* device memory would exceed the context's HBM budget */
+  SRCU_ERR_CUDA = 6,             /* CUDA runtime error; text in srcu_last_error() */
+  SRCU_ERR_TIMEOUT = 7,          /* a bounded device-side wait gave up */
+  SRCU_ERR_KEY_OVERFLOW = 8,     /* packed voxel/cell key would need more than 64 bits */
+  SRCU_ERR_NO_DEVICE = 9,        /* no CUDA device of compute capability 10.x */
+  SRCU_ERR_BUSY = 10             /* serving loop: request not admitted yet (retry) */
+} srcu_status;
+
+typedef struct srcu_ctx srcu_ctx;
+
+/* One point cloud as SoA f32 columns (PointCloud::positions3 plus the F32
+ * attribute columns, crates/spatialrust-core/src/capabilities.rs:22-29).
+ * Non-F32 attribute columns are widened to f32 by the caller, as the
+ * reference's read_buffer_f32 does (voxel.rs:692-701).
+ * When on_device != 0 every pointer is a device pointer on the context's
+ * device; otherwise host memory (pageable or pinned). */
+typedef struct srcu_cloud {
+  const float *x;
+  const float *y;
+  const float *z;
+  const float *const *attrs; /* n_attrs columns, e.g. { intensity }; may be NULL if n_attrs == 0 */
+  uint32_t n_attrs;
+  int32_t on_device;
+  uint64_t n;
+} srcu_cloud;
+
+/* VoxelGridDownsampleConfig for Centroid + Average
+ * (crates/spatialrust-filtering/src/voxel.rs:112-183). */
+typedef struct srcu_voxel_params {
+  float leaf_size;  /* must be > 0 (NaN passes, as in voxel.rs:260) */
+  int32_t has_origin;
+  float origin[3];  /* used when has_origin != 0: floor keys; else origin = min corner, truncated keys */
+} srcu_voxel_params;
+
+/* Voxel output.  Each column needs capacity >= input n (the voxel count is
+ * never larger).  Voxels are emitted in ascending (ix, iy, iz) order, the
+ * reference's output order for point_xyzi (voxel.rs:522-536). */
+typedef struct srcu_voxel_out {
+  float *x;
+  float *y;
+  float *z;
+  float *const *attrs; /* n_attrs columns (same count as the input cloud) */
+  int64_t *keys;       /* nullable: 3 int64 per voxel, the reference's (ix, iy, iz) */
+  uint32_t *counts;    /* nullable: points per voxel */
+  int32_t on_device;
+} srcu_voxel_out;
+
+/* NormalEstimationConfig in radius mode
+ * (crates/spatialrust-features/src/normal.rs:17-71). */
+typedef struct srcu_normal_params {
+  float radius;            /* search_radius; must be >= 0 (normal.rs:109-111) */
+  uint32_t min_neighbors;  /* default 3 */
+  int32_t has_viewpoint;
+  float viewpoint[3];
+  int32_t include_self;    /* 0: NormalEstimator CPU semantics (self excluded, NaN when invalid).
+                              1: GpuNormalEstimator grid semantics (self included, fewer than
+                                 3 points -> (0,0,1), curvature 0; normals_grid.rs:86-197). */
+} srcu_normal_params;
+
+typedef struct srcu_normal_out {
+  float *nx;
+  float *ny;
+  float *nz;
+  float *curvature;
+  uint32_t *neighbor_counts; /* nullable: neighbours found per point (self excluded unless include_self) */
+  int32_t on_device;
+} srcu_normal_out;
+
+/* NormalEstimationResult (normal.rs:74-80) plus diagnostics. */
+typedef struct srcu_normal_stats {
+  uint64_t valid_count;
+  uint64_t invalid_count;
+  uint64_t shell_points;  /* points with some other point at |d^2 - r^2| <= 1e-6 r^2 */
+  uint64_t fp64_eigensolves; /* covariances whose eigengap sent them to the FP64 Jacobi path */
+} srcu_normal_stats;
+
+/* ---- context ------------------------------------------------------------ */
+
+int srcu_abi_version(void);
+
+/* Creates a context on CUDA device `device`.  hbm_budget_bytes caps the device
+ * memory this context may hold (0 = no cap); allocations beyond it fail with
+ * SRCU_ERR_OUT_OF_BUDGET.  Replaces WgpuRuntime::shared()
+ * (crates/spatialrust-gpu/src/runtime.rs:72-95). */
+srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out);
+void srcu_destroy(srcu_ctx *ctx);
+const char *srcu_last_error(const srcu_ctx *ctx);
+
+/* Runs subsequent work on a caller stream (a cudaStream_t); NULL restores the
+ * context's own stream. */
+srcu_status srcu_set_stream(srcu_ctx *ctx, void *cuda_stream);
+srcu_status srcu_synchronize(srcu_ctx *ctx);
+/* Device bytes currently held by the context. */
+uint64_t srcu_device_bytes(const srcu_ctx *ctx);
+
+/* ---- one cloud ------------------------------------------------------------ */
+
+/* VoxelGridDownsample::filter_with_policy(cloud, Gpu(Cuda)) for
+ * Centroid + Average (voxel.rs:213-237, 251-368, 464-540): per-voxel means of
+ * x, y, z and every attribute, accumulated in FP64, emitted in key order.
+ * Synchronous: returns after the outputs are written; *out_voxels = V. */
+srcu_status srcu_voxel_centroid(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                const srcu_voxel_params *params, const srcu_voxel_out *out,
+                                uint64_t *out_voxels);
+
+/* NormalEstimator::estimate_with_policy(cloud, Gpu(Cuda)) with
+ * search_radius = Some(r) (normal.rs:102-164, 321-573), or, with
+ * include_self = 1, GpuNormalEstimator::estimate (normal_gpu.rs:33-83).
+ * Outputs are in input point order.  Synchronous.  stats is nullable. */
+srcu_status srcu_radius_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                const srcu_normal_params *params, const srcu_normal_out *out,
+                                srcu_normal_stats *stats);
+
+/* MvpPipeline voxel -> normals chain (crates/spatialrust-pipeline/src/mvp.rs:193-226):
+ * centroid downsample, then radius normals on the centroids, all on the
+ * device.  vout gets the centroids, nout the normals of each centroid (both
+ * V long, capacity n).  Synchronous. */
+srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
+                               const srcu_voxel_params *vparams, const srcu_normal_params *nparams,
+                               const srcu_voxel_out *vout, const srcu_normal_out *nout,
+                               uint64_t *out_voxels, srcu_normal_stats *stats);
+
+/* ---- device-resident chain (GpuSpatialFrame, gpu_frame.rs:71-365) --------- */
+
+/* Enqueues the voxel -> normals chain on the context stream for a cloud
+ * already on the device, without any host synchronisation; results stay in
+ * context-owned device buffers (valid until the next enqueue).  Safe to
+ * capture in a CUDA graph after one uncaptured warm-up call of the same size. */
+srcu_status srcu_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                       const srcu_voxel_params *vparams,
+                                       const srcu_normal_params *nparams);
+
+typedef struct srcu_frame_view {
+  const float *x, *y, *z;        /* device: centroids (capacity n) */
+  const float *const *attrs;     /* host array of device column pointers */
+  const float *nx, *ny, *nz, *curvature; /* device */
+  const uint32_t *counts;        /* device: points per voxel */
+  const uint64_t *voxel_count;   /* device: V */
+  uint32_t n_attrs;
+} srcu_frame_view;
+
+/* Device pointers of the last enqueued chain's results. */
+srcu_status srcu_frame_view_get(srcu_ctx *ctx, srcu_frame_view *view);
+/* Synchronises and checks the device status word of the last enqueue. */
+srcu_status srcu_frame_check(srcu_ctx *ctx, uint64_t *out_voxels, srcu_normal_stats *stats);
+
+/* Facts about the last chain (after srcu_frame_check or a synchronous call). */
+typedef struct srcu_chain_info {
+  uint64_t points;
+  uint64_t voxels;
+  uint64_t cells;             /* occupied radius-grid cells */
+  uint32_t voxel_key_bits;
+  uint32_t cell_key_bits;
+  uint32_t voxel_sort_passes; /* onesweep digit passes that ran */
+  uint32_t cell_sort_passes;
+  double cell_size;           /* radius-grid cell edge (>= radius) */
+} srcu_chain_info;
+
+srcu_status srcu_chain_info_get(srcu_ctx *ctx, srcu_chain_info *info);
+
+/* Explicit read-back of the last enqueued chain (GpuSpatialFrame readback,
+ * gpu_frame.rs:292-328): synchronises, then copies the V centroids and their
+ * normals into caller buffers (capacity >= V; either out may be NULL). */
+srcu_status srcu_frame_fetch(srcu_ctx *ctx, const srcu_voxel_out *vout, const srcu_normal_out *nout,
+                             uint64_t *out_voxels, srcu_normal_stats *stats);
+
+/* ---- launch accounting and kernel timing ---------------------------------- */
+
+/* Kernel groups of the chain, in launch order. */
+typedef enum srcu_kernel_id {
+  SRCU_K_BEGIN = 0,      /* control-block reset */
+  SRCU_K_BOUNDS,         /* per-axis min/max */
+  SRCU_K_VOXEL_PLAN,     /* voxel-key packing plan */
+  SRCU_K_VOXEL_HIST,     /* digit histograms of the voxel keys */
+  SRCU_K_VOXEL_SORT,     /* onesweep passes over the voxel keys (8 launches) */
+  SRCU_K_VOXEL_SEGMENTS, /* fused voxel segmentation + FP64 centroid reduction */
+  SRCU_K_UNPACK_KEYS,    /* packed key -> (ix, iy, iz) */
+  SRCU_K_CELL_PLAN,      /* radius-grid plan */
+  SRCU_K_CELL_HIST,      /* digit histograms of the cell keys */
+  SRCU_K_CELL_SORT,      /* onesweep passes over the cell keys (8 launches) */
+  SRCU_K_CELLS,          /* cell table + cell-sorted point records */
+  SRCU_K_HASH,           /* cell hash table */
+  SRCU_K_RANGES,         /* 3x3 neighbour column ranges */
+  SRCU_K_NORMALS,        /* radius neighbours + covariance + eigensolve */
+  SRCU_K_COUNT
+} srcu_kernel_id;
+
+typedef struct srcu_kernel_stat {
+  char name[32];
+  uint64_t launches;      /* kernel launches since the last reset */
+  uint64_t timed_regions; /* launch groups timed with CUDA events (see srcu_profile_enable) */
+  double total_ms;        /* summed event time of the timed groups */
+} srcu_kernel_stat;
+
+/* Times every launch group whose bit (1 << srcu_kernel_id) is set with a pair
+ * of CUDA events on the context stream; 0 turns timing off.  Launch counting
+ * is always on. */
+srcu_status srcu_profile_enable(srcu_ctx *ctx, uint64_t timed_kernel_mask);
+/* Synchronises, then fills up to max_entries stats (one per srcu_kernel_id)
+ * and returns how many were written (negative on error).  reset != 0 clears
+ * the counters afterwards. */
+int srcu_profile_read(srcu_ctx *ctx, srcu_kernel_stat *out, int max_entries, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SRCUDA_H */

@@ -1,0 +1,211 @@
+"""TEST INFRASTRUCTURE ONLY: CPU oracle for the uniform-grid hot path.
+
+A C restatement of SpatialRust's CPU voxel-centroid and radius-normal paths
+(``srcu_oracle.c`` cites the reference file:line of each function) plus an
+FP64 normal oracle.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline legs of ``bench.py`` import this package; the product package
+``spatialrust_b200`` never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SRC = os.path.join(_HERE, "srcu_oracle.c")
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+# -ffp-contract=off keeps every f32 a*b+c rounded twice, as Rust does.
+CFLAGS = ["-O3", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-pthread", "-std=c11",
+          "-D_GNU_SOURCE"]
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile srcu_oracle.c into oracle/liboracle.so with gcc."""
+    if (not force and os.path.exists(_LIB_PATH)
+            and os.path.getmtime(_LIB_PATH) >= os.path.getmtime(_SRC)):
+        return _LIB_PATH
+    tmp = _LIB_PATH + ".tmp"
+    subprocess.check_call(["gcc", *CFLAGS, "-o", tmp, _SRC, "-lm"])
+    os.replace(tmp, _LIB_PATH)
+    return _LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        build()
+    lib = ctypes.CDLL(_LIB_PATH)
+    P = ctypes.c_void_p
+    lib.oracle_voxel_centroid.argtypes = [P, P, P, P, ctypes.c_int, ctypes.c_size_t, ctypes.c_float,
+                                          ctypes.c_int, P, ctypes.c_int, P, P, P, P]
+    lib.oracle_voxel_centroid.restype = ctypes.c_int
+    lib.oracle_radius_normals_ref.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float,
+                                              ctypes.c_uint32, ctypes.c_int, P, ctypes.c_int, P, P,
+                                              P, P, P, P, P]
+    lib.oracle_radius_normals_ref.restype = ctypes.c_int
+    lib.oracle_radius_normals_fp64.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float,
+                                               ctypes.c_uint32, ctypes.c_int, P, ctypes.c_double,
+                                               ctypes.c_int, P, P, P, P, P, P, P]
+    lib.oracle_radius_normals_fp64.restype = ctypes.c_int
+    lib.oracle_brute_radius_counts.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float, P]
+    lib.oracle_brute_radius_counts.restype = None
+    lib.oracle_compute_bounds.argtypes = [P, P, P, ctypes.c_size_t, P, P]
+    lib.oracle_compute_bounds.restype = None
+    lib.oracle_smallest_eigenpair_f32.argtypes = [P, P, P]
+    lib.oracle_smallest_eigenpair_f32.restype = None
+    lib.oracle_parallel_worker_count.argtypes = [ctypes.c_size_t, ctypes.c_size_t]
+    lib.oracle_parallel_worker_count.restype = ctypes.c_size_t
+    _lib = lib
+    return lib
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+@dataclass
+class VoxelResult:
+    fields: list  # x, y, z, attrs... (float32 arrays of length V)
+    keys: np.ndarray  # (V, 3) int64
+    counts: np.ndarray  # (V,) uint32
+
+    @property
+    def x(self):
+        return self.fields[0]
+
+    @property
+    def y(self):
+        return self.fields[1]
+
+    @property
+    def z(self):
+        return self.fields[2]
+
+
+def voxel_centroid(x, y, z, attrs=(), leaf=1.0, origin=None, plain_xyz=False) -> VoxelResult:
+    """Reference CPU centroid downsample (voxel.rs:251-275, 464-636)."""
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    attrs = [_f32(a) for a in attrs]
+    n = x.shape[0]
+    cap = max(n, 1)
+    outs = [np.empty(cap, np.float32) for _ in range(3 + len(attrs))]
+    keys = np.empty((cap, 3), np.int64)
+    counts = np.empty(cap, np.uint32)
+    attr_ptrs = (ctypes.c_void_p * max(len(attrs), 1))(*[a.ctypes.data for a in attrs])
+    out_ptrs = (ctypes.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
+    org = np.asarray(origin if origin is not None else (0, 0, 0), np.float32)
+    nv = ctypes.c_size_t(0)
+    rc = lib.oracle_voxel_centroid(_ptr(x), _ptr(y), _ptr(z), ctypes.cast(attr_ptrs, ctypes.c_void_p),
+                                   len(attrs), n, ctypes.c_float(leaf), int(origin is not None),
+                                   _ptr(org), int(bool(plain_xyz)),
+                                   ctypes.cast(out_ptrs, ctypes.c_void_p), _ptr(keys), _ptr(counts),
+                                   ctypes.byref(nv))
+    if rc != 0:
+        raise OracleError(f"oracle_voxel_centroid failed: {rc}")
+    v = nv.value
+    return VoxelResult([o[:v].copy() for o in outs], keys[:v].copy(), counts[:v].copy())
+
+
+@dataclass
+class NormalResult:
+    nx: np.ndarray
+    ny: np.ndarray
+    nz: np.ndarray
+    curvature: np.ndarray
+    counts: np.ndarray
+    valid_count: int = 0
+    invalid_count: int = 0
+    gap: np.ndarray | None = None
+    shell: np.ndarray | None = None
+
+    @property
+    def normals(self) -> np.ndarray:
+        return np.stack([self.nx, self.ny, self.nz], axis=1)
+
+
+def radius_normals_ref(x, y, z, radius, min_neighbors=3, viewpoint=None, threads=0) -> NormalResult:
+    """Reference CPU radius normals, f32 arithmetic (normal.rs:102-573)."""
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    n = x.shape[0]
+    outs = [np.empty(max(n, 1), np.float32) for _ in range(4)]
+    counts = np.zeros(max(n, 1), np.uint32)
+    vp = np.asarray(viewpoint if viewpoint is not None else (0, 0, 0), np.float32)
+    valid = ctypes.c_size_t(0)
+    invalid = ctypes.c_size_t(0)
+    rc = lib.oracle_radius_normals_ref(_ptr(x), _ptr(y), _ptr(z), n, ctypes.c_float(radius),
+                                       min_neighbors, int(viewpoint is not None), _ptr(vp), threads,
+                                       *[_ptr(o) for o in outs], _ptr(counts), ctypes.byref(valid),
+                                       ctypes.byref(invalid))
+    if rc != 0:
+        raise OracleError(f"oracle_radius_normals_ref failed: {rc}")
+    return NormalResult(*[o[:n] for o in outs], counts[:n], valid.value, invalid.value)
+
+
+def radius_normals_fp64(x, y, z, radius, min_neighbors=3, viewpoint=None, shell_rel=1e-6,
+                        threads=0) -> NormalResult:
+    """FP64 oracle: exact f32-predicate neighbour sets, FP64 covariance and Jacobi."""
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    n = x.shape[0]
+    outs = [np.empty(max(n, 1), np.float64) for _ in range(5)]
+    counts = np.zeros(max(n, 1), np.uint32)
+    shell = np.zeros(max(n, 1), np.uint8)
+    vp = np.asarray(viewpoint if viewpoint is not None else (0, 0, 0), np.float32)
+    rc = lib.oracle_radius_normals_fp64(_ptr(x), _ptr(y), _ptr(z), n, ctypes.c_float(radius),
+                                        min_neighbors, int(viewpoint is not None), _ptr(vp),
+                                        ctypes.c_double(shell_rel), threads,
+                                        *[_ptr(o) for o in outs], _ptr(counts), _ptr(shell))
+    if rc != 0:
+        raise OracleError(f"oracle_radius_normals_fp64 failed: {rc}")
+    nx, ny, nz, curv, gap = [o[:n] for o in outs]
+    valid = int(np.count_nonzero(~np.isnan(nx)))
+    return NormalResult(nx, ny, nz, curv, counts[:n], valid, n - valid, gap, shell[:n].astype(bool))
+
+
+def brute_radius_counts(x, y, z, radius) -> np.ndarray:
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    counts = np.zeros(max(x.shape[0], 1), np.uint32)
+    lib.oracle_brute_radius_counts(_ptr(x), _ptr(y), _ptr(z), x.shape[0], ctypes.c_float(radius),
+                                   _ptr(counts))
+    return counts[:x.shape[0]]
+
+
+def compute_bounds(x, y, z):
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    mn = np.zeros(3, np.float32)
+    mx = np.zeros(3, np.float32)
+    lib.oracle_compute_bounds(_ptr(x), _ptr(y), _ptr(z), x.shape[0], _ptr(mn), _ptr(mx))
+    return mn, mx
+
+
+def smallest_eigenpair_f32(c00, c11, c22, c01, c02, c12):
+    lib = _load()
+    c = np.asarray([c00, c11, c22, c01, c02, c12], np.float32)
+    normal = np.zeros(3, np.float32)
+    curv = ctypes.c_float(0)
+    lib.oracle_smallest_eigenpair_f32(_ptr(c), _ptr(normal), ctypes.byref(curv))
+    return normal, curv.value
+
+
+def parallel_worker_count(n: int, available: int) -> int:
+    return int(_load().oracle_parallel_worker_count(n, available))

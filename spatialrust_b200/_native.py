@@ -1,0 +1,463 @@
+"""ctypes binding of libsrcuda.so (the C ABI declared in include/srcuda.h).
+
+The CUDA library is the product path: there is no CPU fallback.  Importing this
+module fails loudly when libsrcuda.so is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Sequence
+
+import numpy as np
+
+from .core import (BufferLengthMismatch, InvalidArgument, MissingField, SpatialError,
+                   UnsupportedDType)
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsrcuda.so")
+
+SRCU_OK = 0
+SRCU_ERR_INVALID_ARGUMENT = 1
+SRCU_ERR_LENGTH_MISMATCH = 2
+SRCU_ERR_UNSUPPORTED_DTYPE = 3
+SRCU_ERR_MISSING_FIELD = 4
+SRCU_ERR_OUT_OF_BUDGET = 5
+SRCU_ERR_CUDA = 6
+SRCU_ERR_TIMEOUT = 7
+SRCU_ERR_KEY_OVERFLOW = 8
+SRCU_ERR_NO_DEVICE = 9
+SRCU_ERR_BUSY = 10
+
+STATUS_NAMES = {
+    SRCU_OK: "SRCU_OK",
+    SRCU_ERR_INVALID_ARGUMENT: "SRCU_ERR_INVALID_ARGUMENT",
+    SRCU_ERR_LENGTH_MISMATCH: "SRCU_ERR_LENGTH_MISMATCH",
+    SRCU_ERR_UNSUPPORTED_DTYPE: "SRCU_ERR_UNSUPPORTED_DTYPE",
+    SRCU_ERR_MISSING_FIELD: "SRCU_ERR_MISSING_FIELD",
+    SRCU_ERR_OUT_OF_BUDGET: "SRCU_ERR_OUT_OF_BUDGET",
+    SRCU_ERR_CUDA: "SRCU_ERR_CUDA",
+    SRCU_ERR_TIMEOUT: "SRCU_ERR_TIMEOUT",
+    SRCU_ERR_KEY_OVERFLOW: "SRCU_ERR_KEY_OVERFLOW",
+    SRCU_ERR_NO_DEVICE: "SRCU_ERR_NO_DEVICE",
+    SRCU_ERR_BUSY: "SRCU_ERR_BUSY",
+}
+
+MAX_ATTRS = 9
+
+
+class CudaError(SpatialError):
+    """A CUDA-side failure (maps to SpatialError::InvalidArgument text in the reference)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class OutOfBudget(CudaError):
+    pass
+
+
+class DeviceTimeout(CudaError):
+    pass
+
+
+class KeyOverflow(CudaError):
+    pass
+
+
+class NoDevice(CudaError):
+    pass
+
+
+c_float3 = ctypes.c_float * 3
+
+
+class SrcuCloud(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("z", ctypes.c_void_p),
+                ("attrs", ctypes.c_void_p), ("n_attrs", ctypes.c_uint32),
+                ("on_device", ctypes.c_int32), ("n", ctypes.c_uint64)]
+
+
+class SrcuVoxelParams(ctypes.Structure):
+    _fields_ = [("leaf_size", ctypes.c_float), ("has_origin", ctypes.c_int32),
+                ("origin", c_float3)]
+
+
+class SrcuVoxelOut(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("z", ctypes.c_void_p),
+                ("attrs", ctypes.c_void_p), ("keys", ctypes.c_void_p), ("counts", ctypes.c_void_p),
+                ("on_device", ctypes.c_int32)]
+
+
+class SrcuNormalParams(ctypes.Structure):
+    _fields_ = [("radius", ctypes.c_float), ("min_neighbors", ctypes.c_uint32),
+                ("has_viewpoint", ctypes.c_int32), ("viewpoint", c_float3),
+                ("include_self", ctypes.c_int32)]
+
+
+class SrcuNormalOut(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_void_p), ("ny", ctypes.c_void_p), ("nz", ctypes.c_void_p),
+                ("curvature", ctypes.c_void_p), ("neighbor_counts", ctypes.c_void_p),
+                ("on_device", ctypes.c_int32)]
+
+
+class SrcuNormalStats(ctypes.Structure):
+    _fields_ = [("valid_count", ctypes.c_uint64), ("invalid_count", ctypes.c_uint64),
+                ("shell_points", ctypes.c_uint64), ("fp64_eigensolves", ctypes.c_uint64)]
+
+
+class SrcuFrameView(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("z", ctypes.c_void_p),
+                ("attrs", ctypes.c_void_p), ("nx", ctypes.c_void_p), ("ny", ctypes.c_void_p),
+                ("nz", ctypes.c_void_p), ("curvature", ctypes.c_void_p),
+                ("counts", ctypes.c_void_p), ("voxel_count", ctypes.c_void_p),
+                ("n_attrs", ctypes.c_uint32)]
+
+
+class SrcuChainInfo(ctypes.Structure):
+    _fields_ = [("points", ctypes.c_uint64), ("voxels", ctypes.c_uint64), ("cells", ctypes.c_uint64),
+                ("voxel_key_bits", ctypes.c_uint32), ("cell_key_bits", ctypes.c_uint32),
+                ("voxel_sort_passes", ctypes.c_uint32), ("cell_sort_passes", ctypes.c_uint32),
+                ("cell_size", ctypes.c_double)]
+
+
+class SrcuKernelStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_uint64),
+                ("timed_regions", ctypes.c_uint64), ("total_ms", ctypes.c_double)]
+
+
+KERNEL_IDS = ["begin", "bounds", "voxel_plan", "voxel_hist", "voxel_sort", "voxel_segments",
+              "unpack_keys", "cell_plan", "cell_hist", "cell_sort", "cells", "hash", "ranges",
+              "normals"]
+
+
+# Every symbol include/srcuda.h declares, with its ctypes signature.
+_P = ctypes.c_void_p
+SIGNATURES = {
+    "srcu_abi_version": ([], ctypes.c_int),
+    "srcu_create": ([ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "srcu_destroy": ([_P], None),
+    "srcu_last_error": ([_P], ctypes.c_char_p),
+    "srcu_set_stream": ([_P, _P], ctypes.c_int),
+    "srcu_synchronize": ([_P], ctypes.c_int),
+    "srcu_device_bytes": ([_P], ctypes.c_uint64),
+    "srcu_voxel_centroid": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuVoxelParams),
+                             ctypes.POINTER(SrcuVoxelOut), ctypes.POINTER(ctypes.c_uint64)],
+                            ctypes.c_int),
+    "srcu_radius_normals": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuNormalParams),
+                             ctypes.POINTER(SrcuNormalOut), ctypes.POINTER(SrcuNormalStats)],
+                            ctypes.c_int),
+    "srcu_voxel_normals": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuVoxelParams),
+                            ctypes.POINTER(SrcuNormalParams), ctypes.POINTER(SrcuVoxelOut),
+                            ctypes.POINTER(SrcuNormalOut), ctypes.POINTER(ctypes.c_uint64),
+                            ctypes.POINTER(SrcuNormalStats)], ctypes.c_int),
+    "srcu_voxel_normals_enqueue": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuVoxelParams),
+                                    ctypes.POINTER(SrcuNormalParams)], ctypes.c_int),
+    "srcu_frame_view_get": ([_P, ctypes.POINTER(SrcuFrameView)], ctypes.c_int),
+    "srcu_frame_check": ([_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(SrcuNormalStats)],
+                         ctypes.c_int),
+    "srcu_frame_fetch": ([_P, ctypes.POINTER(SrcuVoxelOut), ctypes.POINTER(SrcuNormalOut),
+                          ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(SrcuNormalStats)],
+                         ctypes.c_int),
+    "srcu_chain_info_get": ([_P, ctypes.POINTER(SrcuChainInfo)], ctypes.c_int),
+    "srcu_profile_enable": ([_P, ctypes.c_uint64], ctypes.c_int),
+    "srcu_profile_read": ([_P, ctypes.POINTER(SrcuKernelStat), ctypes.c_int, ctypes.c_int],
+                          ctypes.c_int),
+}
+
+_lib = None
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def load() -> ctypes.CDLL:
+    """Loads libsrcuda.so; raises ImportError if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(
+            f"{_LIB_PATH} is missing: build it with `python -m spatialrust_b200.csrc.build` "
+            "(the CUDA library is required; there is no CPU fallback)")
+    lib = ctypes.CDLL(_LIB_PATH)
+    for name, (args, res) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _raise(status: int, message: str):
+    if status == SRCU_ERR_INVALID_ARGUMENT:
+        raise InvalidArgument(message)
+    if status == SRCU_ERR_LENGTH_MISMATCH:
+        raise BufferLengthMismatch(message)
+    if status == SRCU_ERR_UNSUPPORTED_DTYPE:
+        raise UnsupportedDType(message)
+    if status == SRCU_ERR_MISSING_FIELD:
+        raise MissingField(message)
+    if status == SRCU_ERR_OUT_OF_BUDGET:
+        raise OutOfBudget(status, message)
+    if status == SRCU_ERR_TIMEOUT:
+        raise DeviceTimeout(status, message)
+    if status == SRCU_ERR_KEY_OVERFLOW:
+        raise KeyOverflow(status, message)
+    if status == SRCU_ERR_NO_DEVICE:
+        raise NoDevice(status, message)
+    raise CudaError(status, message)
+
+
+def _is_device(a) -> bool:
+    return hasattr(a, "data_ptr") and getattr(a, "is_cuda", False)
+
+
+def _addr(a) -> int:
+    if a is None:
+        return 0
+    if hasattr(a, "data_ptr"):
+        return int(a.data_ptr())
+    return int(a.ctypes.data)
+
+
+def _as_f32_host(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class _Keep:
+    """Keeps ctypes arrays and converted buffers alive for one call."""
+
+    def __init__(self):
+        self.items = []
+
+    def add(self, x):
+        self.items.append(x)
+        return x
+
+
+def make_cloud(x, y, z, attrs: Sequence = (), keep: _Keep | None = None) -> SrcuCloud:
+    keep = keep or _Keep()
+    on_dev = _is_device(x)
+    cols = [x, y, z, *attrs]
+    if on_dev:
+        import torch
+        for c in cols:
+            if not _is_device(c) or c.dtype != torch.float32 or not c.is_contiguous():
+                raise InvalidArgument("device columns must be contiguous float32 CUDA tensors")
+    else:
+        cols = [keep.add(_as_f32_host(c)) for c in cols]
+    n = int(cols[0].shape[0])
+    for c in cols:
+        if int(c.shape[0]) != n:
+            raise BufferLengthMismatch(f"expected {n}, found {int(c.shape[0])}")
+    if len(attrs) > MAX_ATTRS:
+        raise InvalidArgument(f"at most {MAX_ATTRS} attribute columns are supported")
+    attr_arr = keep.add((ctypes.c_void_p * max(len(attrs), 1))(*[_addr(c) for c in cols[3:]]))
+    return SrcuCloud(_addr(cols[0]), _addr(cols[1]), _addr(cols[2]),
+                     ctypes.cast(attr_arr, ctypes.c_void_p), len(attrs), int(on_dev), n)
+
+
+class Context:
+    """One srcu_ctx: a CUDA device, a stream and the HBM-budgeted buffer pool."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self._lib = load()
+        h = ctypes.c_void_p()
+        st = self._lib.srcu_create(device, hbm_budget_bytes, ctypes.byref(h))
+        if st != SRCU_OK:
+            _raise(st, f"srcu_create(device={device}) failed")
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.srcu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != SRCU_OK:
+            msg = self._lib.srcu_last_error(self._h)
+            _raise(st, msg.decode() if msg else "")
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(self._lib.srcu_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)))
+
+    def synchronize(self):
+        self._check(self._lib.srcu_synchronize(self._h))
+
+    def device_bytes(self) -> int:
+        return int(self._lib.srcu_device_bytes(self._h))
+
+    def chain_info(self) -> dict:
+        info = SrcuChainInfo()
+        self._check(self._lib.srcu_chain_info_get(self._h, ctypes.byref(info)))
+        return {name: getattr(info, name) for name, _ in SrcuChainInfo._fields_}
+
+    def profile_enable(self, kernels=()):
+        """Times the named kernel groups (see KERNEL_IDS) with CUDA events."""
+        mask = 0
+        for k in kernels:
+            mask |= 1 << KERNEL_IDS.index(k)
+        self._check(self._lib.srcu_profile_enable(self._h, mask))
+
+    def profile_read(self, reset: bool = True) -> dict:
+        """{group: {name, launches, timed_regions, total_ms}} since the last reset."""
+        arr = (SrcuKernelStat * len(KERNEL_IDS))()
+        n = self._lib.srcu_profile_read(self._h, arr, len(KERNEL_IDS), int(reset))
+        if n < 0:
+            self._check(-n)
+        return {KERNEL_IDS[i]: dict(name=arr[i].name.decode(), launches=int(arr[i].launches),
+                                    timed_regions=int(arr[i].timed_regions),
+                                    total_ms=float(arr[i].total_ms)) for i in range(n)}
+
+    # ---- one cloud --------------------------------------------------------
+
+    def voxel_centroid(self, x, y, z, attrs=(), leaf: float = 1.0, origin=None,
+                       want_keys: bool = False):
+        """Returns (columns [x, y, z, attrs...], keys (V,3) int64 or None, counts) as numpy."""
+        keep = _Keep()
+        cloud = make_cloud(x, y, z, attrs, keep)
+        n = int(cloud.n)
+        ncol = 3 + len(attrs)
+        outs = [np.empty(max(n, 1), np.float32) for _ in range(ncol)]
+        counts = np.empty(max(n, 1), np.uint32)
+        keys = np.empty((max(n, 1), 3), np.int64) if want_keys else None
+        attr_out = keep.add((ctypes.c_void_p * max(ncol - 3, 1))(*[o.ctypes.data for o in outs[3:]]))
+        vout = SrcuVoxelOut(outs[0].ctypes.data, outs[1].ctypes.data, outs[2].ctypes.data,
+                            ctypes.cast(attr_out, ctypes.c_void_p),
+                            keys.ctypes.data if keys is not None else 0, counts.ctypes.data, 0)
+        vp = _voxel_params(leaf, origin)
+        nv = ctypes.c_uint64(0)
+        self._check(self._lib.srcu_voxel_centroid(self._h, ctypes.byref(cloud), ctypes.byref(vp),
+                                                  ctypes.byref(vout), ctypes.byref(nv)))
+        v = int(nv.value)
+        return ([o[:v] for o in outs], keys[:v] if keys is not None else None, counts[:v])
+
+    def radius_normals(self, x, y, z, radius: float, min_neighbors: int = 3, viewpoint=None,
+                       include_self: bool = False):
+        """Returns (nx, ny, nz, curvature, neighbor_counts, stats dict) as numpy, input order."""
+        keep = _Keep()
+        cloud = make_cloud(x, y, z, (), keep)
+        n = int(cloud.n)
+        outs = [np.empty(max(n, 1), np.float32) for _ in range(4)]
+        counts = np.empty(max(n, 1), np.uint32)
+        nout = SrcuNormalOut(*[o.ctypes.data for o in outs], counts.ctypes.data, 0)
+        np_ = _normal_params(radius, min_neighbors, viewpoint, include_self)
+        stats = SrcuNormalStats()
+        self._check(self._lib.srcu_radius_normals(self._h, ctypes.byref(cloud), ctypes.byref(np_),
+                                                  ctypes.byref(nout), ctypes.byref(stats)))
+        return (*[o[:n] for o in outs], counts[:n], _stats(stats))
+
+    def voxel_normals(self, x, y, z, attrs=(), leaf: float = 1.0, origin=None, radius: float = 0.5,
+                      min_neighbors: int = 3, viewpoint=None, include_self: bool = False,
+                      want_keys: bool = False):
+        """Voxel centroids then radius normals on them (MvpPipeline chain), numpy outputs."""
+        keep = _Keep()
+        cloud = make_cloud(x, y, z, attrs, keep)
+        n = int(cloud.n)
+        ncol = 3 + len(attrs)
+        vcols = [np.empty(max(n, 1), np.float32) for _ in range(ncol)]
+        counts = np.empty(max(n, 1), np.uint32)
+        keys = np.empty((max(n, 1), 3), np.int64) if want_keys else None
+        attr_out = keep.add((ctypes.c_void_p * max(ncol - 3, 1))(*[o.ctypes.data for o in vcols[3:]]))
+        vout = SrcuVoxelOut(vcols[0].ctypes.data, vcols[1].ctypes.data, vcols[2].ctypes.data,
+                            ctypes.cast(attr_out, ctypes.c_void_p),
+                            keys.ctypes.data if keys is not None else 0, counts.ctypes.data, 0)
+        nouts = [np.empty(max(n, 1), np.float32) for _ in range(4)]
+        ncounts = np.empty(max(n, 1), np.uint32)
+        nout = SrcuNormalOut(*[o.ctypes.data for o in nouts], ncounts.ctypes.data, 0)
+        vp = _voxel_params(leaf, origin)
+        np_ = _normal_params(radius, min_neighbors, viewpoint, include_self)
+        nv = ctypes.c_uint64(0)
+        stats = SrcuNormalStats()
+        self._check(self._lib.srcu_voxel_normals(self._h, ctypes.byref(cloud), ctypes.byref(vp),
+                                                 ctypes.byref(np_), ctypes.byref(vout),
+                                                 ctypes.byref(nout), ctypes.byref(nv),
+                                                 ctypes.byref(stats)))
+        v = int(nv.value)
+        return dict(columns=[c[:v] for c in vcols], keys=keys[:v] if keys is not None else None,
+                    counts=counts[:v], nx=nouts[0][:v], ny=nouts[1][:v], nz=nouts[2][:v],
+                    curvature=nouts[3][:v], neighbor_counts=ncounts[:v], stats=_stats(stats))
+
+    # ---- device-resident chain -------------------------------------------
+
+    def voxel_normals_enqueue(self, cloud: SrcuCloud, leaf: float, origin, radius: float,
+                              min_neighbors: int = 3, viewpoint=None, include_self: bool = False):
+        vp = _voxel_params(leaf, origin)
+        np_ = _normal_params(radius, min_neighbors, viewpoint, include_self)
+        self._check(self._lib.srcu_voxel_normals_enqueue(self._h, ctypes.byref(cloud),
+                                                         ctypes.byref(vp), ctypes.byref(np_)))
+
+    def frame_view(self) -> SrcuFrameView:
+        view = SrcuFrameView()
+        self._check(self._lib.srcu_frame_view_get(self._h, ctypes.byref(view)))
+        return view
+
+    def frame_check(self):
+        nv = ctypes.c_uint64(0)
+        stats = SrcuNormalStats()
+        self._check(self._lib.srcu_frame_check(self._h, ctypes.byref(nv), ctypes.byref(stats)))
+        return int(nv.value), _stats(stats)
+
+    def frame_fetch(self, capacity: int, n_attrs: int = 0):
+        """Reads the last enqueued chain back to numpy (capacity >= V)."""
+        keep = _Keep()
+        vcols = [np.empty(max(capacity, 1), np.float32) for _ in range(3 + n_attrs)]
+        counts = np.empty(max(capacity, 1), np.uint32)
+        attr_out = keep.add((ctypes.c_void_p * max(n_attrs, 1))(*[o.ctypes.data for o in vcols[3:]]))
+        vout = SrcuVoxelOut(vcols[0].ctypes.data, vcols[1].ctypes.data, vcols[2].ctypes.data,
+                            ctypes.cast(attr_out, ctypes.c_void_p), 0, counts.ctypes.data, 0)
+        nouts = [np.empty(max(capacity, 1), np.float32) for _ in range(4)]
+        ncounts = np.empty(max(capacity, 1), np.uint32)
+        nout = SrcuNormalOut(*[o.ctypes.data for o in nouts], ncounts.ctypes.data, 0)
+        nv = ctypes.c_uint64(0)
+        stats = SrcuNormalStats()
+        self._check(self._lib.srcu_frame_fetch(self._h, ctypes.byref(vout), ctypes.byref(nout),
+                                               ctypes.byref(nv), ctypes.byref(stats)))
+        v = int(nv.value)
+        return dict(columns=[c[:v] for c in vcols], counts=counts[:v], nx=nouts[0][:v],
+                    ny=nouts[1][:v], nz=nouts[2][:v], curvature=nouts[3][:v],
+                    neighbor_counts=ncounts[:v], stats=_stats(stats))
+
+
+def _voxel_params(leaf, origin) -> SrcuVoxelParams:
+    if origin is None:
+        return SrcuVoxelParams(float(leaf), 0, c_float3(0, 0, 0))
+    o = [float(v) for v in origin]
+    return SrcuVoxelParams(float(leaf), 1, c_float3(*o))
+
+
+def _normal_params(radius, min_neighbors, viewpoint, include_self) -> SrcuNormalParams:
+    vp = c_float3(*(float(v) for v in viewpoint)) if viewpoint is not None else c_float3(0, 0, 0)
+    return SrcuNormalParams(float(radius), int(min_neighbors), int(viewpoint is not None), vp,
+                            int(bool(include_self)))
+
+
+def _stats(s: SrcuNormalStats) -> dict:
+    return dict(valid_count=int(s.valid_count), invalid_count=int(s.invalid_count),
+                shell_points=int(s.shell_points), fp64_eigensolves=int(s.fp64_eigensolves))
+
+
+_default_ctx: dict[int, Context] = {}
+
+
+def shared_context(device: int = 0) -> Context:
+    """Process-wide context per device, the analogue of WgpuRuntime::shared()
+    (crates/spatialrust-gpu/src/runtime.rs:72-95)."""
+    ctx = _default_ctx.get(device)
+    if ctx is None:
+        ctx = Context(device)
+        _default_ctx[device] = ctx
+    return ctx

@@ -1,0 +1,451 @@
+// normals.cuh -- uniform-grid radius normals: cell plan, cell table, hashed
+// cell lookup, 3x3-column neighbour ranges, and the radius-neighbour
+// covariance + eigensolve kernel.
+//
+// Semantics follow NormalEstimator's CPU radius mode
+// (crates/spatialrust-features/src/normal.rs:102-164, 321-473): a neighbour
+// of query q is any other point p with
+//   (px-qx)^2 + (py-qy)^2 + (pz-qz)^2 <= r*r
+// evaluated in f32 with round-to-nearest and no FMA, in exactly that order
+// (kdtree.rs:544-549), so neighbour sets -- and counts -- are bit-identical
+// to the reference's KD-tree search.  Points with fewer than min_neighbors
+// neighbours get a NaN normal and curvature 0 (normal.rs:331-346).
+#pragma once
+
+#include "eig3.cuh"
+#include "radix.cuh"
+
+namespace srcu {
+
+// Cell plan from the bounds of the cloud (any box that contains every finite
+// point works).  h >= r (1 + 1e-5): points within r (f32 predicate) then
+// differ by at most one cell per axis even after the FP64 cell arithmetic.
+// h is also kept >= extent / 2^19 so every axis fits in 20 bits; larger
+// cells only add candidates, never drop neighbours.
+__global__ void k_cell_plan(Control *ctl, float radius) {
+  if (threadIdx.x != 0 || ld_relaxed_u32(&ctl->status)) return;
+  if (!(radius >= 0.0f) || isinf(radius)) {
+    atomicOr(&ctl->status, ST_BAD_PARAMS);
+    return;
+  }
+  CellPlan pl{};
+  const Bounds b = ctl->bounds;
+  double lo[3], ext[3], max_ext = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    const bool any = b.mn[a] != 0xffffffffu;
+    lo[a] = any ? double(ord2f(b.mn[a])) : 0.0;
+    const double hi = any ? double(ord2f(b.mx[a])) : 0.0;
+    ext[a] = hi - lo[a];
+    max_ext = fmax(max_ext, ext[a]);
+  }
+  double h = double(radius) * (1.0 + 1e-5);
+  h = fmax(h, max_ext * (1.0 / 524288.0));
+  h = fmax(h, 1e-30);
+  uint32_t total = 0;
+  for (int a = 0; a < 3; ++a) {
+    const double d = floor(ext[a] / h) + 1.0;
+    pl.dims[a] = d > 1048576.0 ? 1048576u : uint32_t(d);
+    pl.bits[a] = bit_width_u64(pl.dims[a] - 1);
+    total += pl.bits[a];
+    pl.origin[a] = lo[a];
+  }
+  pl.h = h;
+  pl.inv_h = 1.0 / h;
+  pl.shift_y = pl.bits[2];
+  pl.shift_x = pl.bits[1] + pl.bits[2];
+  pl.total_bits = total;
+  pl.num_digits = total == 0 ? 1u : (total + RADIX_BITS - 1) / RADIX_BITS;
+  pl.r2 = __fmul_rn(radius, radius);
+  pl.shell_tol = __fmul_rn(1e-6f, pl.r2);
+  pl.valid = 1;
+  ctl->cplan = pl;
+}
+
+// Key source for the cell sort over `count_dev` points (V for the chained
+// voxel -> normals path, n otherwise).
+struct CellKeySrc {
+  const float *x, *y, *z;
+  const unsigned long long *count_dev;
+  CellPlan pl;
+  __device__ __forceinline__ void prepare(const Control *ctl) { pl = ctl->cplan; }
+  __device__ __forceinline__ uint32_t count(const Control *ctl) const {
+    return uint32_t(count_dev ? *count_dev : ctl->n_points);
+  }
+  __device__ __forceinline__ uint32_t num_digits() const { return pl.num_digits; }
+  __device__ __forceinline__ void load(uint32_t i, uint64_t &k, uint32_t &v) const {
+    k = cell_pack(pl, x[i], y[i], z[i]);
+    v = i;
+  }
+};
+
+constexpr int CELL_THREADS = 256;
+constexpr int CELL_ITEMS = 8;
+constexpr int CELL_TILE = CELL_THREADS * CELL_ITEMS;
+
+struct CellSmem {
+  uint64_t keys[CELL_TILE + 1];
+  uint32_t scratch[CELL_THREADS / 32];
+  uint32_t tile;
+};
+
+// Cell table: gathers points into cell-sorted float4 records
+// (x, y, z, bits of the original index) and numbers the occupied cells
+// (start offsets in the sorted order, cell keys).  cell_start[U] = n.
+__global__ void __launch_bounds__(CELL_THREADS) k_cells(Control *ctl, SortBuffers sort,
+                                                        const uint32_t *final_buf,
+                                                        const unsigned long long *count_dev,
+                                                        const float *x, const float *y,
+                                                        const float *z, float4 *pts,
+                                                        uint64_t *cell_key, uint32_t *cell_start,
+                                                        uint64_t *lookback) {
+  __shared__ CellSmem sm;
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint32_t n = uint32_t(count_dev ? *count_dev : ctl->n_points);
+  if (n == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ctl->n_cells = 0;
+      cell_start[0] = 0;
+    }
+    return;
+  }
+  const uint32_t fb = *final_buf;
+  const uint64_t *keys = sort.keys[fb];
+  const uint32_t *vals = sort.vals[fb];
+  const uint32_t epoch = ctl->epoch + EP_CELLS;
+  const uint32_t num_tiles = (n + CELL_TILE - 1) / CELL_TILE;
+  const uint32_t t = threadIdx.x;
+  for (;;) {
+    if (t == 0) sm.tile = atomicAdd(&ctl->work[WK_CELLS], 1u);
+    __syncthreads();
+    const uint32_t tile = sm.tile;
+    if (tile >= num_tiles) break;
+    const uint32_t base = tile * CELL_TILE;
+    const uint32_t tile_n = min(uint32_t(CELL_TILE), n - base);
+    for (uint32_t j = t; j < tile_n; j += CELL_THREADS) {
+      sm.keys[1 + j] = keys[base + j];
+      const uint32_t v = vals[base + j];
+      if (v < n) {
+        pts[base + j] = make_float4(x[v], y[v], z[v], __uint_as_float(v));
+      } else {  // a consistent sort never produces this; never read out of bounds
+        pts[base + j] = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, __uint_as_float(0u));
+        atomicOr(&ctl->status, ST_INTERNAL);
+      }
+    }
+    if (t == 0) sm.keys[0] = base > 0 ? keys[base - 1] : ~keys[0];
+    __syncthreads();
+    const uint32_t j0 = t * CELL_ITEMS;
+    uint32_t flags = 0;
+#pragma unroll
+    for (int i = 0; i < CELL_ITEMS; ++i) {
+      const uint32_t j = j0 + i;
+      if (j < tile_n && sm.keys[1 + j] != sm.keys[j]) flags |= 1u << i;
+    }
+    uint32_t tile_count;
+    const uint32_t local = block_exclusive_sum<CELL_THREADS>(__popc(flags), sm.scratch, &tile_count);
+    if (t == 0) sm.scratch[0] = lookback_exclusive(lookback, 1, tile, tile_count, epoch, &ctl->status);
+    __syncthreads();
+    const uint32_t cbase = sm.scratch[0];
+    uint32_t c = cbase + local;
+#pragma unroll
+    for (int i = 0; i < CELL_ITEMS; ++i) {
+      if (flags & (1u << i)) {
+        if (c < n) {
+          cell_key[c] = sm.keys[1 + j0 + i];
+          cell_start[c] = base + j0 + i;
+        } else {
+          atomicOr(&ctl->status, ST_INTERNAL);
+        }
+        ++c;
+      }
+    }
+    if (t == 0 && tile == num_tiles - 1) {
+      const uint32_t u_total = min(cbase + tile_count, n);
+      ctl->n_cells = u_total;
+      cell_start[u_total] = n;
+    }
+    __syncthreads();
+  }
+}
+
+// Open-addressing table from cell key to cell number.  A slot holds
+// [epoch:32][cell:32]; slots from earlier chains read as empty, so the table
+// is cleared once at allocation only.  Keys are compared through cell_key[].
+__device__ __forceinline__ uint32_t cell_hash(uint64_t key, uint32_t log2cap) {
+  return uint32_t((key * 0x9E3779B97F4A7C15ull) >> (64 - log2cap));
+}
+
+__global__ void k_hash_insert(Control *ctl, const uint64_t *cell_key, uint64_t *table,
+                              uint32_t log2cap) {
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint64_t u_count = ctl->n_cells;
+  const uint32_t epoch = ctl->epoch + EP_CELLS;
+  const uint32_t mask = (1u << log2cap) - 1u;
+  for (uint64_t u = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; u < u_count;
+       u += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t key = cell_key[u];
+    uint32_t h = cell_hash(key, log2cap);
+    const uint64_t mine = (uint64_t(epoch) << 32) | u;
+    bool done = false;
+    for (uint32_t probe = 0; probe <= mask && !done; ++probe) {
+      unsigned long long *slot = reinterpret_cast<unsigned long long *>(table + h);
+      unsigned long long old = *reinterpret_cast<volatile unsigned long long *>(slot);
+      while (uint32_t(old >> 32) != epoch) {
+        const unsigned long long seen = atomicCAS(slot, old, (unsigned long long)mine);
+        if (seen == old) {
+          done = true;
+          break;
+        }
+        old = seen;
+      }
+      h = (h + 1) & mask;
+    }
+    if (!done) atomicOr(&ctl->status, ST_HASH_FULL);
+  }
+}
+
+__device__ __forceinline__ int32_t cell_lookup(const uint64_t *table, const uint64_t *cell_key,
+                                               uint64_t key, uint32_t log2cap, uint32_t epoch) {
+  const uint32_t mask = (1u << log2cap) - 1u;
+  uint32_t h = cell_hash(key, log2cap);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const uint64_t w = table[h];
+    if (uint32_t(w >> 32) != epoch) return -1;
+    const uint32_t u = uint32_t(w);
+    if (cell_key[u] == key) return int32_t(u);
+    h = (h + 1) & mask;
+  }
+  return -1;
+}
+
+// For every occupied cell and each of the 3x3 neighbouring columns, the range
+// of cell-sorted points in cells (cx+dx, cy+dy, cz-1 .. cz+1).  Those (at
+// most three) cells are consecutive in key order, so each column is one
+// contiguous range: 9 ranges cover the 27-cell neighbourhood.
+__global__ void k_ranges(Control *ctl, const uint64_t *cell_key, const uint32_t *cell_start,
+                         const uint64_t *table, uint32_t log2cap, uint2 *ranges) {
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const CellPlan pl = ctl->cplan;
+  const uint64_t u_count = ctl->n_cells;
+  const uint32_t epoch = ctl->epoch + EP_CELLS;
+  for (uint64_t w = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; w < u_count * 9;
+       w += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t u = w / 9;
+    const uint32_t col = uint32_t(w - u * 9);
+    uint32_t cx, cy, cz;
+    cell_unpack(pl, cell_key[u], cx, cy, cz);
+    const int64_t nx = int64_t(cx) + int64_t(col / 3) - 1;
+    const int64_t ny = int64_t(cy) + int64_t(col % 3) - 1;
+    uint2 rg = make_uint2(0, 0);
+    if (nx >= 0 && ny >= 0 && nx < pl.dims[0] && ny < pl.dims[1]) {
+      int32_t first = -1, last = -1;
+      for (int dz = -1; dz <= 1; ++dz) {
+        const int64_t nz = int64_t(cz) + dz;
+        if (nz < 0 || nz >= pl.dims[2]) continue;
+        const uint64_t key = (uint64_t(nx) << pl.shift_x) | (uint64_t(ny) << pl.shift_y) | uint64_t(nz);
+        const int32_t f = cell_lookup(table, cell_key, key, log2cap, epoch);
+        if (f >= 0) {
+          if (first < 0) first = f;
+          last = f;
+        }
+      }
+      if (first >= 0) rg = make_uint2(cell_start[first], cell_start[last + 1]);
+    }
+    ranges[w] = rg;
+  }
+}
+
+struct NormalParamsDev {
+  uint32_t min_neighbors;
+  int32_t include_self;
+  int32_t has_viewpoint;
+  float vp[3];
+};
+
+constexpr int NM_WARPS = 8;
+constexpr int NM_THREADS = NM_WARPS * 32;
+constexpr int NM_CAP = 512;  // staged candidate records per warp
+constexpr int NM_FLUSH = 32; // f32 partial moments are folded into FP64 every NM_FLUSH candidates
+
+struct NormalSmem {
+  float4 cand[NM_WARPS][NM_CAP];
+};
+
+// Radius normals, one warp per occupied cell (dynamic scheduling).  The
+// cell's points are processed in batches of <= 32 queries; the batch's
+// candidates (the 9 column ranges) are staged in shared memory and each
+// candidate is broadcast to the lanes.  With q queries in a batch, lanes are
+// split into 32/q' groups (q' = q rounded up to a power of two) that walk
+// disjoint candidate subsets, so every lane does useful work even for sparse
+// cells; the groups' moments are combined with shuffles.
+//
+// Moments are taken about the query point (d = p - q, the predicate's own
+// differences): count, sum d, sum d d^T, accumulated in f32 for NM_FLUSH
+// candidates and then folded into FP64; the covariance
+// C = S2/n - (S1/n)(S1/n)^T and its eigensolve are FP64.
+__global__ void __launch_bounds__(NM_THREADS) k_normals(Control *ctl, const float4 *pts,
+                                                        const uint32_t *cell_start,
+                                                        const uint2 *ranges, NormalParamsDev prm,
+                                                        const unsigned long long *count_dev,
+                                                        float *nx, float *ny, float *nz,
+                                                        float *curv, uint32_t *counts) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  NormalSmem &sm = *reinterpret_cast<NormalSmem *>(smem_raw);
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint64_t u_count = ctl->n_cells;
+  const uint32_t n_pts = uint32_t(count_dev ? *count_dev : ctl->n_points);
+  const float r2 = ctl->cplan.r2;
+  const float shell_tol = ctl->cplan.shell_tol;
+  float4 *buf = sm.cand[warp];
+  unsigned long long n_valid = 0, n_invalid = 0, n_shell = 0, n_fp64 = 0;
+
+  for (;;) {
+    uint32_t u = 0;
+    if (lane == 0) u = atomicAdd(&ctl->work[WK_NORMALS], 1u);
+    u = __shfl_sync(FULL_MASK, u, 0);
+    if (u >= u_count) break;
+    // the 9 column ranges and their prefix offsets
+    uint2 rg = lane < 9 ? ranges[size_t(u) * 9 + lane] : make_uint2(0, 0);
+    const uint32_t len = rg.y - rg.x;
+    uint32_t total;
+    const uint32_t excl = warp_exclusive_sum(len, &total);
+    const uint32_t q_begin = cell_start[u], q_end = cell_start[u + 1];
+
+    for (uint32_t b0 = q_begin; b0 < q_end; b0 += 32) {
+      const uint32_t q = min(32u, q_end - b0);
+      uint32_t qpad_log = 0;
+      while ((1u << qpad_log) < q) ++qpad_log;
+      const uint32_t qpad = 1u << qpad_log;
+      const uint32_t my_q = lane & (qpad - 1);
+      const uint32_t my_g = lane >> qpad_log;
+      const uint32_t groups = 32u >> qpad_log;
+      const float4 qp = pts[b0 + min(my_q, q - 1)];
+      const uint32_t qidx = __float_as_uint(qp.w);
+
+      uint32_t cnt = 0, shell = 0;
+      double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // sx sy sz sxx syy szz sxy sxz syz
+      float F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      uint32_t since_flush = 0;
+
+      for (uint32_t c0 = 0; c0 < total; c0 += NM_CAP) {
+        const uint32_t clen = min(uint32_t(NM_CAP), total - c0);
+        // stage candidates [c0, c0 + clen) of the concatenated ranges
+        for (int r = 0; r < 9; ++r) {
+          const uint32_t rs = __shfl_sync(FULL_MASK, rg.x, r);
+          const uint32_t re = __shfl_sync(FULL_MASK, excl, r);
+          const uint32_t rl = __shfl_sync(FULL_MASK, len, r);
+          const uint32_t lo = max(re, c0), hi = min(re + rl, c0 + clen);
+          for (uint32_t p = lo + lane; p < hi; p += 32) buf[p - c0] = pts[rs + (p - re)];
+        }
+        __syncwarp();
+        for (uint32_t j = my_g; j < clen; j += groups) {
+          const float4 c = buf[j];
+          const float dx = __fsub_rn(c.x, qp.x);
+          const float dy = __fsub_rn(c.y, qp.y);
+          const float dz = __fsub_rn(c.z, qp.z);
+          const float xx = __fmul_rn(dx, dx), yy = __fmul_rn(dy, dy), zz = __fmul_rn(dz, dz);
+          const float d2 = __fadd_rn(__fadd_rn(xx, yy), zz);
+          const bool other = __float_as_uint(c.w) != qidx;
+          const bool hit = (d2 <= r2) && other;
+          if (other && fabsf(__fsub_rn(d2, r2)) <= shell_tol) shell = 1;
+          if (hit) {
+            ++cnt;
+            F[0] += dx;
+            F[1] += dy;
+            F[2] += dz;
+            F[3] += xx;
+            F[4] += yy;
+            F[5] += zz;
+            F[6] = fmaf(dx, dy, F[6]);
+            F[7] = fmaf(dx, dz, F[7]);
+            F[8] = fmaf(dy, dz, F[8]);
+          }
+          if (++since_flush == NM_FLUSH) {
+            since_flush = 0;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+              S[k] += double(F[k]);
+              F[k] = 0.f;
+            }
+          }
+        }
+        __syncwarp();
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) S[k] += double(F[k]);
+      // combine the lane groups that share a query
+      for (uint32_t o = qpad; o < 32; o <<= 1) {
+        cnt += __shfl_xor_sync(FULL_MASK, cnt, o);
+        shell |= __shfl_xor_sync(FULL_MASK, shell, o);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) S[k] += __shfl_xor_sync(FULL_MASK, S[k], o);
+      }
+      if (my_g == 0 && my_q < q) {
+        const uint32_t n_eff = prm.include_self ? cnt + 1 : cnt;
+        const bool valid = prm.include_self ? (n_eff >= 3) : (cnt >= prm.min_neighbors && cnt > 0);
+        float ox, oy, oz, oc;
+        if (valid) {
+          const double inv = 1.0 / double(n_eff);
+          const double mx = S[0] * inv, my = S[1] * inv, mz = S[2] * inv;
+          const double cxx = S[3] * inv - mx * mx, cyy = S[4] * inv - my * my;
+          const double czz = S[5] * inv - mz * mz, cxy = S[6] * inv - mx * my;
+          const double cxz = S[7] * inv - mx * mz, cyz = S[8] * inv - my * mz;
+          const Eig3 e = smallest_eigenpair(cxx, cyy, czz, cxy, cxz, cyz);
+          double v0 = e.v[0], v1 = e.v[1], v2 = e.v[2];
+          if (prm.has_viewpoint) {
+            // orient_normal_towards_viewpoint, normal.rs:408-421
+            const double wx = double(prm.vp[0]) - double(qp.x);
+            const double wy = double(prm.vp[1]) - double(qp.y);
+            const double wz = double(prm.vp[2]) - double(qp.z);
+            if (v0 * wx + v1 * wy + v2 * wz < 0.0) {
+              v0 = -v0;
+              v1 = -v1;
+              v2 = -v2;
+            }
+          }
+          const double nn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+          ox = float(v0 / nn);
+          oy = float(v1 / nn);
+          oz = float(v2 / nn);
+          const double sum = e.l0 + e.l1 + e.l2;
+          oc = sum > 0.0 ? float(e.l0 / sum) : 0.0f;
+          ++n_valid;
+          n_fp64 += e.jacobi ? 1 : 0;
+        } else {
+          const float nanv = __int_as_float(0x7fc00000);
+          ox = prm.include_self ? 0.0f : nanv;
+          oy = prm.include_self ? 0.0f : nanv;
+          oz = prm.include_self ? 1.0f : nanv;
+          oc = 0.0f;
+          ++n_invalid;
+        }
+        n_shell += shell;
+        if (qidx >= n_pts) {  // cannot happen: records carry indices < n
+          atomicOr(&ctl->status, ST_INTERNAL);
+          continue;
+        }
+        nx[qidx] = ox;
+        ny[qidx] = oy;
+        nz[qidx] = oz;
+        curv[qidx] = oc;
+        if (counts) counts[qidx] = prm.include_self ? n_eff : cnt;
+      }
+    }
+  }
+  // one atomic per warp for the counters
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    n_valid += __shfl_xor_sync(FULL_MASK, n_valid, o);
+    n_invalid += __shfl_xor_sync(FULL_MASK, n_invalid, o);
+    n_shell += __shfl_xor_sync(FULL_MASK, n_shell, o);
+    n_fp64 += __shfl_xor_sync(FULL_MASK, n_fp64, o);
+  }
+  if (lane == 0) {
+    if (n_valid) atomicAdd(&ctl->ncount.valid, n_valid);
+    if (n_invalid) atomicAdd(&ctl->ncount.invalid, n_invalid);
+    if (n_shell) atomicAdd(&ctl->ncount.shell, n_shell);
+    if (n_fp64) atomicAdd(&ctl->ncount.fp64, n_fp64);
+  }
+}
+
+}  // namespace srcu

@@ -1,0 +1,180 @@
+// plans.cuh -- device control block, voxel-key and cell-key plans.
+//
+// Voxel keys reproduce the reference's integer keys bit for bit:
+//   explicit origin : ix = floor((x - ox) * inv_leaf) as i64  (voxel.rs:1088-1093)
+//   origin = min    : ix = ((x - ox) * inv_leaf) as i64        (voxel.rs:1095-1107)
+// computed with round-to-nearest f32 subtract and multiply (no FMA), with
+// Rust's saturating cast (NaN -> 0).  The three per-axis keys are packed
+// order-preservingly into one u64: (ix - kmin_x) in the high bits, then y,
+// then z, so ascending u64 order is the reference's lexicographic
+// (ix, iy, iz) order (voxel.rs:522-524).
+#pragma once
+
+#include <cstddef>
+
+#include "common.cuh"
+
+namespace srcu {
+
+constexpr int RADIX_BITS = 8;
+constexpr int RADIX_BINS = 256;
+constexpr int MAX_DIGITS = 8;  // 64-bit keys
+constexpr int MAX_COLS = 12;   // x, y, z + up to 9 attribute columns
+
+// Bounds over finite coordinates (ordered-uint encoded), with flags for
+// NaN / infinite values per axis.
+struct Bounds {
+  uint32_t mn[3];
+  uint32_t mx[3];
+  uint32_t flags;  // bit a: NaN seen on axis a; bit 3+a: +-inf seen on axis a
+  uint32_t pad;
+};
+
+struct VoxelPlan {
+  float origin[3];
+  float inv_leaf;
+  int32_t floor_mode;  // 1: explicit origin (floor), 0: min-corner origin (trunc)
+  uint32_t bits[3];
+  uint32_t shift_x, shift_y;
+  uint32_t total_bits;
+  uint32_t num_digits;
+  int64_t kmin[3];
+  uint32_t valid;
+  uint32_t pad;
+};
+
+// Uniform grid for the radius search.  Cell size h >= r (1 + 1e-5) so any two
+// points within r of each other (under the f32 predicate) lie in the same or
+// adjacent cells; cells are computed in FP64 from the f32 coordinates.
+struct CellPlan {
+  double origin[3];
+  double inv_h;
+  double h;
+  uint32_t dims[3];
+  uint32_t bits[3];
+  uint32_t shift_x, shift_y;
+  uint32_t total_bits;
+  uint32_t num_digits;
+  float r2;          // fl(r * r), the reference predicate bound (kdtree.rs:350-357)
+  float shell_tol;   // 1e-6 * r2
+  uint32_t valid;
+  uint32_t pad;
+};
+
+struct NormalCounters {
+  unsigned long long valid;
+  unsigned long long invalid;
+  unsigned long long shell;
+  unsigned long long fp64;
+};
+
+// One control block per context, zeroed (except the epoch) by k_begin at the
+// start of every chain so the whole chain can be replayed from a CUDA graph.
+struct Control {
+  uint32_t epoch;   // bumped by EPOCHS_PER_RUN per chain; look-back words carry it
+  uint32_t status;  // StatusBits
+  unsigned long long n_points;  // input points of this chain
+  unsigned long long n_voxels;  // V
+  unsigned long long n_cells;   // U (occupied radius-grid cells)
+  uint32_t work[64];            // per-kernel dynamic tile counters
+  Bounds bounds;
+  VoxelPlan vplan;
+  CellPlan cplan;
+  NormalCounters ncount;
+  uint32_t vsort_final;  // ping-pong buffer holding the sorted voxel keys
+  uint32_t csort_final;  // ping-pong buffer holding the sorted cell keys
+  uint32_t vsort_passes; // digit passes that ran (non-trivial digits)
+  uint32_t csort_passes;
+  uint32_t hist_v[MAX_DIGITS * RADIX_BINS];  // voxel-key digit histograms
+  uint32_t hist_c[MAX_DIGITS * RADIX_BINS];  // cell-key digit histograms
+};
+
+static_assert(offsetof(Control, vsort_passes) == offsetof(Control, vsort_final) + 8,
+              "k_onesweep writes the pass count two words after the buffer index");
+static_assert(offsetof(Control, csort_passes) == offsetof(Control, csort_final) + 8,
+              "k_onesweep writes the pass count two words after the buffer index");
+
+constexpr uint32_t EPOCHS_PER_RUN = 64;
+// Epoch offsets (within a run) of each look-back user.
+constexpr uint32_t EP_VSORT = 0;     // 8 passes
+constexpr uint32_t EP_VSEG = 8;
+constexpr uint32_t EP_CSORT = 16;    // 8 passes
+constexpr uint32_t EP_CELLS = 24;
+// Work-counter slots.
+constexpr int WK_VSORT = 0;   // 8 slots
+constexpr int WK_VSEG = 8;
+constexpr int WK_CSORT = 16;  // 8 slots
+constexpr int WK_CELLS = 24;
+constexpr int WK_NORMALS = 25;
+
+__device__ __forceinline__ int64_t rs_sat_i64(float t) {
+  if (isnan(t)) return 0;
+  if (t >= 9223372036854775808.0f) return INT64_MAX;
+  if (t < -9223372036854775808.0f) return INT64_MIN;
+  return static_cast<int64_t>(t);
+}
+
+__device__ __forceinline__ int64_t voxel_axis_key(float p, float o, float inv, int floor_mode) {
+  float t = __fmul_rn(__fsub_rn(p, o), inv);
+  if (floor_mode) t = floorf(t);
+  return rs_sat_i64(t);
+}
+
+__device__ __forceinline__ uint64_t voxel_pack(const VoxelPlan &pl, float x, float y, float z) {
+  const int64_t kx = voxel_axis_key(x, pl.origin[0], pl.inv_leaf, pl.floor_mode);
+  const int64_t ky = voxel_axis_key(y, pl.origin[1], pl.inv_leaf, pl.floor_mode);
+  const int64_t kz = voxel_axis_key(z, pl.origin[2], pl.inv_leaf, pl.floor_mode);
+  const uint64_t ox = uint64_t(kx) - uint64_t(pl.kmin[0]);
+  const uint64_t oy = uint64_t(ky) - uint64_t(pl.kmin[1]);
+  const uint64_t oz = uint64_t(kz) - uint64_t(pl.kmin[2]);
+  // shift by 64 is undefined; an axis with 0 bits always has offset 0.
+  const uint64_t hx = pl.shift_x >= 64 ? 0 : (ox << pl.shift_x);
+  const uint64_t hy = pl.shift_y >= 64 ? 0 : (oy << pl.shift_y);
+  return hx | hy | oz;
+}
+
+__host__ __device__ __forceinline__ void voxel_unpack(const VoxelPlan &pl, uint64_t key,
+                                                      int64_t out[3]) {
+  const uint64_t mz = pl.bits[2] >= 64 ? ~0ull : ((1ull << pl.bits[2]) - 1);
+  const uint64_t my = pl.bits[1] >= 64 ? ~0ull : ((1ull << pl.bits[1]) - 1);
+  const uint64_t oz = key & mz;
+  const uint64_t oy = pl.shift_y >= 64 ? 0 : ((key >> pl.shift_y) & my);
+  const uint64_t ox = pl.shift_x >= 64 ? 0 : (key >> pl.shift_x);
+  out[0] = int64_t(ox + uint64_t(pl.kmin[0]));
+  out[1] = int64_t(oy + uint64_t(pl.kmin[1]));
+  out[2] = int64_t(oz + uint64_t(pl.kmin[2]));
+}
+
+__device__ __forceinline__ uint32_t cell_axis(float p, double o, double inv_h, uint32_t dim) {
+  if (!isfinite(p)) return 0;  // never a neighbour: the f32 predicate is false for it
+  double u = (double(p) - o) * inv_h;
+  double f = floor(u);
+  if (!(f > 0.0)) return 0;
+  if (f >= double(dim - 1)) return dim - 1;
+  return uint32_t(f);
+}
+
+__device__ __forceinline__ uint64_t cell_pack(const CellPlan &pl, float x, float y, float z) {
+  const uint64_t cx = cell_axis(x, pl.origin[0], pl.inv_h, pl.dims[0]);
+  const uint64_t cy = cell_axis(y, pl.origin[1], pl.inv_h, pl.dims[1]);
+  const uint64_t cz = cell_axis(z, pl.origin[2], pl.inv_h, pl.dims[2]);
+  return (cx << pl.shift_x) | (cy << pl.shift_y) | cz;
+}
+
+__device__ __forceinline__ void cell_unpack(const CellPlan &pl, uint64_t key, uint32_t &cx,
+                                            uint32_t &cy, uint32_t &cz) {
+  cz = uint32_t(key & ((1ull << pl.bits[2]) - 1));
+  cy = uint32_t((key >> pl.shift_y) & ((1ull << pl.bits[1]) - 1));
+  cx = uint32_t(key >> pl.shift_x);
+}
+
+__host__ __device__ __forceinline__ uint32_t bit_width_u64(uint64_t v) {
+  uint32_t b = 0;
+  while (v) {
+    ++b;
+    v >>= 1;
+  }
+  return b;
+}
+
+}  // namespace srcu

@@ -1,0 +1,774 @@
+// srcuda.cu -- host layer and C ABI (include/srcuda.h) of the sm_100a
+// uniform-grid path: context, HBM-budgeted buffer pool, chain launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/srcuda.h"
+#include "normals.cuh"
+#include "voxel.cuh"
+
+using namespace srcu;
+
+namespace {
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct srcu_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  uint64_t budget = 0;  // 0 = unlimited
+  uint64_t used = 0;
+  std::string err;
+  Control *ctl = nullptr;       // device
+  Control *ctl_host = nullptr;  // pinned mirror for read-back
+  int occ_onesweep_v = 1, occ_onesweep_c = 1, occ_normals = 1, occ_seg = 1, occ_cells = 1;
+  // input staging (host inputs are copied here)
+  DevBuf in[MAX_COLS];
+  // sort
+  DevBuf keys[2], vals[2], lb_sort, lb_seg, lb_cells;
+  // voxel outputs: x, y, z, attrs..., packed keys, counts, unpacked keys
+  DevBuf vout[MAX_COLS], vkeys, vcounts, vkeys3;
+  // radius grid
+  DevBuf pts, cell_key, cell_start, table, ranges;
+  uint32_t table_log2 = 0;
+  // normals outputs
+  DevBuf nout[4], ncounts;
+  uint32_t last_attrs = 0;  // attribute count of the last enqueued chain
+  const float *frame_attr_ptrs[MAX_COLS] = {};
+  // launch accounting / CUDA-event timing per kernel group (srcu_profile_*)
+  uint64_t prof_mask = 0;
+  uint64_t launches[SRCU_K_COUNT] = {};
+  uint64_t timed[SRCU_K_COUNT] = {};
+  double timed_ms[SRCU_K_COUNT] = {};
+  std::vector<cudaEvent_t> ev_pool;     // 2 per pending region
+  std::vector<int> ev_pending;          // kernel id per pending region
+};
+
+namespace {
+
+srcu_status fail(srcu_ctx *c, srcu_status st, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return st;
+}
+
+#define CU_TRY(expr)                                                                     \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(ctx, SRCU_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));   \
+  } while (0)
+
+#define ST_TRY(expr)                 \
+  do {                               \
+    srcu_status s_ = (expr);         \
+    if (s_ != SRCU_OK) return s_;    \
+  } while (0)
+
+// Grows a device buffer to at least `bytes` (contents are not preserved).
+srcu_status ensure(srcu_ctx *ctx, DevBuf &b, size_t bytes, bool zero = false) {
+  if (bytes == 0) bytes = 16;
+  if (b.bytes >= bytes) return SRCU_OK;
+  size_t want = std::max(bytes, b.bytes + b.bytes / 4);  // amortise growth
+  want = (want + 255) & ~size_t(255);
+  if (ctx->budget && ctx->used - b.bytes + want > ctx->budget) {
+    want = (bytes + 255) & ~size_t(255);
+    if (ctx->used - b.bytes + want > ctx->budget)
+      return fail(ctx, SRCU_ERR_OUT_OF_BUDGET,
+                  "device allocation of %zu bytes exceeds the HBM budget (%llu of %llu bytes in use)",
+                  want, (unsigned long long)ctx->used, (unsigned long long)ctx->budget);
+  }
+  if (b.p) {
+    CU_TRY(cudaStreamSynchronize(ctx->stream));
+    CU_TRY(cudaFree(b.p));
+    ctx->used -= b.bytes;
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, SRCU_ERR_OUT_OF_BUDGET, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+  }
+  if (zero) CU_TRY(cudaMemsetAsync(p, 0, want, ctx->stream));
+  b.p = p;
+  b.bytes = want;
+  ctx->used += want;
+  return SRCU_OK;
+}
+
+void release(srcu_ctx *ctx, DevBuf &b) {
+  if (b.p) {
+    cudaFree(b.p);
+    ctx->used -= b.bytes;
+  }
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+template <class T>
+T *ptr(DevBuf &b) {
+  return static_cast<T *>(b.p);
+}
+
+uint32_t ceil_div(uint64_t a, uint64_t b) { return uint32_t((a + b - 1) / b); }
+
+const char *const kKernelNames[SRCU_K_COUNT] = {
+    "k_begin",          "k_bounds",        "k_voxel_plan",  "k_digit_hist<voxel>",
+    "k_onesweep<voxel>", "k_voxel_segments", "k_unpack_voxel_keys", "k_cell_plan",
+    "k_digit_hist<cell>", "k_onesweep<cell>", "k_cells",       "k_hash_insert",
+    "k_ranges",         "k_normals"};
+
+// Counts the launches of one kernel group and, when its bit is set in
+// prof_mask, brackets them with CUDA events on the context stream.
+struct Launch {
+  srcu_ctx *ctx;
+  int id;
+  bool timed;
+  cudaEvent_t stop = nullptr;
+  Launch(srcu_ctx *c, int kid, uint64_t count = 1) : ctx(c), id(kid) {
+    ctx->launches[id] += count;
+    timed = (ctx->prof_mask >> id) & 1u;
+    if (!timed) return;
+    const size_t need = 2 * (ctx->ev_pending.size() + 1);
+    while (ctx->ev_pool.size() < need) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) {
+        timed = false;
+        return;
+      }
+      ctx->ev_pool.push_back(e);
+    }
+    const size_t slot = ctx->ev_pending.size();
+    ctx->ev_pending.push_back(id);
+    cudaEventRecord(ctx->ev_pool[2 * slot], ctx->stream);
+    stop = ctx->ev_pool[2 * slot + 1];
+  }
+  ~Launch() {
+    if (timed) cudaEventRecord(stop, ctx->stream);
+  }
+};
+
+uint32_t log2_ceil(uint64_t v) {
+  uint32_t l = 0;
+  while ((1ull << l) < v) ++l;
+  return l;
+}
+
+srcu_status check_cloud(srcu_ctx *ctx, const srcu_cloud *cloud) {
+  if (!cloud) return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "cloud is NULL");
+  if (cloud->n > LB_MAX_COUNT)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "cloud has %llu points; the limit is %llu",
+                (unsigned long long)cloud->n, (unsigned long long)LB_MAX_COUNT);
+  if (cloud->n_attrs > MAX_COLS - 3)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "at most %d attribute columns are supported",
+                MAX_COLS - 3);
+  if (cloud->n > 0 && (!cloud->x || !cloud->y || !cloud->z))
+    return fail(ctx, SRCU_ERR_MISSING_FIELD, "position column is NULL");
+  for (uint32_t a = 0; a < cloud->n_attrs; ++a)
+    if (cloud->n > 0 && (!cloud->attrs || !cloud->attrs[a]))
+      return fail(ctx, SRCU_ERR_MISSING_FIELD, "attribute column %u is NULL", a);
+  return SRCU_OK;
+}
+
+// Buffers for a chain over n points with `cols` columns.
+srcu_status reserve(srcu_ctx *ctx, uint64_t n, uint32_t cols, bool host_input, bool voxel,
+                    bool normals) {
+  const uint64_t m = std::max<uint64_t>(n, 1);
+  if (host_input)
+    for (uint32_t c = 0; c < cols; ++c) ST_TRY(ensure(ctx, ctx->in[c], m * 4));
+  ST_TRY(ensure(ctx, ctx->keys[0], m * 8));
+  ST_TRY(ensure(ctx, ctx->keys[1], m * 8));
+  ST_TRY(ensure(ctx, ctx->vals[0], m * 4));
+  ST_TRY(ensure(ctx, ctx->vals[1], m * 4));
+  ST_TRY(ensure(ctx, ctx->lb_sort, size_t(ceil_div(m, OS_TILE)) * RADIX_BINS * 8, true));
+  if (voxel) {
+    ST_TRY(ensure(ctx, ctx->lb_seg, size_t(ceil_div(m, SEG_TILE)) * 8, true));
+    for (uint32_t c = 0; c < cols; ++c) ST_TRY(ensure(ctx, ctx->vout[c], m * 4));
+    ST_TRY(ensure(ctx, ctx->vkeys, m * 8));
+    ST_TRY(ensure(ctx, ctx->vcounts, m * 4));
+  }
+  if (normals) {
+    ST_TRY(ensure(ctx, ctx->lb_cells, size_t(ceil_div(m, CELL_TILE)) * 8, true));
+    ST_TRY(ensure(ctx, ctx->pts, m * 16));
+    ST_TRY(ensure(ctx, ctx->cell_key, m * 8));
+    ST_TRY(ensure(ctx, ctx->cell_start, (m + 1) * 4));
+    ST_TRY(ensure(ctx, ctx->ranges, m * 9 * sizeof(uint2)));
+    const uint32_t l2 = std::max<uint32_t>(log2_ceil(2 * m), 4);
+    const size_t tbytes = (size_t(1) << l2) * 8;
+    if (ctx->table.bytes < tbytes || ctx->table_log2 == 0) {
+      ST_TRY(ensure(ctx, ctx->table, tbytes, true));
+    }
+    // use the whole allocation (a power of two no smaller than 2m)
+    uint32_t have = 4;
+    while ((size_t(1) << (have + 1)) * 8 <= ctx->table.bytes) ++have;
+    ctx->table_log2 = have;
+    for (int c = 0; c < 4; ++c) ST_TRY(ensure(ctx, ctx->nout[c], m * 4));
+    ST_TRY(ensure(ctx, ctx->ncounts, m * 4));
+  }
+  return SRCU_OK;
+}
+
+srcu_status stage_input(srcu_ctx *ctx, const srcu_cloud *cloud, const float **cols) {
+  const uint32_t nc = 3 + cloud->n_attrs;
+  const float *src[MAX_COLS] = {cloud->x, cloud->y, cloud->z};
+  for (uint32_t a = 0; a < cloud->n_attrs; ++a) src[3 + a] = cloud->attrs[a];
+  for (uint32_t c = 0; c < nc; ++c) {
+    if (cloud->on_device) {
+      cols[c] = src[c];
+    } else {
+      if (cloud->n)
+        CU_TRY(cudaMemcpyAsync(ctx->in[c].p, src[c], cloud->n * 4, cudaMemcpyHostToDevice,
+                               ctx->stream));
+      cols[c] = ptr<const float>(ctx->in[c]);
+    }
+  }
+  return SRCU_OK;
+}
+
+SortBuffers sort_buffers(srcu_ctx *ctx) {
+  SortBuffers sb;
+  sb.keys[0] = ptr<uint64_t>(ctx->keys[0]);
+  sb.keys[1] = ptr<uint64_t>(ctx->keys[1]);
+  sb.vals[0] = ptr<uint32_t>(ctx->vals[0]);
+  sb.vals[1] = ptr<uint32_t>(ctx->vals[1]);
+  sb.lookback = ptr<uint64_t>(ctx->lb_sort);
+  return sb;
+}
+
+template <class Src>
+srcu_status launch_sort(srcu_ctx *ctx, const Src &src, uint64_t n_max, uint32_t *hist,
+                        uint32_t epoch_off, int work_slot, uint32_t *final_buf, int occ,
+                        int hist_id, int sort_id) {
+  const uint32_t grid_h = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n_max, HIST_THREADS * 8),
+                                                                    uint32_t(ctx->num_sms) * 4));
+  {
+    Launch l(ctx, hist_id);
+    k_digit_hist<Src><<<grid_h, HIST_THREADS, 0, ctx->stream>>>(src, ctx->ctl, hist);
+  }
+  const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, OS_TILE));
+  const uint32_t grid_s = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(occ));
+  const SortBuffers sb = sort_buffers(ctx);
+  Launch l(ctx, sort_id, MAX_DIGITS);
+  for (int k = 0; k < MAX_DIGITS; ++k)
+    k_onesweep<Src><<<grid_s, OS_THREADS, sizeof(OnesweepSmem), ctx->stream>>>(
+        src, ctx->ctl, hist, sb, k, epoch_off, work_slot, final_buf);
+  CU_TRY(cudaGetLastError());
+  return SRCU_OK;
+}
+
+template <int NC>
+void launch_segments_nc(srcu_ctx *ctx, const float **in, uint32_t grid) {
+  Columns<NC> cols;
+  for (int c = 0; c < NC; ++c) {
+    cols.in[c] = in[c];
+    cols.out[c] = ptr<float>(ctx->vout[c]);
+  }
+  k_voxel_segments<NC><<<grid, SEG_THREADS, 0, ctx->stream>>>(
+      ctx->ctl, sort_buffers(ctx), &ctx->ctl->vsort_final, cols, ptr<uint64_t>(ctx->vkeys),
+      ptr<uint32_t>(ctx->vcounts), ptr<uint64_t>(ctx->lb_seg));
+}
+
+// Voxel stage: bounds -> plan -> sort -> fused segment/centroid reduction.
+srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t n,
+                          const srcu_voxel_params *vp) {
+  const uint32_t grid_b = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4),
+                                                                    uint32_t(ctx->num_sms) * 8));
+  {
+    Launch l(ctx, SRCU_K_BOUNDS);
+    k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(in[0], in[1], in[2], ctx->ctl, nullptr);
+  }
+  {
+    Launch l(ctx, SRCU_K_VOXEL_PLAN);
+    k_voxel_plan<<<1, 32, 0, ctx->stream>>>(ctx->ctl, vp->leaf_size, vp->has_origin,
+                                            vp->origin[0], vp->origin[1], vp->origin[2]);
+  }
+  VoxelKeySrc src;
+  src.x = in[0];
+  src.y = in[1];
+  src.z = in[2];
+  ST_TRY(launch_sort(ctx, src, n, ctx->ctl->hist_v, EP_VSORT, WK_VSORT, &ctx->ctl->vsort_final,
+                     ctx->occ_onesweep_v, SRCU_K_VOXEL_HIST, SRCU_K_VOXEL_SORT));
+  const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n, SEG_TILE));
+  const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(ctx->occ_seg));
+  Launch l(ctx, SRCU_K_VOXEL_SEGMENTS);
+  switch (nc) {
+    case 3: launch_segments_nc<3>(ctx, in, grid); break;
+    case 4: launch_segments_nc<4>(ctx, in, grid); break;
+    case 5: launch_segments_nc<5>(ctx, in, grid); break;
+    case 6: launch_segments_nc<6>(ctx, in, grid); break;
+    case 7: launch_segments_nc<7>(ctx, in, grid); break;
+    case 8: launch_segments_nc<8>(ctx, in, grid); break;
+    case 9: launch_segments_nc<9>(ctx, in, grid); break;
+    case 10: launch_segments_nc<10>(ctx, in, grid); break;
+    case 11: launch_segments_nc<11>(ctx, in, grid); break;
+    case 12: launch_segments_nc<12>(ctx, in, grid); break;
+    default: return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "unsupported column count %u", nc);
+  }
+  CU_TRY(cudaGetLastError());
+  return SRCU_OK;
+}
+
+// Normals stage over (x, y, z) with the point count in *count_dev (device)
+// or ctl->n_points when count_dev is null; n_max bounds the grid sizes.
+srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const float *z,
+                            const unsigned long long *count_dev, uint64_t n_max,
+                            const srcu_normal_params *np) {
+  {
+    Launch l(ctx, SRCU_K_CELL_PLAN);
+    k_cell_plan<<<1, 32, 0, ctx->stream>>>(ctx->ctl, np->radius);
+  }
+  CellKeySrc src;
+  src.x = x;
+  src.y = y;
+  src.z = z;
+  src.count_dev = count_dev;
+  ST_TRY(launch_sort(ctx, src, n_max, ctx->ctl->hist_c, EP_CSORT, WK_CSORT,
+                     &ctx->ctl->csort_final, ctx->occ_onesweep_c, SRCU_K_CELL_HIST,
+                     SRCU_K_CELL_SORT));
+  const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, CELL_TILE));
+  const uint32_t grid_c = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(ctx->occ_cells));
+  {
+    Launch l(ctx, SRCU_K_CELLS);
+    k_cells<<<grid_c, CELL_THREADS, 0, ctx->stream>>>(
+        ctx->ctl, sort_buffers(ctx), &ctx->ctl->csort_final, count_dev, x, y, z,
+        ptr<float4>(ctx->pts), ptr<uint64_t>(ctx->cell_key), ptr<uint32_t>(ctx->cell_start),
+        ptr<uint64_t>(ctx->lb_cells));
+  }
+  const uint32_t grid_g = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n_max, 256),
+                                                                    uint32_t(ctx->num_sms) * 8));
+  {
+    Launch l(ctx, SRCU_K_HASH);
+    k_hash_insert<<<grid_g, 256, 0, ctx->stream>>>(ctx->ctl, ptr<uint64_t>(ctx->cell_key),
+                                                   ptr<uint64_t>(ctx->table), ctx->table_log2);
+  }
+  const uint32_t grid_r = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n_max * 9, 256),
+                                                                    uint32_t(ctx->num_sms) * 16));
+  {
+    Launch l(ctx, SRCU_K_RANGES);
+    k_ranges<<<grid_r, 256, 0, ctx->stream>>>(ctx->ctl, ptr<uint64_t>(ctx->cell_key),
+                                              ptr<uint32_t>(ctx->cell_start),
+                                              ptr<uint64_t>(ctx->table), ctx->table_log2,
+                                              ptr<uint2>(ctx->ranges));
+  }
+  NormalParamsDev prm;
+  prm.min_neighbors = np->min_neighbors;
+  prm.include_self = np->include_self;
+  prm.has_viewpoint = np->has_viewpoint;
+  prm.vp[0] = np->viewpoint[0];
+  prm.vp[1] = np->viewpoint[1];
+  prm.vp[2] = np->viewpoint[2];
+  const uint32_t grid_n = uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals);
+  Launch l(ctx, SRCU_K_NORMALS);
+  k_normals<<<grid_n, NM_THREADS, sizeof(NormalSmem), ctx->stream>>>(
+      ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->cell_start), ptr<uint2>(ctx->ranges),
+      prm, count_dev, ptr<float>(ctx->nout[0]), ptr<float>(ctx->nout[1]), ptr<float>(ctx->nout[2]),
+      ptr<float>(ctx->nout[3]), ptr<uint32_t>(ctx->ncounts));
+  CU_TRY(cudaGetLastError());
+  return SRCU_OK;
+}
+
+void begin_chain(srcu_ctx *ctx, uint64_t n) {
+  Launch l(ctx, SRCU_K_BEGIN);
+  k_begin<<<1, 256, 0, ctx->stream>>>(ctx->ctl, n);
+}
+
+srcu_status read_control(srcu_ctx *ctx) {
+  CU_TRY(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(Control), cudaMemcpyDeviceToHost,
+                         ctx->stream));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  const uint32_t st = ctx->ctl_host->status;
+  if (st == 0) return SRCU_OK;
+  if (st & ST_TIMEOUT)
+    return fail(ctx, SRCU_ERR_TIMEOUT, "a bounded device-side wait gave up (status 0x%x)", st);
+  if (st & ST_TOO_MANY_POINTS)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "too many points for one chain (status 0x%x)", st);
+  if (st & ST_KEY_OVERFLOW)
+    return fail(ctx, SRCU_ERR_KEY_OVERFLOW,
+                "voxel keys of this cloud need more than 64 bits or a coordinate is infinite "
+                "(status 0x%x)", st);
+  if (st & ST_BAD_PARAMS)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "search_radius must be a finite, non-negative number");
+  if (st & ST_INTERNAL)
+    return fail(ctx, SRCU_ERR_CUDA, "internal consistency check failed on the device (status 0x%x)", st);
+  return fail(ctx, SRCU_ERR_CUDA, "device status 0x%x", st);
+}
+
+srcu_status copy_out(srcu_ctx *ctx, void *dst, const void *src, size_t bytes, int on_device) {
+  if (!dst || bytes == 0) return SRCU_OK;
+  CU_TRY(cudaMemcpyAsync(dst, src, bytes,
+                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+  return SRCU_OK;
+}
+
+srcu_status check_voxel_params(srcu_ctx *ctx, const srcu_voxel_params *vp) {
+  if (!vp) return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "voxel params are NULL");
+  if (vp->leaf_size <= 0.0f)  // voxel.rs:260-264 (a NaN leaf is not rejected there either)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "leaf_size must be greater than zero");
+  return SRCU_OK;
+}
+
+srcu_status check_normal_params(srcu_ctx *ctx, const srcu_normal_params *np) {
+  if (!np) return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "normal params are NULL");
+  if (np->radius < 0.0f)  // normal.rs:109-111
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "search_radius must be non-negative");
+  if (!(np->radius >= 0.0f) || np->radius == INFINITY)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "search_radius must be finite");
+  return SRCU_OK;
+}
+
+srcu_status fetch_voxels(srcu_ctx *ctx, uint32_t nc, const srcu_voxel_out *out, uint64_t v) {
+  if (!out) return SRCU_OK;
+  float *dst[MAX_COLS] = {out->x, out->y, out->z};
+  for (uint32_t a = 3; a < nc; ++a) dst[a] = out->attrs ? out->attrs[a - 3] : nullptr;
+  for (uint32_t c = 0; c < nc; ++c)
+    ST_TRY(copy_out(ctx, dst[c], ctx->vout[c].p, v * 4, out->on_device));
+  ST_TRY(copy_out(ctx, out->counts, ctx->vcounts.p, v * 4, out->on_device));
+  if (out->keys) ST_TRY(copy_out(ctx, out->keys, ctx->vkeys3.p, v * 24, out->on_device));
+  return SRCU_OK;
+}
+
+srcu_status fetch_normals(srcu_ctx *ctx, const srcu_normal_out *out, uint64_t m,
+                          srcu_normal_stats *stats) {
+  if (out) {
+    float *dst[4] = {out->nx, out->ny, out->nz, out->curvature};
+    for (int c = 0; c < 4; ++c) ST_TRY(copy_out(ctx, dst[c], ctx->nout[c].p, m * 4, out->on_device));
+    ST_TRY(copy_out(ctx, out->neighbor_counts, ctx->ncounts.p, m * 4, out->on_device));
+  }
+  if (stats) {
+    stats->valid_count = ctx->ctl_host->ncount.valid;
+    stats->invalid_count = ctx->ctl_host->ncount.invalid;
+    stats->shell_points = ctx->ctl_host->ncount.shell;
+    stats->fp64_eigensolves = ctx->ctl_host->ncount.fp64;
+  }
+  return SRCU_OK;
+}
+
+srcu_status unpack_keys(srcu_ctx *ctx, uint64_t n) {
+  ST_TRY(ensure(ctx, ctx->vkeys3, std::max<uint64_t>(n, 1) * 24));
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, 256), ctx->num_sms * 8));
+  Launch l(ctx, SRCU_K_UNPACK_KEYS);
+  k_unpack_voxel_keys<<<grid, 256, 0, ctx->stream>>>(ctx->ctl, ptr<uint64_t>(ctx->vkeys),
+                                                     ptr<int64_t>(ctx->vkeys3));
+  CU_TRY(cudaGetLastError());
+  return SRCU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int srcu_abi_version(void) { return SRCU_ABI_VERSION; }
+
+srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
+  if (!out) return SRCU_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) {
+    cudaGetLastError();
+    return SRCU_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+    cudaGetLastError();
+    return SRCU_ERR_NO_DEVICE;
+  }
+  srcu_ctx *ctx = new srcu_ctx();
+  ctx->device = device;
+  ctx->budget = hbm_budget_bytes;
+  ctx->num_sms = prop.multiProcessorCount;
+  auto bail = [&](srcu_status st) {
+    srcu_destroy(ctx);
+    return st;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) return bail(SRCU_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(SRCU_ERR_CUDA);
+  ctx->stream = ctx->own_stream;
+  if (cudaMalloc(&ctx->ctl, sizeof(Control)) != cudaSuccess) return bail(SRCU_ERR_OUT_OF_BUDGET);
+  ctx->used += sizeof(Control);
+  if (cudaMemset(ctx->ctl, 0, sizeof(Control)) != cudaSuccess) return bail(SRCU_ERR_CUDA);
+  if (cudaMallocHost(&ctx->ctl_host, sizeof(Control)) != cudaSuccess) return bail(SRCU_ERR_CUDA);
+  // Kernels with more than 48 KB of dynamic shared memory opt in once.
+  if (cudaFuncSetAttribute(k_onesweep<VoxelKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           sizeof(OnesweepSmem)) != cudaSuccess ||
+      cudaFuncSetAttribute(k_onesweep<CellKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           sizeof(OnesweepSmem)) != cudaSuccess ||
+      cudaFuncSetAttribute(k_normals, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           sizeof(NormalSmem)) != cudaSuccess)
+    return bail(SRCU_ERR_CUDA);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_v, k_onesweep<VoxelKeySrc>,
+                                                OS_THREADS, sizeof(OnesweepSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_c, k_onesweep<CellKeySrc>,
+                                                OS_THREADS, sizeof(OnesweepSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals, k_normals, NM_THREADS,
+                                                sizeof(NormalSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_seg, k_voxel_segments<4>, SEG_THREADS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_cells, k_cells, CELL_THREADS, 0);
+  ctx->occ_onesweep_v = std::max(1, ctx->occ_onesweep_v);
+  ctx->occ_onesweep_c = std::max(1, ctx->occ_onesweep_c);
+  ctx->occ_normals = std::max(1, ctx->occ_normals);
+  ctx->occ_seg = std::max(1, ctx->occ_seg);
+  ctx->occ_cells = std::max(1, ctx->occ_cells);
+  if (cudaGetLastError() != cudaSuccess) return bail(SRCU_ERR_CUDA);
+  *out = ctx;
+  return SRCU_OK;
+}
+
+void srcu_destroy(srcu_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  DevBuf *all[] = {&ctx->keys[0], &ctx->keys[1], &ctx->vals[0], &ctx->vals[1], &ctx->lb_sort,
+                   &ctx->lb_seg, &ctx->lb_cells, &ctx->vkeys, &ctx->vcounts, &ctx->vkeys3,
+                   &ctx->pts, &ctx->cell_key, &ctx->cell_start, &ctx->table, &ctx->ranges,
+                   &ctx->ncounts};
+  for (DevBuf *b : all) release(ctx, *b);
+  for (auto &b : ctx->in) release(ctx, b);
+  for (auto &b : ctx->vout) release(ctx, b);
+  for (auto &b : ctx->nout) release(ctx, b);
+  for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+  if (ctx->ctl) cudaFree(ctx->ctl);
+  if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+}
+
+const char *srcu_last_error(const srcu_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+srcu_status srcu_set_stream(srcu_ctx *ctx, void *cuda_stream) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  ctx->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->own_stream;
+  return SRCU_OK;
+}
+
+srcu_status srcu_synchronize(srcu_ctx *ctx) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  return SRCU_OK;
+}
+
+uint64_t srcu_device_bytes(const srcu_ctx *ctx) { return ctx ? ctx->used : 0; }
+
+srcu_status srcu_voxel_centroid(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                const srcu_voxel_params *params, const srcu_voxel_out *out,
+                                uint64_t *out_voxels) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  if (out_voxels) *out_voxels = 0;
+  ST_TRY(check_cloud(ctx, cloud));
+  ST_TRY(check_voxel_params(ctx, params));
+  CU_TRY(cudaSetDevice(ctx->device));
+  const uint64_t n = cloud->n;
+  if (n == 0) return SRCU_OK;  // voxel.rs:257-259: empty input is returned unchanged
+  const uint32_t nc = 3 + cloud->n_attrs;
+  ST_TRY(reserve(ctx, n, nc, !cloud->on_device, true, false));
+  if (out && out->keys) ST_TRY(ensure(ctx, ctx->vkeys3, n * 24));
+  const float *cols[MAX_COLS];
+  ST_TRY(stage_input(ctx, cloud, cols));
+  begin_chain(ctx, n);
+  ST_TRY(enqueue_voxel(ctx, cols, nc, n, params));
+  if (out && out->keys) ST_TRY(unpack_keys(ctx, n));
+  ST_TRY(read_control(ctx));
+  const uint64_t v = ctx->ctl_host->n_voxels;
+  ST_TRY(fetch_voxels(ctx, nc, out, v));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  if (out_voxels) *out_voxels = v;
+  return SRCU_OK;
+}
+
+srcu_status srcu_radius_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                const srcu_normal_params *params, const srcu_normal_out *out,
+                                srcu_normal_stats *stats) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  if (stats) memset(stats, 0, sizeof(*stats));
+  ST_TRY(check_cloud(ctx, cloud));
+  ST_TRY(check_normal_params(ctx, params));
+  CU_TRY(cudaSetDevice(ctx->device));
+  const uint64_t n = cloud->n;
+  if (n == 0) return SRCU_OK;  // normal.rs:106-108
+  ST_TRY(reserve(ctx, n, 3, !cloud->on_device, false, true));
+  srcu_cloud xyz = *cloud;
+  xyz.n_attrs = 0;
+  const float *cols[MAX_COLS];
+  ST_TRY(stage_input(ctx, &xyz, cols));
+  begin_chain(ctx, n);
+  const uint32_t grid_b = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4),
+                                                                    uint32_t(ctx->num_sms) * 8));
+  {
+    Launch l(ctx, SRCU_K_BOUNDS);
+    k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(cols[0], cols[1], cols[2], ctx->ctl, nullptr);
+  }
+  ST_TRY(enqueue_normals(ctx, cols[0], cols[1], cols[2], nullptr, n, params));
+  ST_TRY(read_control(ctx));
+  ST_TRY(fetch_normals(ctx, out, n, stats));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  return SRCU_OK;
+}
+
+srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
+                               const srcu_voxel_params *vparams, const srcu_normal_params *nparams,
+                               const srcu_voxel_out *vout, const srcu_normal_out *nout,
+                               uint64_t *out_voxels, srcu_normal_stats *stats) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  if (out_voxels) *out_voxels = 0;
+  if (stats) memset(stats, 0, sizeof(*stats));
+  ST_TRY(check_cloud(ctx, cloud));
+  ST_TRY(check_voxel_params(ctx, vparams));
+  ST_TRY(check_normal_params(ctx, nparams));
+  CU_TRY(cudaSetDevice(ctx->device));
+  const uint64_t n = cloud->n;
+  if (n == 0) return SRCU_OK;
+  const uint32_t nc = 3 + cloud->n_attrs;
+  ST_TRY(reserve(ctx, n, nc, !cloud->on_device, true, true));
+  if (vout && vout->keys) ST_TRY(ensure(ctx, ctx->vkeys3, n * 24));
+  const float *cols[MAX_COLS];
+  ST_TRY(stage_input(ctx, cloud, cols));
+  begin_chain(ctx, n);
+  ST_TRY(enqueue_voxel(ctx, cols, nc, n, vparams));
+  // Normals on the centroids (mvp.rs:220-222); the input bounds contain them.
+  ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
+                         ptr<float>(ctx->vout[2]), &ctx->ctl->n_voxels, n, nparams));
+  if (vout && vout->keys) ST_TRY(unpack_keys(ctx, n));
+  ST_TRY(read_control(ctx));
+  const uint64_t v = ctx->ctl_host->n_voxels;
+  ST_TRY(fetch_voxels(ctx, nc, vout, v));
+  ST_TRY(fetch_normals(ctx, nout, v, stats));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  if (out_voxels) *out_voxels = v;
+  return SRCU_OK;
+}
+
+srcu_status srcu_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                       const srcu_voxel_params *vparams,
+                                       const srcu_normal_params *nparams) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  ST_TRY(check_cloud(ctx, cloud));
+  ST_TRY(check_voxel_params(ctx, vparams));
+  ST_TRY(check_normal_params(ctx, nparams));
+  if (!cloud->on_device)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "enqueue needs a device-resident cloud");
+  const uint64_t n = cloud->n;
+  const uint32_t nc = 3 + cloud->n_attrs;
+  ST_TRY(reserve(ctx, n, nc, false, true, true));
+  const float *cols[MAX_COLS];
+  ST_TRY(stage_input(ctx, cloud, cols));
+  begin_chain(ctx, n);
+  if (n > 0) {
+    ST_TRY(enqueue_voxel(ctx, cols, nc, n, vparams));
+    ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
+                           ptr<float>(ctx->vout[2]), &ctx->ctl->n_voxels, n, nparams));
+  }
+  ctx->last_attrs = cloud->n_attrs;
+  CU_TRY(cudaGetLastError());
+  return SRCU_OK;
+}
+
+srcu_status srcu_frame_view_get(srcu_ctx *ctx, srcu_frame_view *view) {
+  if (!ctx || !view) return SRCU_ERR_INVALID_ARGUMENT;
+  view->x = ptr<const float>(ctx->vout[0]);
+  view->y = ptr<const float>(ctx->vout[1]);
+  view->z = ptr<const float>(ctx->vout[2]);
+  for (uint32_t a = 0; a < ctx->last_attrs; ++a) ctx->frame_attr_ptrs[a] = ptr<const float>(ctx->vout[3 + a]);
+  view->attrs = ctx->frame_attr_ptrs;
+  view->n_attrs = ctx->last_attrs;
+  view->nx = ptr<const float>(ctx->nout[0]);
+  view->ny = ptr<const float>(ctx->nout[1]);
+  view->nz = ptr<const float>(ctx->nout[2]);
+  view->curvature = ptr<const float>(ctx->nout[3]);
+  view->counts = ptr<const uint32_t>(ctx->vcounts);
+  view->voxel_count = reinterpret_cast<const uint64_t *>(&ctx->ctl->n_voxels);
+  return SRCU_OK;
+}
+
+srcu_status srcu_frame_check(srcu_ctx *ctx, uint64_t *out_voxels, srcu_normal_stats *stats) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  ST_TRY(read_control(ctx));
+  if (out_voxels) *out_voxels = ctx->ctl_host->n_voxels;
+  return fetch_normals(ctx, nullptr, 0, stats);
+}
+
+srcu_status srcu_frame_fetch(srcu_ctx *ctx, const srcu_voxel_out *vout, const srcu_normal_out *nout,
+                             uint64_t *out_voxels, srcu_normal_stats *stats) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  ST_TRY(read_control(ctx));
+  const uint64_t v = ctx->ctl_host->n_voxels;
+  if (vout && vout->keys)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "frame read-back does not unpack voxel keys");
+  ST_TRY(fetch_voxels(ctx, 3 + ctx->last_attrs, vout, v));
+  ST_TRY(fetch_normals(ctx, nout, v, stats));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  if (out_voxels) *out_voxels = v;
+  return SRCU_OK;
+}
+
+srcu_status srcu_chain_info_get(srcu_ctx *ctx, srcu_chain_info *info) {
+  if (!ctx || !info) return SRCU_ERR_INVALID_ARGUMENT;
+  CU_TRY(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(Control), cudaMemcpyDeviceToHost,
+                         ctx->stream));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  const Control &c = *ctx->ctl_host;
+  info->points = c.n_points;
+  info->voxels = c.n_voxels;
+  info->cells = c.n_cells;
+  info->voxel_key_bits = c.vplan.total_bits;
+  info->cell_key_bits = c.cplan.total_bits;
+  info->voxel_sort_passes = c.vsort_passes;
+  info->cell_sort_passes = c.csort_passes;
+  info->cell_size = c.cplan.h;
+  return SRCU_OK;
+}
+
+srcu_status srcu_profile_enable(srcu_ctx *ctx, uint64_t timed_kernel_mask) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  ctx->prof_mask = timed_kernel_mask;
+  return SRCU_OK;
+}
+
+int srcu_profile_read(srcu_ctx *ctx, srcu_kernel_stat *out, int max_entries, int reset) {
+  if (!ctx || (!out && max_entries > 0)) return -int(SRCU_ERR_INVALID_ARGUMENT);
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return -int(SRCU_ERR_CUDA);
+  for (size_t r = 0; r < ctx->ev_pending.size(); ++r) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->ev_pool[2 * r], ctx->ev_pool[2 * r + 1]) == cudaSuccess) {
+      ctx->timed_ms[ctx->ev_pending[r]] += double(ms);
+      ctx->timed[ctx->ev_pending[r]] += 1;
+    }
+  }
+  ctx->ev_pending.clear();
+  const int n = std::min<int>(max_entries, SRCU_K_COUNT);
+  for (int i = 0; i < n; ++i) {
+    memset(&out[i], 0, sizeof(out[i]));
+    strncpy(out[i].name, kKernelNames[i], sizeof(out[i].name) - 1);
+    out[i].launches = ctx->launches[i];
+    out[i].timed_regions = ctx->timed[i];
+    out[i].total_ms = ctx->timed_ms[i];
+  }
+  if (reset) {
+    for (int i = 0; i < SRCU_K_COUNT; ++i) {
+      ctx->launches[i] = 0;
+      ctx->timed[i] = 0;
+      ctx->timed_ms[i] = 0.0;
+    }
+  }
+  return n;
+}
+
+}  // extern "C"

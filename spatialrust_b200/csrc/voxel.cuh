@@ -1,0 +1,338 @@
+// voxel.cuh -- bounds, voxel-key plan, and the fused segment + centroid
+// reduction of the VoxelGrid centroid downsample.
+#pragma once
+
+#include "radix.cuh"
+
+namespace srcu {
+
+constexpr int BND_THREADS = 256;
+
+// k_begin: zeroes the control block for a new chain and advances the epoch.
+__global__ void k_begin(Control *ctl, unsigned long long n_points) {
+  const uint32_t t = threadIdx.x;
+  uint32_t *w = reinterpret_cast<uint32_t *>(ctl);
+  const uint32_t words = sizeof(Control) / 4;
+  // word 0 is the epoch
+  for (uint32_t i = 1 + t; i < words; i += blockDim.x) w[i] = 0;
+  __syncthreads();
+  if (t == 0) {
+    ctl->epoch += EPOCHS_PER_RUN;
+    ctl->n_points = n_points;
+    for (int a = 0; a < 3; ++a) {
+      ctl->bounds.mn[a] = 0xffffffffu;  // f2ord(+max) sentinel: atomicMin target
+      ctl->bounds.mx[a] = 0u;
+    }
+  }
+}
+
+// Per-axis min/max over finite coordinates plus NaN / inf flags
+// (compute_bounds, voxel.rs:1067-1079, ignores NaN through f32::min/max).
+// Reads `count` from *count_dev when non-null, else uses n.
+__global__ void __launch_bounds__(BND_THREADS) k_bounds(const float *x, const float *y,
+                                                        const float *z, Control *ctl,
+                                                        const unsigned long long *count_dev) {
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint64_t n = count_dev ? *count_dev : ctl->n_points;
+  uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0, 0, 0};
+  uint32_t flags = 0;
+  const float *cols[3] = {x, y, z};
+  for (uint64_t i = blockIdx.x * uint64_t(BND_THREADS) + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * BND_THREADS) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float v = cols[a][i];
+      if (isnan(v)) {
+        flags |= 1u << a;
+      } else if (isinf(v)) {
+        flags |= 8u << a;
+      } else {
+        const uint32_t o = f2ord(v);
+        mn[a] = min(mn[a], o);
+        mx[a] = max(mx[a], o);
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[a] = min(mn[a], __shfl_xor_sync(FULL_MASK, mn[a], o));
+      mx[a] = max(mx[a], __shfl_xor_sync(FULL_MASK, mx[a], o));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) flags |= __shfl_xor_sync(FULL_MASK, flags, o);
+  __shared__ uint32_t s[BND_THREADS / 32][7];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    for (int a = 0; a < 3; ++a) {
+      s[warp][a] = mn[a];
+      s[warp][3 + a] = mx[a];
+    }
+    s[warp][6] = flags;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < BND_THREADS / 32; ++w) {
+      for (int a = 0; a < 3; ++a) {
+        s[0][a] = min(s[0][a], s[w][a]);
+        s[0][3 + a] = max(s[0][3 + a], s[w][3 + a]);
+      }
+      s[0][6] |= s[w][6];
+    }
+    for (int a = 0; a < 3; ++a) {
+      if (s[0][a] != 0xffffffffu) atomicMin(&ctl->bounds.mn[a], s[0][a]);
+      if (s[0][3 + a] != 0u) atomicMax(&ctl->bounds.mx[a], s[0][3 + a]);
+    }
+    if (s[0][6]) atomicOr(&ctl->bounds.flags, s[0][6]);
+  }
+}
+
+// Builds the voxel-key plan from the bounds (filter_internal, voxel.rs:266-275).
+__global__ void k_voxel_plan(Control *ctl, float leaf, int has_origin, float ox, float oy,
+                             float oz) {
+  if (threadIdx.x != 0 || ld_relaxed_u32(&ctl->status)) return;
+  VoxelPlan pl{};
+  pl.inv_leaf = __fdiv_rn(1.0f, leaf);  // f32 IEEE division, voxel.rs:267
+  pl.floor_mode = has_origin ? 1 : 0;
+  const Bounds b = ctl->bounds;
+  float lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    const bool any = b.mn[a] != 0xffffffffu;
+    lo[a] = any ? ord2f(b.mn[a]) : __int_as_float(0x7fc00000);  // all-NaN axis -> NaN
+    hi[a] = any ? ord2f(b.mx[a]) : __int_as_float(0x7fc00000);
+  }
+  if (has_origin) {
+    pl.origin[0] = ox;
+    pl.origin[1] = oy;
+    pl.origin[2] = oz;
+  } else {
+    for (int a = 0; a < 3; ++a) pl.origin[a] = lo[a];
+  }
+  bool ok = (b.flags & (7u << 3)) == 0;  // an infinite coordinate saturates the key
+  uint32_t total = 0;
+  for (int a = 0; a < 3; ++a) {
+    int64_t k0 = voxel_axis_key(lo[a], pl.origin[a], pl.inv_leaf, pl.floor_mode);
+    int64_t k1 = voxel_axis_key(hi[a], pl.origin[a], pl.inv_leaf, pl.floor_mode);
+    if (isnan(lo[a])) k0 = k1 = 0;
+    if (b.flags & (1u << a)) {  // NaN coordinates get key 0 (saturating cast)
+      k0 = min(k0, int64_t(0));
+      k1 = max(k1, int64_t(0));
+    }
+    pl.kmin[a] = k0;
+    const uint64_t range = uint64_t(k1) - uint64_t(k0);
+    pl.bits[a] = bit_width_u64(range);
+    total += pl.bits[a];
+  }
+  pl.shift_y = pl.bits[2];
+  pl.shift_x = pl.bits[1] + pl.bits[2];
+  pl.total_bits = total;
+  pl.num_digits = total == 0 ? 1u : (total + RADIX_BITS - 1) / RADIX_BITS;
+  if (total > 64) ok = false;
+  if (ctl->n_points > LB_MAX_COUNT) {
+    atomicOr(&ctl->status, ST_TOO_MANY_POINTS);
+    ok = false;
+  }
+  pl.valid = ok ? 1u : 0u;
+  ctl->vplan = pl;
+  if (!ok) atomicOr(&ctl->status, ST_KEY_OVERFLOW);
+}
+
+// Key source for the voxel sort: packs the reference's voxel key of point i.
+struct VoxelKeySrc {
+  const float *x, *y, *z;
+  VoxelPlan pl;
+  __device__ __forceinline__ void prepare(const Control *ctl) { pl = ctl->vplan; }
+  __device__ __forceinline__ uint32_t count(const Control *ctl) const {
+    return uint32_t(ctl->n_points);
+  }
+  __device__ __forceinline__ uint32_t num_digits() const { return pl.num_digits; }
+  __device__ __forceinline__ void load(uint32_t i, uint64_t &k, uint32_t &v) const {
+    k = voxel_pack(pl, x[i], y[i], z[i]);
+    v = i;
+  }
+};
+
+template <int NC>
+struct Columns {
+  const float *in[NC];
+  float *out[NC];
+};
+
+constexpr int SEG_THREADS = 256;
+constexpr int SEG_ITEMS = 8;
+constexpr int SEG_TILE = SEG_THREADS * SEG_ITEMS;  // 2048 sorted positions per tile
+constexpr uint32_t SEG_SHORT = 32;  // longer voxels are reduced by a whole warp
+
+struct SegmentSmem {
+  uint64_t keys[SEG_TILE + 2];  // keys[0] = key before the tile, keys[1 + tile_n] = key after it
+  uint32_t vals[SEG_TILE];
+  uint32_t scratch[SEG_THREADS / 32];
+  uint32_t tile;
+};
+
+template <int NC>
+__device__ __forceinline__ void write_centroid(const Columns<NC> &cols, const double (&s)[NC],
+                                               uint32_t cnt, uint32_t seg, uint64_t key,
+                                               uint64_t *out_keys, uint32_t *out_counts,
+                                               uint32_t n, uint32_t *status) {
+  if (seg >= n) {  // cannot happen for a consistent sort; never write out of bounds
+    atomicOr(status, ST_INTERNAL);
+    return;
+  }
+  // (sum * (1.0 / count)) as f32, voxel.rs:531-536
+  const double inv = 1.0 / double(cnt);
+#pragma unroll
+  for (int c = 0; c < NC; ++c) cols.out[c][seg] = __double2float_rn(__dmul_rn(s[c], inv));
+  out_keys[seg] = key;
+  out_counts[seg] = cnt;
+}
+
+// Fused segment discovery + FP64 centroid reduction over the sorted
+// (key, index) pairs.  Each tile flags voxel starts, numbers them with a
+// block scan plus decoupled look-back, and reduces every voxel that starts in
+// it: one thread per short voxel (sequential FP64 sum in ascending point
+// index, the reference's order, voxel.rs:502-520), one warp per long voxel or
+// per voxel that runs past the tile end.
+template <int NC>
+__global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, SortBuffers sort,
+                                                                 const uint32_t *final_buf,
+                                                                 Columns<NC> cols,
+                                                                 uint64_t *out_keys,
+                                                                 uint32_t *out_counts,
+                                                                 uint64_t *lookback) {
+  __shared__ SegmentSmem sm;
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint32_t n = uint32_t(ctl->n_points);
+  if (n == 0) return;
+  const uint32_t fb = *final_buf;
+  const uint64_t *keys = sort.keys[fb];
+  const uint32_t *vals = sort.vals[fb];
+  const uint32_t epoch = ctl->epoch + EP_VSEG;
+  const uint32_t num_tiles = (n + SEG_TILE - 1) / SEG_TILE;
+  const uint32_t t = threadIdx.x, lane = t & 31u;
+
+  for (;;) {
+    if (t == 0) sm.tile = atomicAdd(&ctl->work[WK_VSEG], 1u);
+    __syncthreads();
+    const uint32_t tile = sm.tile;
+    if (tile >= num_tiles) break;
+    const uint32_t base = tile * SEG_TILE;
+    const uint32_t tile_n = min(uint32_t(SEG_TILE), n - base);
+    for (uint32_t j = t; j < tile_n; j += SEG_THREADS) {
+      sm.keys[1 + j] = keys[base + j];
+      sm.vals[j] = vals[base + j];
+    }
+    if (t == 0) {
+      sm.keys[0] = base > 0 ? keys[base - 1] : ~keys[0];
+      sm.keys[1 + tile_n] = base + tile_n < n ? keys[base + tile_n] : ~keys[n - 1];
+    }
+    __syncthreads();
+
+    const uint32_t j0 = t * SEG_ITEMS;
+    uint32_t flags = 0;
+#pragma unroll
+    for (int i = 0; i < SEG_ITEMS; ++i) {
+      const uint32_t j = j0 + i;
+      if (j < tile_n && sm.keys[1 + j] != sm.keys[j]) flags |= 1u << i;
+    }
+    uint32_t tile_count;
+    const uint32_t local = block_exclusive_sum<SEG_THREADS>(__popc(flags), sm.scratch, &tile_count);
+    uint32_t seg_base = 0;
+    if (t == 0) seg_base = lookback_exclusive(lookback, 1, tile, tile_count, epoch, &ctl->status);
+    if (t == 0) sm.scratch[0] = seg_base;
+    __syncthreads();
+    seg_base = sm.scratch[0];
+    if (t == 0 && tile == num_tiles - 1) ctl->n_voxels = seg_base + tile_count;
+
+    // Short voxels: the owning thread reduces sequentially.  At most one
+    // voxel per thread (its last start) can be long or run past the tile.
+    bool deferred = false;
+    uint32_t def_pos = 0, def_seg = 0;
+    uint32_t seg = seg_base + local;
+    for (int i = 0; i < SEG_ITEMS; ++i) {
+      if (!(flags & (1u << i))) continue;
+      const uint32_t j = j0 + i;
+      const uint64_t key = sm.keys[1 + j];
+      uint32_t e = j + 1;
+      while (e < tile_n && e - j <= SEG_SHORT && sm.keys[1 + e] == key) ++e;
+      const bool closed = sm.keys[1 + e] != key;  // keys[1 + tile_n] is the key after the tile
+      if (closed && e - j <= SEG_SHORT) {
+        double s[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) s[c] = 0.0;
+        for (uint32_t m = j; m < e; ++m) {
+          const uint32_t v = sm.vals[m];
+          if (v >= n) {  // a consistent sort never produces this; never read out of bounds
+            atomicOr(&ctl->status, ST_INTERNAL);
+            continue;
+          }
+#pragma unroll
+          for (int c = 0; c < NC; ++c) s[c] += double(cols.in[c][v]);
+        }
+        write_centroid<NC>(cols, s, e - j, seg, key, out_keys, out_counts, n, &ctl->status);
+      } else {
+        deferred = true;
+        def_pos = base + j;
+        def_seg = seg;
+      }
+      ++seg;
+    }
+    // Long voxels: the whole warp finds the end and reduces.
+    uint32_t pending = __ballot_sync(FULL_MASK, deferred);
+    while (pending) {
+      const uint32_t src_lane = __ffs(pending) - 1;
+      pending &= pending - 1;
+      const uint32_t p = __shfl_sync(FULL_MASK, def_pos, src_lane);
+      const uint32_t sg = __shfl_sync(FULL_MASK, def_seg, src_lane);
+      const uint64_t key = keys[p];
+      uint32_t e = p + 1;
+      for (;;) {
+        const uint32_t idx = e + lane;
+        const bool stop = idx >= n || keys[idx] != key;
+        const uint32_t b = __ballot_sync(FULL_MASK, stop);
+        if (b) {
+          e += __ffs(b) - 1;
+          break;
+        }
+        e += 32;
+      }
+      double s[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) s[c] = 0.0;
+      for (uint32_t m = p + lane; m < e; m += 32) {
+        const uint32_t v = vals[m];
+        if (v >= n) {
+          atomicOr(&ctl->status, ST_INTERNAL);
+          continue;
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) s[c] += double(cols.in[c][v]);
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s[c] += __shfl_xor_sync(FULL_MASK, s[c], o);
+      if (lane == 0) write_centroid<NC>(cols, s, e - p, sg, key, out_keys, out_counts, n, &ctl->status);
+    }
+    __syncthreads();
+  }
+}
+
+// Unpacks packed voxel keys into the reference's (ix, iy, iz) int64 triples.
+__global__ void k_unpack_voxel_keys(const Control *ctl, const uint64_t *packed, int64_t *out) {
+  if (ctl->status) return;
+  const VoxelPlan pl = ctl->vplan;
+  const uint64_t v = ctl->n_voxels;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < v;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    int64_t k[3];
+    voxel_unpack(pl, packed[i], k);
+    out[3 * i] = k[0];
+    out[3 * i + 1] = k[1];
+    out[3 * i + 2] = k[2];
+  }
+}
+
+}  // namespace srcu

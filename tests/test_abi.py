@@ -1,0 +1,90 @@
+"""C ABI checks that need no GPU: libsrcuda.so loads, exports every entry point
+include/srcuda.h declares, and the ctypes mirrors have the C struct layouts."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from spatialrust_b200 import _native
+from spatialrust_b200.csrc import build as csrc_build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "srcuda.h")
+
+
+@pytest.fixture(scope="module")
+def lib():
+    csrc_build.build()
+    return _native.load()
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(srcu_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "srcu_voxel_centroid" in names and "srcu_radius_normals" in names
+    assert len(names) >= 12
+
+
+def test_library_exports_every_declared_symbol(lib):
+    out = subprocess.check_output(["nm", "-D", "--defined-only", _native.library_path()], text=True)
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = [n for n in declared_functions() if n not in exported]
+    assert not missing, f"not exported: {missing}"
+
+
+def test_ctypes_signatures_cover_header(lib):
+    assert set(declared_functions()) == set(_native.SIGNATURES)
+
+
+def test_abi_version(lib):
+    assert lib.srcu_abi_version() == 1
+
+
+def test_struct_layouts_match_c(tmp_path):
+    src = tmp_path / "sizes.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "srcuda.h"\n'
+        "int main(void){\n"
+        'printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(srcu_cloud), sizeof(srcu_voxel_params),'
+        " sizeof(srcu_voxel_out), sizeof(srcu_normal_params), sizeof(srcu_normal_out),"
+        " sizeof(srcu_normal_stats), sizeof(srcu_frame_view));\n"
+        'printf("%zu %zu %zu\\n", offsetof(srcu_cloud, n), offsetof(srcu_normal_params, include_self),'
+        " offsetof(srcu_frame_view, n_attrs));\n"
+        "return 0;}\n")
+    exe = tmp_path / "sizes"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)])
+    lines = subprocess.check_output([str(exe)], text=True).split("\n")
+    sizes = [int(v) for v in lines[0].split()]
+    offs = [int(v) for v in lines[1].split()]
+    assert sizes == [ctypes.sizeof(t) for t in (
+        _native.SrcuCloud, _native.SrcuVoxelParams, _native.SrcuVoxelOut, _native.SrcuNormalParams,
+        _native.SrcuNormalOut, _native.SrcuNormalStats, _native.SrcuFrameView)]
+    assert offs == [_native.SrcuCloud.n.offset, _native.SrcuNormalParams.include_self.offset,
+                    _native.SrcuFrameView.n_attrs.offset]
+
+
+def test_header_compiles_as_c_and_cxx(tmp_path):
+    for comp, ext in (("gcc", "c"), ("g++", "cpp")):
+        src = tmp_path / f"inc.{ext}"
+        src.write_text('#include "srcuda.h"\nint main(void){ return srcu_abi_version() == 1 ? 0 : 1; }\n')
+        subprocess.check_call([comp, "-c", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                               "-o", str(tmp_path / f"inc_{ext}.o"), str(src)])
+
+
+def test_create_without_device_reports_no_device(lib):
+    """On a machine without a B200 the context refuses cleanly (no abort)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    h = ctypes.c_void_p()
+    st = lib.srcu_create(0, 0, ctypes.byref(h))
+    assert st == _native.SRCU_ERR_NO_DEVICE
+    assert not h.value
+    assert lib.srcu_last_error(None) == b"no context"
