@@ -242,7 +242,11 @@ def run_gpu(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     cloud = workload_cloud()
-    stream = torch.cuda.current_stream(dev)
+    # A dedicated stream: the library and the timing events must share it (the
+    # legacy default stream's handle is 0, which srcu_set_stream reads as
+    # "the context's own stream").
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     # one context per leaf so both chains' results stay resident
     ctxs = [_native.Context(local) for _ in LEAVES]
     for c in ctxs:

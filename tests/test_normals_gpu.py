@@ -19,17 +19,26 @@ CURV_TOL = 1e-5
 GAP_MIN = 1e-3
 
 
+def angle_between(a, b):
+    """Angle in radians via atan2(|a x b|, a . b) -- accurate near 0, unlike
+    arccos of a dot product, which turns float32 rounding into ~1e-4 rad."""
+    a = a.astype(np.float64)
+    a = a / np.linalg.norm(a, axis=1, keepdims=True)
+    b = b / np.linalg.norm(b, axis=1, keepdims=True)
+    return np.arctan2(np.linalg.norm(np.cross(a, b), axis=1), np.sum(a * b, axis=1))
+
+
 def angle_errors(gpu, ref, points, viewpoint):
     """Angle between GPU and FP64 normals; sign-free where the viewpoint does
     not decide the sign robustly (or no viewpoint is given)."""
-    dots = np.sum(gpu.astype(np.float64) * ref, axis=1)
+    err = angle_between(gpu, ref)
+    sign_free = np.minimum(err, np.pi - err)
     if viewpoint is None:
-        return np.arccos(np.clip(np.abs(dots), 0, 1))
+        return sign_free
     view = np.asarray(viewpoint, np.float64)[None, :] - points.astype(np.float64)
     cos_view = np.abs(np.sum(ref * view, axis=1)) / np.linalg.norm(view, axis=1)
     ambiguous = cos_view < 1e-3
-    err = np.arccos(np.clip(dots, -1, 1))
-    err[ambiguous] = np.arccos(np.clip(np.abs(dots[ambiguous]), 0, 1))
+    err[ambiguous] = sign_free[ambiguous]
     return err
 
 
@@ -167,14 +176,15 @@ def test_shapes_scene_crop(cuda_ctx):
     # the 5M-point radius workload at full density, cropped to a 12 m cube
     c = synthetic.shapes_scene(5_000_000, seed=2)
     xyz = c.xyz()
-    lo = np.array([44.0, 44.0, 44.0], np.float32)
-    m = np.all((xyz >= lo) & (xyz < lo + 12), axis=1)
-    p = xyz[m]
-    assert p.shape[0] > 5_000
-    rep = {}
-    check_normals(cuda_ctx, p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy(), 0.3,
-                  viewpoint=(50, 50, 150), report=rep)
-    print("shapes crop:", p.shape[0], rep)
+    for centre in xyz[:3]:  # 12 m cubes around three random surface points
+        lo = centre - 6.0
+        m = np.all((xyz >= lo) & (xyz < lo + 12), axis=1)
+        p = xyz[m]
+        assert p.shape[0] > 5_000
+        rep = {}
+        check_normals(cuda_ctx, p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy(), 0.3,
+                      viewpoint=(50, 50, 150), report=rep)
+        print("shapes crop:", p.shape[0], rep)
 
 
 def test_georeferenced_centroid_normals(cuda_ctx):
