@@ -250,6 +250,32 @@ srcu_status srcu_profile_enable(srcu_ctx *ctx, uint64_t timed_kernel_mask);
  * the counters afterwards. */
 int srcu_profile_read(srcu_ctx *ctx, srcu_kernel_stat *out, int max_entries, int reset);
 
+/* ---- allocation-free entry point ------------------------------------------ */
+
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory once they are running: a real-time loop (a ROS 2 executor thread
+ * handling each LiDAR frame) that must not allocate after start-up, or a host
+ * application whose device memory belongs to another allocator that forbids
+ * raw cudaMalloc.  It runs the centroid downsample of srcu_voxel_centroid
+ * without a context and calls no cudaMalloc / cudaFree: its scratch (about
+ * 4.6 MB) is one file-scope __device__ array that every GPU which loads this
+ * library holds until the process exits.
+ *  - At most SRCU_NOALLOC_MAX_POINTS points; larger clouds are rejected with
+ *    SRCU_ERR_INVALID_ARGUMENT.
+ *  - cloud and out must be device pointers (on_device = 1) on the current
+ *    device; cuda_stream (NULL = legacy default stream) must belong to it.
+ *  - The first call on each device performs one-time set-up (the scratch's
+ *    device address and launch attributes); make that first call before any
+ *    stream capture.
+ *  - Every call uses the same scratch array and leaves its contents behind;
+ *    calls that overlap on the GPU (different streams or host threads) race.
+ *  - Synchronous: returns after the outputs are written.  Status codes only;
+ *    no message is recorded. */
+#define SRCU_NOALLOC_MAX_POINTS 131072
+srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud, const srcu_voxel_params *params,
+                                        const srcu_voxel_out *out, uint64_t *out_voxels,
+                                        void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

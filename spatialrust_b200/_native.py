@@ -161,6 +161,9 @@ SIGNATURES = {
                          ctypes.c_int),
     "srcu_chain_info_get": ([_P, ctypes.POINTER(SrcuChainInfo)], ctypes.c_int),
     "srcu_profile_enable": ([_P, ctypes.c_uint64], ctypes.c_int),
+    "srcu_voxel_centroid_noalloc": ([ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuVoxelParams),
+                                     ctypes.POINTER(SrcuVoxelOut), ctypes.POINTER(ctypes.c_uint64),
+                                     _P], ctypes.c_int),
     "srcu_profile_read": ([_P, ctypes.POINTER(SrcuKernelStat), ctypes.c_int, ctypes.c_int],
                           ctypes.c_int),
 }

@@ -1,0 +1,199 @@
+// noalloc.cu -- allocation-free voxel centroid downsample (srcu_voxel_centroid_noalloc).
+//
+// Some callers cannot call cudaMalloc: a real-time loop (for example a ROS 2
+// executor thread handling each LiDAR frame) that must not allocate after
+// start-up, or a host application whose device memory belongs to another
+// allocator that forbids raw allocations.  This entry point runs the same
+// voxel chain as srcu_voxel_centroid, but its scratch -- control block, sort
+// ping-pong buffers, look-back words, packed keys -- lives in one file-scope
+// __device__ array of fixed size, so no call allocates device memory.  The
+// caller passes device-resident input and output columns.
+//
+// Included at the end of srcuda.cu, so it shares that translation unit's
+// kernels; the scratch array and the code that takes its address are here.
+
+#include <mutex>
+
+namespace {
+
+constexpr uint64_t NA_MAX_POINTS = SRCU_NOALLOC_MAX_POINTS;
+constexpr size_t na_align(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t NA_CTL = 0;
+constexpr size_t NA_KEYS0 = NA_CTL + na_align(sizeof(Control));
+constexpr size_t NA_KEYS1 = NA_KEYS0 + na_align(NA_MAX_POINTS * 8);
+constexpr size_t NA_VALS0 = NA_KEYS1 + na_align(NA_MAX_POINTS * 8);
+constexpr size_t NA_VALS1 = NA_VALS0 + na_align(NA_MAX_POINTS * 4);
+constexpr size_t NA_LB_SORT = NA_VALS1 + na_align(NA_MAX_POINTS * 4);
+constexpr size_t NA_LB_SEG =
+    NA_LB_SORT + na_align(((NA_MAX_POINTS + OS_TILE - 1) / OS_TILE) * RADIX_BINS * 8);
+constexpr size_t NA_VKEYS = NA_LB_SEG + na_align(((NA_MAX_POINTS + SEG_TILE - 1) / SEG_TILE) * 8);
+constexpr size_t NA_VCOUNTS = NA_VKEYS + na_align(NA_MAX_POINTS * 8);
+constexpr size_t NA_BYTES = NA_VCOUNTS + na_align(NA_MAX_POINTS * 4);
+constexpr int NA_MAX_DEVICES = 64;
+
+}  // namespace
+
+// The scratch.  Zero at module load on each device (look-back words then
+// carry epoch 0, which no chain uses); every call reuses it and leaves its
+// contents behind.  In host code this name is only a stand-in for the device
+// symbol: its device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+namespace {
+
+struct NoallocDevice {
+  bool ready = false;
+  unsigned char *base = nullptr;  // device address of g_noalloc_scratch on this device
+  int num_sms = 0;
+  int occ_sort = 1;
+  int occ_seg = 1;
+};
+
+NoallocDevice g_noalloc_dev[NA_MAX_DEVICES];
+std::mutex g_noalloc_mu;
+
+// One-time set-up per device, with that device current: the scratch's device
+// address and the launch attributes.  Runs inside the first call on a device.
+srcu_status noalloc_setup(int device, NoallocDevice **out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoallocDevice &d = g_noalloc_dev[device];
+  if (!d.ready) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
+      cudaGetLastError();
+      return SRCU_ERR_CUDA;
+    }
+    if (cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaFuncSetAttribute(k_onesweep<VoxelKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             sizeof(OnesweepSmem)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_sort, k_onesweep<VoxelKeySrc>,
+                                                      OS_THREADS, sizeof(OnesweepSmem)) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_seg, k_voxel_segments<4>, SEG_THREADS,
+                                                      0) != cudaSuccess) {
+      cudaGetLastError();
+      return SRCU_ERR_CUDA;
+    }
+    d.occ_sort = std::max(1, d.occ_sort);
+    d.occ_seg = std::max(1, d.occ_seg);
+    d.base = static_cast<unsigned char *>(p);
+    d.ready = true;
+  }
+  *out = &d;
+  return SRCU_OK;
+}
+
+template <int NC>
+void noalloc_segments(cudaStream_t s, uint32_t grid, Control *ctl, const SortBuffers &sb,
+                      const float **in, float *const *out, uint64_t *vkeys, uint32_t *vcounts) {
+  Columns<NC> cols;
+  for (int c = 0; c < NC; ++c) {
+    cols.in[c] = in[c];
+    cols.out[c] = out[c];
+  }
+  k_voxel_segments<NC><<<grid, SEG_THREADS, 0, s>>>(ctl, sb, &ctl->vsort_final, cols, vkeys,
+                                                     vcounts, sb.lookback + 0);
+}
+
+}  // namespace
+
+extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
+                                                   const srcu_voxel_params *params,
+                                                   const srcu_voxel_out *out, uint64_t *out_voxels,
+                                                   void *cuda_stream) {
+  if (out_voxels) *out_voxels = 0;
+  if (!cloud || !params || !out) return SRCU_ERR_INVALID_ARGUMENT;
+  if (cloud->n > NA_MAX_POINTS) return SRCU_ERR_INVALID_ARGUMENT;  // beyond the scratch size
+  if (cloud->n_attrs > MAX_COLS - 3) return SRCU_ERR_INVALID_ARGUMENT;
+  if (!cloud->on_device || !out->on_device) return SRCU_ERR_INVALID_ARGUMENT;
+  if (params->leaf_size <= 0.0f) return SRCU_ERR_INVALID_ARGUMENT;  // voxel.rs:260-264
+  const uint64_t n = cloud->n;
+  if (n == 0) return SRCU_OK;
+  if (!cloud->x || !cloud->y || !cloud->z || !out->x || !out->y || !out->z)
+    return SRCU_ERR_MISSING_FIELD;
+  for (uint32_t a = 0; a < cloud->n_attrs; ++a)
+    if (!cloud->attrs || !cloud->attrs[a] || !out->attrs || !out->attrs[a])
+      return SRCU_ERR_MISSING_FIELD;
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= NA_MAX_DEVICES) {
+    cudaGetLastError();
+    return SRCU_ERR_NO_DEVICE;
+  }
+  NoallocDevice *dev = nullptr;
+  {
+    const srcu_status st = noalloc_setup(device, &dev);
+    if (st != SRCU_OK) return st;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+  unsigned char *b = dev->base;
+  Control *ctl = reinterpret_cast<Control *>(b + NA_CTL);
+  SortBuffers sb;
+  sb.keys[0] = reinterpret_cast<uint64_t *>(b + NA_KEYS0);
+  sb.keys[1] = reinterpret_cast<uint64_t *>(b + NA_KEYS1);
+  sb.vals[0] = reinterpret_cast<uint32_t *>(b + NA_VALS0);
+  sb.vals[1] = reinterpret_cast<uint32_t *>(b + NA_VALS1);
+  sb.lookback = reinterpret_cast<uint64_t *>(b + NA_LB_SORT);
+  SortBuffers seg = sb;
+  seg.lookback = reinterpret_cast<uint64_t *>(b + NA_LB_SEG);
+  uint64_t *vkeys = reinterpret_cast<uint64_t *>(b + NA_VKEYS);
+  uint32_t *vcounts = out->counts ? out->counts : reinterpret_cast<uint32_t *>(b + NA_VCOUNTS);
+
+  const uint32_t nc = 3 + cloud->n_attrs;
+  const float *in[MAX_COLS] = {cloud->x, cloud->y, cloud->z};
+  float *outc[MAX_COLS] = {out->x, out->y, out->z};
+  for (uint32_t a = 0; a < cloud->n_attrs; ++a) {
+    in[3 + a] = cloud->attrs[a];
+    outc[3 + a] = out->attrs[a];
+  }
+  const uint32_t sms = uint32_t(dev->num_sms);
+  // k_begin zeroes the control block (all but the epoch) on every call.
+  k_begin<<<1, 256, 0, s>>>(ctl, n);
+  k_bounds<<<std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4), sms * 8)),
+             BND_THREADS, 0, s>>>(in[0], in[1], in[2], ctl, nullptr);
+  k_voxel_plan<<<1, 32, 0, s>>>(ctl, params->leaf_size, params->has_origin, params->origin[0],
+                                params->origin[1], params->origin[2]);
+  VoxelKeySrc src;
+  src.x = in[0];
+  src.y = in[1];
+  src.z = in[2];
+  k_digit_hist<VoxelKeySrc>
+      <<<std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, HIST_THREADS * 8), sms * 4)),
+         HIST_THREADS, 0, s>>>(src, ctl, ctl->hist_v);
+  const uint32_t grid_s =
+      std::min<uint32_t>(std::max<uint32_t>(1, ceil_div(n, OS_TILE)), sms * uint32_t(dev->occ_sort));
+  for (int k = 0; k < MAX_DIGITS; ++k)
+    k_onesweep<VoxelKeySrc><<<grid_s, OS_THREADS, sizeof(OnesweepSmem), s>>>(
+        src, ctl, ctl->hist_v, sb, k, EP_VSORT, WK_VSORT, &ctl->vsort_final);
+  const uint32_t grid_g =
+      std::min<uint32_t>(std::max<uint32_t>(1, ceil_div(n, SEG_TILE)), sms * uint32_t(dev->occ_seg));
+  switch (nc) {
+    case 3: noalloc_segments<3>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    case 4: noalloc_segments<4>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    case 5: noalloc_segments<5>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    case 6: noalloc_segments<6>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    case 7: noalloc_segments<7>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    case 8: noalloc_segments<8>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    case 9: noalloc_segments<9>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    case 10: noalloc_segments<10>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    case 11: noalloc_segments<11>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    case 12: noalloc_segments<12>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    default: return SRCU_ERR_INVALID_ARGUMENT;
+  }
+  if (out->keys)
+    k_unpack_voxel_keys<<<std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, 256), sms * 8)), 256,
+                          0, s>>>(ctl, vkeys, out->keys);
+  if (cudaGetLastError() != cudaSuccess) return SRCU_ERR_CUDA;
+  // Read back the status word and V (two words of the control block).
+  uint32_t status = 0;
+  unsigned long long voxels = 0;
+  if (cudaMemcpyAsync(&status, &ctl->status, sizeof(status), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpyAsync(&voxels, &ctl->n_voxels, sizeof(voxels), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaGetLastError();
+    return SRCU_ERR_CUDA;
+  }
+  if (status & ST_TIMEOUT) return SRCU_ERR_TIMEOUT;
+  if (status & ST_KEY_OVERFLOW) return SRCU_ERR_KEY_OVERFLOW;
+  if (status) return SRCU_ERR_CUDA;
+  if (out_voxels) *out_voxels = voxels;
+  return SRCU_OK;
+}

@@ -772,3 +772,6 @@ int srcu_profile_read(srcu_ctx *ctx, srcu_kernel_stat *out, int max_entries, int
 }
 
 }  // extern "C"
+
+// The allocation-free variant of the voxel chain shares this translation unit's kernels.
+#include "noalloc.cu"
