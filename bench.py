@@ -258,7 +258,7 @@ def run_gpu(args):
 
     def step():
         for c, leaf in zip(ctxs, LEAVES):
-            c.voxel_normals_enqueue(dcloud, leaf, None, RADIUS, 3, VIEWPOINT)
+            c.voxel_normals_enqueue(dcloud, leaf, None, RADIUS, 3, VIEWPOINT, count_shell=False)
 
     # warm-up (also sizes every buffer)
     for _ in range(max(args.warmup, 3)):
@@ -380,7 +380,8 @@ def run_e2e(ctx, cloud, args, torch, dev, stream):
                                     ctypes.cast(attr_out, ctypes.c_void_p), 0, counts.data_ptr(), 0)
         nout = _native.SrcuNormalOut(*[c.data_ptr() for c in ncols], ncount.data_ptr(), 0)
         outs.append((vcols, counts, ncols, ncount, vout, nout))
-    params = [(_native._voxel_params(leaf, None), _native._normal_params(RADIUS, 3, VIEWPOINT, False))
+    params = [(_native._voxel_params(leaf, None),
+               _native._normal_params(RADIUS, 3, VIEWPOINT, False, count_shell=False))
               for leaf in LEAVES]
     nv = ctypes.c_uint64(0)
     stats = _native.SrcuNormalStats()

@@ -104,6 +104,8 @@ typedef struct srcu_normal_params {
   int32_t include_self;    /* 0: NormalEstimator CPU semantics (self excluded, NaN when invalid).
                               1: GpuNormalEstimator grid semantics (self included, fewer than
                                  3 points -> (0,0,1), curvature 0; normals_grid.rs:86-197). */
+  int32_t count_shell;     /* 1: count shell points into srcu_normal_stats (a few extra
+                              instructions per candidate); 0: shell_points stays 0 */
 } srcu_normal_params;
 
 typedef struct srcu_normal_out {
@@ -120,7 +122,7 @@ typedef struct srcu_normal_stats {
   uint64_t valid_count;
   uint64_t invalid_count;
   uint64_t shell_points;  /* points with some other point at |d^2 - r^2| <= 1e-6 r^2 */
-  uint64_t fp64_eigensolves; /* covariances whose eigengap sent them to the FP64 Jacobi path */
+  uint64_t fp64_eigensolves; /* near-degenerate covariances recomputed with FP64 moments */
 } srcu_normal_stats;
 
 /* ---- context ------------------------------------------------------------ */

@@ -92,7 +92,7 @@ class SrcuVoxelOut(ctypes.Structure):
 class SrcuNormalParams(ctypes.Structure):
     _fields_ = [("radius", ctypes.c_float), ("min_neighbors", ctypes.c_uint32),
                 ("has_viewpoint", ctypes.c_int32), ("viewpoint", c_float3),
-                ("include_self", ctypes.c_int32)]
+                ("include_self", ctypes.c_int32), ("count_shell", ctypes.c_int32)]
 
 
 class SrcuNormalOut(ctypes.Structure):
@@ -397,9 +397,10 @@ class Context:
     # ---- device-resident chain -------------------------------------------
 
     def voxel_normals_enqueue(self, cloud: SrcuCloud, leaf: float, origin, radius: float,
-                              min_neighbors: int = 3, viewpoint=None, include_self: bool = False):
+                              min_neighbors: int = 3, viewpoint=None, include_self: bool = False,
+                              count_shell: bool = True):
         vp = _voxel_params(leaf, origin)
-        np_ = _normal_params(radius, min_neighbors, viewpoint, include_self)
+        np_ = _normal_params(radius, min_neighbors, viewpoint, include_self, count_shell)
         self._check(self._lib.srcu_voxel_normals_enqueue(self._h, ctypes.byref(cloud),
                                                          ctypes.byref(vp), ctypes.byref(np_)))
 
@@ -442,10 +443,11 @@ def _voxel_params(leaf, origin) -> SrcuVoxelParams:
     return SrcuVoxelParams(float(leaf), 1, c_float3(*o))
 
 
-def _normal_params(radius, min_neighbors, viewpoint, include_self) -> SrcuNormalParams:
+def _normal_params(radius, min_neighbors, viewpoint, include_self,
+                   count_shell=True) -> SrcuNormalParams:
     vp = c_float3(*(float(v) for v in viewpoint)) if viewpoint is not None else c_float3(0, 0, 0)
     return SrcuNormalParams(float(radius), int(min_neighbors), int(viewpoint is not None), vp,
-                            int(bool(include_self)))
+                            int(bool(include_self)), int(bool(count_shell)))
 
 
 def _stats(s: SrcuNormalStats) -> dict:

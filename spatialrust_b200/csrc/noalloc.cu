@@ -68,8 +68,9 @@ srcu_status noalloc_setup(int device, NoallocDevice **out) {
                              sizeof(OnesweepSmem)) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_sort, k_onesweep<VoxelKeySrc>,
                                                       OS_THREADS, sizeof(OnesweepSmem)) != cudaSuccess ||
+        configure_segment_kernels() != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_seg, k_voxel_segments<4>, SEG_THREADS,
-                                                      0) != cudaSuccess) {
+                                                      segment_smem_bytes(4)) != cudaSuccess) {
       cudaGetLastError();
       return SRCU_ERR_CUDA;
     }
@@ -90,8 +91,8 @@ void noalloc_segments(cudaStream_t s, uint32_t grid, Control *ctl, const SortBuf
     cols.in[c] = in[c];
     cols.out[c] = out[c];
   }
-  k_voxel_segments<NC><<<grid, SEG_THREADS, 0, s>>>(ctl, sb, &ctl->vsort_final, cols, vkeys,
-                                                     vcounts, sb.lookback + 0);
+  k_voxel_segments<NC><<<grid, SEG_THREADS, segment_smem_bytes(NC), s>>>(
+      ctl, sb, &ctl->vsort_final, cols, vkeys, vcounts, sb.lookback + 0, nullptr, nullptr);
 }
 
 }  // namespace
@@ -148,7 +149,7 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
   // k_begin zeroes the control block (all but the epoch) on every call.
   k_begin<<<1, 256, 0, s>>>(ctl, n);
   k_bounds<<<std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4), sms * 8)),
-             BND_THREADS, 0, s>>>(in[0], in[1], in[2], ctl, nullptr);
+             BND_THREADS, 0, s>>>(in[0], in[1], in[2], ctl, nullptr, nullptr, nullptr);
   k_voxel_plan<<<1, 32, 0, s>>>(ctl, params->leaf_size, params->has_origin, params->origin[0],
                                 params->origin[1], params->origin[2]);
   VoxelKeySrc src;

@@ -89,15 +89,15 @@ struct CellSmem {
 };
 
 // Cell table: gathers points into cell-sorted float4 records
-// (x, y, z, bits of the original index) and numbers the occupied cells
-// (start offsets in the sorted order, cell keys).  cell_start[U] = n.
+// (x, y, z, bits of the original index), numbers the occupied cells (start
+// offsets in the sorted order, cell keys; cell_start[U] = n) and records each
+// sorted point's cell number.
 __global__ void __launch_bounds__(CELL_THREADS) k_cells(Control *ctl, SortBuffers sort,
                                                         const uint32_t *final_buf,
                                                         const unsigned long long *count_dev,
-                                                        const float *x, const float *y,
-                                                        const float *z, float4 *pts,
-                                                        uint64_t *cell_key, uint32_t *cell_start,
-                                                        uint64_t *lookback) {
+                                                        const float4 *aos, float4 *pts,
+                                                        uint32_t *pt_cell, uint64_t *cell_key,
+                                                        uint32_t *cell_start, uint64_t *lookback) {
   __shared__ CellSmem sm;
   if (ld_relaxed_u32(&ctl->status)) return;
   const uint32_t n = uint32_t(count_dev ? *count_dev : ctl->n_points);
@@ -125,7 +125,8 @@ __global__ void __launch_bounds__(CELL_THREADS) k_cells(Control *ctl, SortBuffer
       sm.keys[1 + j] = keys[base + j];
       const uint32_t v = vals[base + j];
       if (v < n) {
-        pts[base + j] = make_float4(x[v], y[v], z[v], __uint_as_float(v));
+        const float4 p = aos[v];
+        pts[base + j] = make_float4(p.x, p.y, p.z, __uint_as_float(v));
       } else {  // a consistent sort never produces this; never read out of bounds
         pts[base + j] = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, __uint_as_float(0u));
         atomicOr(&ctl->status, ST_INTERNAL);
@@ -148,15 +149,17 @@ __global__ void __launch_bounds__(CELL_THREADS) k_cells(Control *ctl, SortBuffer
     uint32_t c = cbase + local;
 #pragma unroll
     for (int i = 0; i < CELL_ITEMS; ++i) {
+      const uint32_t j = j0 + i;
       if (flags & (1u << i)) {
         if (c < n) {
-          cell_key[c] = sm.keys[1 + j0 + i];
-          cell_start[c] = base + j0 + i;
+          cell_key[c] = sm.keys[1 + j];
+          cell_start[c] = base + j;
         } else {
           atomicOr(&ctl->status, ST_INTERNAL);
         }
         ++c;
       }
+      if (j < tile_n) pt_cell[base + j] = c - 1;  // the cell this point belongs to
     }
     if (t == 0 && tile == num_tiles - 1) {
       const uint32_t u_total = min(cbase + tile_count, n);
@@ -258,179 +261,194 @@ struct NormalParamsDev {
   uint32_t min_neighbors;
   int32_t include_self;
   int32_t has_viewpoint;
+  int32_t count_shell;  // report points with a candidate on the radius shell
   float vp[3];
 };
 
-constexpr int NM_WARPS = 8;
-constexpr int NM_THREADS = NM_WARPS * 32;
-constexpr int NM_CAP = 512;  // staged candidate records per warp
-constexpr int NM_FLUSH = 32; // f32 partial moments are folded into FP64 every NM_FLUSH candidates
+constexpr int NM_THREADS = 256;
+constexpr int NM_FLUSH = 32;  // f32 partial moments are folded into FP64 every NM_FLUSH candidates
+constexpr double NM_REFINE_GAP = 0.05;  // (l1 - l0) / trace below this -> FP64 moments
 
-struct NormalSmem {
-  float4 cand[NM_WARPS][NM_CAP];
-};
+// Covariance from moments about the query (S: sx sy sz sxx syy szz sxy sxz syz
+// over n points) and its smallest eigenpair, FP64.
+__device__ __forceinline__ Eig3 eig_from_moments(const double (&S)[9], uint32_t n) {
+  const double inv = 1.0 / double(n);
+  const double mx = S[0] * inv, my = S[1] * inv, mz = S[2] * inv;
+  const double cxx = S[3] * inv - mx * mx, cyy = S[4] * inv - my * my;
+  const double czz = S[5] * inv - mz * mz, cxy = S[6] * inv - mx * my;
+  const double cxz = S[7] * inv - mx * mz, cyz = S[8] * inv - my * mz;
+  return smallest_eigenpair(cxx, cyy, czz, cxy, cxz, cyz);
+}
 
-// Radius normals, one warp per occupied cell (dynamic scheduling).  The
-// cell's points are processed in batches of <= 32 queries; the batch's
-// candidates (the 9 column ranges) are staged in shared memory and each
-// candidate is broadcast to the lanes.  With q queries in a batch, lanes are
-// split into 32/q' groups (q' = q rounded up to a power of two) that walk
-// disjoint candidate subsets, so every lane does useful work even for sparse
-// cells; the groups' moments are combined with shuffles.
+// The same neighbour set (the f32 predicate), with every moment term formed
+// and summed in FP64 -- used for near-degenerate covariances only.
+__device__ __noinline__ void moments_fp64(const float4 *pts, const uint2 *rg, float4 qp, float r2,
+                                          double (&S)[9]) {
+#pragma unroll
+  for (int k = 0; k < 9; ++k) S[k] = 0.0;
+  for (int r = 0; r < 9; ++r) {
+    const uint2 range = rg[r];
+    for (uint32_t j = range.x; j < range.y; ++j) {
+      const float4 c = __ldg(pts + j);
+      const float fx = __fsub_rn(c.x, qp.x), fy = __fsub_rn(c.y, qp.y), fz = __fsub_rn(c.z, qp.z);
+      const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)), __fmul_rn(fz, fz));
+      if (!(d2 <= r2)) continue;
+      const double dx = double(c.x) - double(qp.x);
+      const double dy = double(c.y) - double(qp.y);
+      const double dz = double(c.z) - double(qp.z);
+      S[0] += dx;
+      S[1] += dy;
+      S[2] += dz;
+      S[3] += dx * dx;
+      S[4] += dy * dy;
+      S[5] += dz * dz;
+      S[6] += dx * dy;
+      S[7] += dx * dz;
+      S[8] += dy * dz;
+    }
+  }
+}
+
+// Radius normals.  One warp per 32 consecutive cell-sorted points, one query
+// per lane.  Each lane walks the 9 column ranges of its own cell (the 27-cell
+// neighbourhood) and reads candidates through L1: lanes of the same cell read
+// the same record at the same step, so loads are broadcasts, and the
+// eigensolve runs on all 32 lanes.
+//
+// The query is a candidate of itself with d = p - q = 0 exactly, so it is
+// counted and removed afterwards (hits - 1) instead of being compared by
+// index in the loop; duplicates of the query stay neighbours, as in the
+// reference (normal.rs:381-386).
 //
 // Moments are taken about the query point (d = p - q, the predicate's own
 // differences): count, sum d, sum d d^T, accumulated in f32 for NM_FLUSH
-// candidates and then folded into FP64; the covariance
-// C = S2/n - (S1/n)(S1/n)^T and its eigensolve are FP64.
-__global__ void __launch_bounds__(NM_THREADS) k_normals(Control *ctl, const float4 *pts,
-                                                        const uint32_t *cell_start,
-                                                        const uint2 *ranges, NormalParamsDev prm,
-                                                        const unsigned long long *count_dev,
-                                                        float *nx, float *ny, float *nz,
-                                                        float *curv, uint32_t *counts) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  NormalSmem &sm = *reinterpret_cast<NormalSmem *>(smem_raw);
+// candidates and then folded into FP64; C = S2/n - (S1/n)(S1/n)^T and its
+// eigensolve are FP64.
+__global__ void __launch_bounds__(NM_THREADS, 3) k_normals(Control *ctl, const float4 *pts,
+                                                           const uint32_t *pt_cell,
+                                                           const uint2 *ranges, NormalParamsDev prm,
+                                                           const unsigned long long *count_dev,
+                                                           float *nx, float *ny, float *nz,
+                                                           float *curv, uint32_t *counts) {
   if (ld_relaxed_u32(&ctl->status)) return;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t n = uint32_t(count_dev ? *count_dev : ctl->n_points);
   const uint64_t u_count = ctl->n_cells;
-  const uint32_t n_pts = uint32_t(count_dev ? *count_dev : ctl->n_points);
   const float r2 = ctl->cplan.r2;
   const float shell_tol = ctl->cplan.shell_tol;
-  float4 *buf = sm.cand[warp];
+  const uint32_t batches = (n + 31) / 32;
+  const uint32_t warps = gridDim.x * (NM_THREADS / 32);
   unsigned long long n_valid = 0, n_invalid = 0, n_shell = 0, n_fp64 = 0;
 
-  for (;;) {
-    uint32_t u = 0;
-    if (lane == 0) u = atomicAdd(&ctl->work[WK_NORMALS], 1u);
-    u = __shfl_sync(FULL_MASK, u, 0);
-    if (u >= u_count) break;
-    // the 9 column ranges and their prefix offsets
-    uint2 rg = lane < 9 ? ranges[size_t(u) * 9 + lane] : make_uint2(0, 0);
-    const uint32_t len = rg.y - rg.x;
-    uint32_t total;
-    const uint32_t excl = warp_exclusive_sum(len, &total);
-    const uint32_t q_begin = cell_start[u], q_end = cell_start[u + 1];
-
-    for (uint32_t b0 = q_begin; b0 < q_end; b0 += 32) {
-      const uint32_t q = min(32u, q_end - b0);
-      uint32_t qpad_log = 0;
-      while ((1u << qpad_log) < q) ++qpad_log;
-      const uint32_t qpad = 1u << qpad_log;
-      const uint32_t my_q = lane & (qpad - 1);
-      const uint32_t my_g = lane >> qpad_log;
-      const uint32_t groups = 32u >> qpad_log;
-      const float4 qp = pts[b0 + min(my_q, q - 1)];
-      const uint32_t qidx = __float_as_uint(qp.w);
-
-      uint32_t cnt = 0, shell = 0;
-      double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // sx sy sz sxx syy szz sxy sxz syz
-      float F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      uint32_t since_flush = 0;
-
-      for (uint32_t c0 = 0; c0 < total; c0 += NM_CAP) {
-        const uint32_t clen = min(uint32_t(NM_CAP), total - c0);
-        // stage candidates [c0, c0 + clen) of the concatenated ranges
-        for (int r = 0; r < 9; ++r) {
-          const uint32_t rs = __shfl_sync(FULL_MASK, rg.x, r);
-          const uint32_t re = __shfl_sync(FULL_MASK, excl, r);
-          const uint32_t rl = __shfl_sync(FULL_MASK, len, r);
-          const uint32_t lo = max(re, c0), hi = min(re + rl, c0 + clen);
-          for (uint32_t p = lo + lane; p < hi; p += 32) buf[p - c0] = pts[rs + (p - re)];
+  for (uint32_t b = blockIdx.x * (NM_THREADS / 32) + (threadIdx.x >> 5); b < batches; b += warps) {
+    const uint32_t i = b * 32 + lane;
+    const bool active = i < n;
+    const uint32_t ii = active ? i : n - 1;
+    const float4 qp = pts[ii];
+    const uint32_t u = pt_cell[ii];
+    if (u >= u_count) {  // cannot happen for a consistent cell table
+      atomicOr(&ctl->status, ST_INTERNAL);
+      continue;
+    }
+    const uint2 *rg = ranges + size_t(u) * 9;
+    float hits = 0.f;
+    uint32_t shell = 0;
+    double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // sx sy sz sxx syy szz sxy sxz syz
+    float F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t since = 0;
+#pragma unroll 1
+    for (int r = 0; r < 9; ++r) {
+      const uint2 range = rg[r];
+      for (uint32_t j = range.x; j < range.y; ++j) {
+        const float4 c = __ldg(pts + j);
+        const float dx = __fsub_rn(c.x, qp.x);
+        const float dy = __fsub_rn(c.y, qp.y);
+        const float dz = __fsub_rn(c.z, qp.z);
+        const float xx = __fmul_rn(dx, dx), yy = __fmul_rn(dy, dy), zz = __fmul_rn(dz, dz);
+        const float d2 = __fadd_rn(__fadd_rn(xx, yy), zz);
+        if (d2 <= r2) {
+          hits += 1.f;
+          F[0] += dx;
+          F[1] += dy;
+          F[2] += dz;
+          F[3] += xx;
+          F[4] += yy;
+          F[5] += zz;
+          F[6] = fmaf(dx, dy, F[6]);
+          F[7] = fmaf(dx, dz, F[7]);
+          F[8] = fmaf(dy, dz, F[8]);
         }
-        __syncwarp();
-        for (uint32_t j = my_g; j < clen; j += groups) {
-          const float4 c = buf[j];
-          const float dx = __fsub_rn(c.x, qp.x);
-          const float dy = __fsub_rn(c.y, qp.y);
-          const float dz = __fsub_rn(c.z, qp.z);
-          const float xx = __fmul_rn(dx, dx), yy = __fmul_rn(dy, dy), zz = __fmul_rn(dz, dz);
-          const float d2 = __fadd_rn(__fadd_rn(xx, yy), zz);
-          const bool other = __float_as_uint(c.w) != qidx;
-          const bool hit = (d2 <= r2) && other;
-          if (other && fabsf(__fsub_rn(d2, r2)) <= shell_tol) shell = 1;
-          if (hit) {
-            ++cnt;
-            F[0] += dx;
-            F[1] += dy;
-            F[2] += dz;
-            F[3] += xx;
-            F[4] += yy;
-            F[5] += zz;
-            F[6] = fmaf(dx, dy, F[6]);
-            F[7] = fmaf(dx, dz, F[7]);
-            F[8] = fmaf(dy, dz, F[8]);
-          }
-          if (++since_flush == NM_FLUSH) {
-            since_flush = 0;
+        if (prm.count_shell && d2 != 0.f && fabsf(__fsub_rn(d2, r2)) <= shell_tol) shell = 1;
+        if (++since == NM_FLUSH) {
+          since = 0;
 #pragma unroll
-            for (int k = 0; k < 9; ++k) {
-              S[k] += double(F[k]);
-              F[k] = 0.f;
-            }
+          for (int k = 0; k < 9; ++k) {
+            S[k] += double(F[k]);
+            F[k] = 0.f;
           }
         }
-        __syncwarp();
-      }
-#pragma unroll
-      for (int k = 0; k < 9; ++k) S[k] += double(F[k]);
-      // combine the lane groups that share a query
-      for (uint32_t o = qpad; o < 32; o <<= 1) {
-        cnt += __shfl_xor_sync(FULL_MASK, cnt, o);
-        shell |= __shfl_xor_sync(FULL_MASK, shell, o);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) S[k] += __shfl_xor_sync(FULL_MASK, S[k], o);
-      }
-      if (my_g == 0 && my_q < q) {
-        const uint32_t n_eff = prm.include_self ? cnt + 1 : cnt;
-        const bool valid = prm.include_self ? (n_eff >= 3) : (cnt >= prm.min_neighbors && cnt > 0);
-        float ox, oy, oz, oc;
-        if (valid) {
-          const double inv = 1.0 / double(n_eff);
-          const double mx = S[0] * inv, my = S[1] * inv, mz = S[2] * inv;
-          const double cxx = S[3] * inv - mx * mx, cyy = S[4] * inv - my * my;
-          const double czz = S[5] * inv - mz * mz, cxy = S[6] * inv - mx * my;
-          const double cxz = S[7] * inv - mx * mz, cyz = S[8] * inv - my * mz;
-          const Eig3 e = smallest_eigenpair(cxx, cyy, czz, cxy, cxz, cyz);
-          double v0 = e.v[0], v1 = e.v[1], v2 = e.v[2];
-          if (prm.has_viewpoint) {
-            // orient_normal_towards_viewpoint, normal.rs:408-421
-            const double wx = double(prm.vp[0]) - double(qp.x);
-            const double wy = double(prm.vp[1]) - double(qp.y);
-            const double wz = double(prm.vp[2]) - double(qp.z);
-            if (v0 * wx + v1 * wy + v2 * wz < 0.0) {
-              v0 = -v0;
-              v1 = -v1;
-              v2 = -v2;
-            }
-          }
-          const double nn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-          ox = float(v0 / nn);
-          oy = float(v1 / nn);
-          oz = float(v2 / nn);
-          const double sum = e.l0 + e.l1 + e.l2;
-          oc = sum > 0.0 ? float(e.l0 / sum) : 0.0f;
-          ++n_valid;
-          n_fp64 += e.jacobi ? 1 : 0;
-        } else {
-          const float nanv = __int_as_float(0x7fc00000);
-          ox = prm.include_self ? 0.0f : nanv;
-          oy = prm.include_self ? 0.0f : nanv;
-          oz = prm.include_self ? 1.0f : nanv;
-          oc = 0.0f;
-          ++n_invalid;
-        }
-        n_shell += shell;
-        if (qidx >= n_pts) {  // cannot happen: records carry indices < n
-          atomicOr(&ctl->status, ST_INTERNAL);
-          continue;
-        }
-        nx[qidx] = ox;
-        ny[qidx] = oy;
-        nz[qidx] = oz;
-        curv[qidx] = oc;
-        if (counts) counts[qidx] = prm.include_self ? n_eff : cnt;
       }
     }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) S[k] += double(F[k]);
+    if (!active) continue;
+    // hits includes the query itself exactly once when it is finite.
+    const bool finite = isfinite(qp.x) && isfinite(qp.y) && isfinite(qp.z);
+    const uint32_t h = uint32_t(hits);
+    const uint32_t cnt = (finite && h > 0) ? h - 1 : 0;
+    const uint32_t n_eff = prm.include_self ? cnt + (finite ? 1 : 0) : cnt;
+    const bool valid = prm.include_self ? (n_eff >= 3) : (cnt >= prm.min_neighbors && cnt > 0);
+    float ox, oy, oz, oc;
+    if (valid) {
+      Eig3 e = eig_from_moments(S, n_eff);
+      // The f32 moments carry ~1e-7 r^2 of rounding; when the gap to the
+      // second eigenvalue is under NM_REFINE_GAP of the trace that rounding
+      // can tilt the normal by more than 1e-5 rad, so this point's moments
+      // are recomputed with FP64 products (same neighbour set) and re-solved.
+      const double trace = e.l0 + e.l1 + e.l2;
+      if (!(e.l1 - e.l0 >= NM_REFINE_GAP * trace)) {
+        moments_fp64(pts, rg, qp, r2, S);
+        e = eig_from_moments(S, n_eff);
+        ++n_fp64;
+      }
+      double v0 = e.v[0], v1 = e.v[1], v2 = e.v[2];
+      if (prm.has_viewpoint) {
+        // orient_normal_towards_viewpoint, normal.rs:408-421
+        const double wx = double(prm.vp[0]) - double(qp.x);
+        const double wy = double(prm.vp[1]) - double(qp.y);
+        const double wz = double(prm.vp[2]) - double(qp.z);
+        if (v0 * wx + v1 * wy + v2 * wz < 0.0) {
+          v0 = -v0;
+          v1 = -v1;
+          v2 = -v2;
+        }
+      }
+      const double nn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+      ox = float(v0 / nn);
+      oy = float(v1 / nn);
+      oz = float(v2 / nn);
+      const double sum = e.l0 + e.l1 + e.l2;
+      oc = sum > 0.0 ? float(e.l0 / sum) : 0.0f;
+      ++n_valid;
+    } else {
+      const float nanv = __int_as_float(0x7fc00000);
+      ox = prm.include_self ? 0.0f : nanv;
+      oy = prm.include_self ? 0.0f : nanv;
+      oz = prm.include_self ? 1.0f : nanv;
+      oc = 0.0f;
+      ++n_invalid;
+    }
+    n_shell += shell;
+    const uint32_t qidx = __float_as_uint(qp.w);
+    if (qidx >= n) {  // cannot happen: records carry indices < n
+      atomicOr(&ctl->status, ST_INTERNAL);
+      continue;
+    }
+    nx[qidx] = ox;
+    ny[qidx] = oy;
+    nz[qidx] = oz;
+    curv[qidx] = oc;
+    if (counts) counts[qidx] = prm.include_self ? n_eff : cnt;
   }
   // one atomic per warp for the counters
 #pragma unroll

@@ -40,9 +40,10 @@ struct srcu_ctx {
   // sort
   DevBuf keys[2], vals[2], lb_sort, lb_seg, lb_cells;
   // voxel outputs: x, y, z, attrs..., packed keys, counts, unpacked keys
-  DevBuf vout[MAX_COLS], vkeys, vcounts, vkeys3;
+  DevBuf vout[MAX_COLS], vkeys, vcounts, vkeys3, vaos;
+  DevBuf in_aos;  // AoS (x, y, z, first attribute) copy of the chain's input
   // radius grid
-  DevBuf pts, cell_key, cell_start, table, ranges;
+  DevBuf pts, pt_cell, cell_key, cell_start, table, ranges;
   uint32_t table_log2 = 0;
   // normals outputs
   DevBuf nout[4], ncounts;
@@ -200,7 +201,9 @@ srcu_status reserve(srcu_ctx *ctx, uint64_t n, uint32_t cols, bool host_input, b
   ST_TRY(ensure(ctx, ctx->vals[0], m * 4));
   ST_TRY(ensure(ctx, ctx->vals[1], m * 4));
   ST_TRY(ensure(ctx, ctx->lb_sort, size_t(ceil_div(m, OS_TILE)) * RADIX_BINS * 8, true));
+  ST_TRY(ensure(ctx, ctx->in_aos, m * 16));
   if (voxel) {
+    ST_TRY(ensure(ctx, ctx->vaos, m * 16));
     ST_TRY(ensure(ctx, ctx->lb_seg, size_t(ceil_div(m, SEG_TILE)) * 8, true));
     for (uint32_t c = 0; c < cols; ++c) ST_TRY(ensure(ctx, ctx->vout[c], m * 4));
     ST_TRY(ensure(ctx, ctx->vkeys, m * 8));
@@ -209,6 +212,7 @@ srcu_status reserve(srcu_ctx *ctx, uint64_t n, uint32_t cols, bool host_input, b
   if (normals) {
     ST_TRY(ensure(ctx, ctx->lb_cells, size_t(ceil_div(m, CELL_TILE)) * 8, true));
     ST_TRY(ensure(ctx, ctx->pts, m * 16));
+    ST_TRY(ensure(ctx, ctx->pt_cell, m * 4));
     ST_TRY(ensure(ctx, ctx->cell_key, m * 8));
     ST_TRY(ensure(ctx, ctx->cell_start, (m + 1) * 4));
     ST_TRY(ensure(ctx, ctx->ranges, m * 9 * sizeof(uint2)));
@@ -282,9 +286,10 @@ void launch_segments_nc(srcu_ctx *ctx, const float **in, uint32_t grid) {
     cols.in[c] = in[c];
     cols.out[c] = ptr<float>(ctx->vout[c]);
   }
-  k_voxel_segments<NC><<<grid, SEG_THREADS, 0, ctx->stream>>>(
+  k_voxel_segments<NC><<<grid, SEG_THREADS, segment_smem_bytes(NC), ctx->stream>>>(
       ctx->ctl, sort_buffers(ctx), &ctx->ctl->vsort_final, cols, ptr<uint64_t>(ctx->vkeys),
-      ptr<uint32_t>(ctx->vcounts), ptr<uint64_t>(ctx->lb_seg));
+      ptr<uint32_t>(ctx->vcounts), ptr<uint64_t>(ctx->lb_seg), ptr<const float4>(ctx->in_aos),
+      ptr<float4>(ctx->vaos));
 }
 
 // Voxel stage: bounds -> plan -> sort -> fused segment/centroid reduction.
@@ -294,7 +299,9 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
                                                                     uint32_t(ctx->num_sms) * 8));
   {
     Launch l(ctx, SRCU_K_BOUNDS);
-    k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(in[0], in[1], in[2], ctx->ctl, nullptr);
+    k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(in[0], in[1], in[2], ctx->ctl, nullptr,
+                                                       nc > 3 ? in[3] : nullptr,
+                                                       ptr<float4>(ctx->in_aos));
   }
   {
     Launch l(ctx, SRCU_K_VOXEL_PLAN);
@@ -330,7 +337,7 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
 // Normals stage over (x, y, z) with the point count in *count_dev (device)
 // or ctl->n_points when count_dev is null; n_max bounds the grid sizes.
 srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const float *z,
-                            const unsigned long long *count_dev, uint64_t n_max,
+                            const float4 *aos, const unsigned long long *count_dev, uint64_t n_max,
                             const srcu_normal_params *np) {
   {
     Launch l(ctx, SRCU_K_CELL_PLAN);
@@ -349,9 +356,9 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
   {
     Launch l(ctx, SRCU_K_CELLS);
     k_cells<<<grid_c, CELL_THREADS, 0, ctx->stream>>>(
-        ctx->ctl, sort_buffers(ctx), &ctx->ctl->csort_final, count_dev, x, y, z,
-        ptr<float4>(ctx->pts), ptr<uint64_t>(ctx->cell_key), ptr<uint32_t>(ctx->cell_start),
-        ptr<uint64_t>(ctx->lb_cells));
+        ctx->ctl, sort_buffers(ctx), &ctx->ctl->csort_final, count_dev, aos,
+        ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint64_t>(ctx->cell_key),
+        ptr<uint32_t>(ctx->cell_start), ptr<uint64_t>(ctx->lb_cells));
   }
   const uint32_t grid_g = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n_max, 256),
                                                                     uint32_t(ctx->num_sms) * 8));
@@ -373,13 +380,14 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
   prm.min_neighbors = np->min_neighbors;
   prm.include_self = np->include_self;
   prm.has_viewpoint = np->has_viewpoint;
+  prm.count_shell = np->count_shell;
   prm.vp[0] = np->viewpoint[0];
   prm.vp[1] = np->viewpoint[1];
   prm.vp[2] = np->viewpoint[2];
   const uint32_t grid_n = uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals);
   Launch l(ctx, SRCU_K_NORMALS);
-  k_normals<<<grid_n, NM_THREADS, sizeof(NormalSmem), ctx->stream>>>(
-      ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->cell_start), ptr<uint2>(ctx->ranges),
+  k_normals<<<grid_n, NM_THREADS, 0, ctx->stream>>>(
+      ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint2>(ctx->ranges),
       prm, count_dev, ptr<float>(ctx->nout[0]), ptr<float>(ctx->nout[1]), ptr<float>(ctx->nout[2]),
       ptr<float>(ctx->nout[3]), ptr<uint32_t>(ctx->ncounts));
   CU_TRY(cudaGetLastError());
@@ -512,16 +520,16 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
                            sizeof(OnesweepSmem)) != cudaSuccess ||
       cudaFuncSetAttribute(k_onesweep<CellKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            sizeof(OnesweepSmem)) != cudaSuccess ||
-      cudaFuncSetAttribute(k_normals, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           sizeof(NormalSmem)) != cudaSuccess)
+      false)
     return bail(SRCU_ERR_CUDA);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_v, k_onesweep<VoxelKeySrc>,
                                                 OS_THREADS, sizeof(OnesweepSmem));
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_c, k_onesweep<CellKeySrc>,
                                                 OS_THREADS, sizeof(OnesweepSmem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals, k_normals, NM_THREADS,
-                                                sizeof(NormalSmem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_seg, k_voxel_segments<4>, SEG_THREADS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals, k_normals, NM_THREADS, 0);
+  if (configure_segment_kernels() != cudaSuccess) return bail(SRCU_ERR_CUDA);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_seg, k_voxel_segments<4>, SEG_THREADS,
+                                                segment_smem_bytes(4));
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_cells, k_cells, CELL_THREADS, 0);
   ctx->occ_onesweep_v = std::max(1, ctx->occ_onesweep_v);
   ctx->occ_onesweep_c = std::max(1, ctx->occ_onesweep_c);
@@ -537,9 +545,9 @@ void srcu_destroy(srcu_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  DevBuf *all[] = {&ctx->keys[0], &ctx->keys[1], &ctx->vals[0], &ctx->vals[1], &ctx->lb_sort,
+  DevBuf *all[] = {&ctx->in_aos, &ctx->vaos, &ctx->keys[0], &ctx->keys[1], &ctx->vals[0], &ctx->vals[1], &ctx->lb_sort,
                    &ctx->lb_seg, &ctx->lb_cells, &ctx->vkeys, &ctx->vcounts, &ctx->vkeys3,
-                   &ctx->pts, &ctx->cell_key, &ctx->cell_start, &ctx->table, &ctx->ranges,
+                   &ctx->pts, &ctx->pt_cell, &ctx->cell_key, &ctx->cell_start, &ctx->table, &ctx->ranges,
                    &ctx->ncounts};
   for (DevBuf *b : all) release(ctx, *b);
   for (auto &b : ctx->in) release(ctx, b);
@@ -614,9 +622,11 @@ srcu_status srcu_radius_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
                                                                     uint32_t(ctx->num_sms) * 8));
   {
     Launch l(ctx, SRCU_K_BOUNDS);
-    k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(cols[0], cols[1], cols[2], ctx->ctl, nullptr);
+    k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(cols[0], cols[1], cols[2], ctx->ctl, nullptr,
+                                                       nullptr, ptr<float4>(ctx->in_aos));
   }
-  ST_TRY(enqueue_normals(ctx, cols[0], cols[1], cols[2], nullptr, n, params));
+  ST_TRY(enqueue_normals(ctx, cols[0], cols[1], cols[2], ptr<const float4>(ctx->in_aos), nullptr, n,
+                         params));
   ST_TRY(read_control(ctx));
   ST_TRY(fetch_normals(ctx, out, n, stats));
   CU_TRY(cudaStreamSynchronize(ctx->stream));
@@ -645,7 +655,8 @@ srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
   ST_TRY(enqueue_voxel(ctx, cols, nc, n, vparams));
   // Normals on the centroids (mvp.rs:220-222); the input bounds contain them.
   ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
-                         ptr<float>(ctx->vout[2]), &ctx->ctl->n_voxels, n, nparams));
+                         ptr<float>(ctx->vout[2]), ptr<const float4>(ctx->vaos),
+                         &ctx->ctl->n_voxels, n, nparams));
   if (vout && vout->keys) ST_TRY(unpack_keys(ctx, n));
   ST_TRY(read_control(ctx));
   const uint64_t v = ctx->ctl_host->n_voxels;
@@ -674,7 +685,8 @@ srcu_status srcu_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
   if (n > 0) {
     ST_TRY(enqueue_voxel(ctx, cols, nc, n, vparams));
     ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
-                           ptr<float>(ctx->vout[2]), &ctx->ctl->n_voxels, n, nparams));
+                           ptr<float>(ctx->vout[2]), ptr<const float4>(ctx->vaos),
+                         &ctx->ctl->n_voxels, n, nparams));
   }
   ctx->last_attrs = cloud->n_attrs;
   CU_TRY(cudaGetLastError());

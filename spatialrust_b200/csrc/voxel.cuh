@@ -28,10 +28,11 @@ __global__ void k_begin(Control *ctl, unsigned long long n_points) {
 
 // Per-axis min/max over finite coordinates plus NaN / inf flags
 // (compute_bounds, voxel.rs:1067-1079, ignores NaN through f32::min/max).
-// Reads `count` from *count_dev when non-null, else uses n.
+// Reads the point count from *count_dev when non-null, else ctl->n_points.
 __global__ void __launch_bounds__(BND_THREADS) k_bounds(const float *x, const float *y,
                                                         const float *z, Control *ctl,
-                                                        const unsigned long long *count_dev) {
+                                                        const unsigned long long *count_dev,
+                                                        const float *a0, float4 *aos) {
   if (ld_relaxed_u32(&ctl->status)) return;
   const uint64_t n = count_dev ? *count_dev : ctl->n_points;
   uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0, 0, 0};
@@ -39,6 +40,9 @@ __global__ void __launch_bounds__(BND_THREADS) k_bounds(const float *x, const fl
   const float *cols[3] = {x, y, z};
   for (uint64_t i = blockIdx.x * uint64_t(BND_THREADS) + threadIdx.x; i < n;
        i += uint64_t(gridDim.x) * BND_THREADS) {
+    // Optional AoS copy (x, y, z, first attribute): later gathers by point
+    // index then touch one 32-byte sector per point instead of one per column.
+    if (aos) aos[i] = make_float4(x[i], y[i], z[i], a0 ? a0[i] : 0.0f);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const float v = cols[a][i];
@@ -161,48 +165,64 @@ struct Columns {
 };
 
 constexpr int SEG_THREADS = 256;
-constexpr int SEG_ITEMS = 8;
-constexpr int SEG_TILE = SEG_THREADS * SEG_ITEMS;  // 2048 sorted positions per tile
+constexpr int SEG_ITEMS = 4;
+constexpr int SEG_TILE = SEG_THREADS * SEG_ITEMS;  // 1024 sorted positions per tile
 constexpr uint32_t SEG_SHORT = 32;  // longer voxels are reduced by a whole warp
 
-struct SegmentSmem {
+// Shared memory of k_voxel_segments<NC>: the tile's keys (plus one before and
+// one after), the scan scratch, and the tile's gathered point columns.
+struct SegmentSmemHead {
   uint64_t keys[SEG_TILE + 2];  // keys[0] = key before the tile, keys[1 + tile_n] = key after it
-  uint32_t vals[SEG_TILE];
   uint32_t scratch[SEG_THREADS / 32];
   uint32_t tile;
+  uint32_t pad;
 };
+__host__ __device__ constexpr size_t segment_smem_bytes(int nc) {
+  return sizeof(SegmentSmemHead) + size_t(nc) * SEG_TILE * sizeof(float);
+}
 
 template <int NC>
 __device__ __forceinline__ void write_centroid(const Columns<NC> &cols, const double (&s)[NC],
                                                uint32_t cnt, uint32_t seg, uint64_t key,
                                                uint64_t *out_keys, uint32_t *out_counts,
-                                               uint32_t n, uint32_t *status) {
+                                               uint32_t n, uint32_t *status, float4 *aos_out) {
   if (seg >= n) {  // cannot happen for a consistent sort; never write out of bounds
     atomicOr(status, ST_INTERNAL);
     return;
   }
   // (sum * (1.0 / count)) as f32, voxel.rs:531-536
   const double inv = 1.0 / double(cnt);
+  float o[NC];
 #pragma unroll
-  for (int c = 0; c < NC; ++c) cols.out[c][seg] = __double2float_rn(__dmul_rn(s[c], inv));
+  for (int c = 0; c < NC; ++c) {
+    o[c] = __double2float_rn(__dmul_rn(s[c], inv));
+    cols.out[c][seg] = o[c];
+  }
+  if (aos_out) aos_out[seg] = make_float4(o[0], o[1], o[2], 0.0f);
   out_keys[seg] = key;
   out_counts[seg] = cnt;
 }
 
 // Fused segment discovery + FP64 centroid reduction over the sorted
-// (key, index) pairs.  Each tile flags voxel starts, numbers them with a
-// block scan plus decoupled look-back, and reduces every voxel that starts in
-// it: one thread per short voxel (sequential FP64 sum in ascending point
-// index, the reference's order, voxel.rs:502-520), one warp per long voxel or
-// per voxel that runs past the tile end.
+// (key, index) pairs.  Each tile gathers its points' columns into shared
+// memory with all threads at once (independent loads, so the random gather
+// overlaps), flags voxel starts, numbers them with a block scan plus
+// decoupled look-back, and reduces every voxel that starts in it: one thread
+// per short voxel (sequential FP64 sum in ascending point index, the
+// reference's order, voxel.rs:502-520), one warp per long voxel or per voxel
+// that runs past the tile end.
 template <int NC>
 __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, SortBuffers sort,
                                                                  const uint32_t *final_buf,
                                                                  Columns<NC> cols,
                                                                  uint64_t *out_keys,
                                                                  uint32_t *out_counts,
-                                                                 uint64_t *lookback) {
-  __shared__ SegmentSmem sm;
+                                                                 uint64_t *lookback,
+                                                                 const float4 *aos_in,
+                                                                 float4 *aos_out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SegmentSmemHead &sm = *reinterpret_cast<SegmentSmemHead *>(smem_raw);
+  float *scol = reinterpret_cast<float *>(smem_raw + sizeof(SegmentSmemHead));  // [NC][SEG_TILE]
   if (ld_relaxed_u32(&ctl->status)) return;
   const uint32_t n = uint32_t(ctl->n_points);
   if (n == 0) return;
@@ -222,7 +242,25 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
     const uint32_t tile_n = min(uint32_t(SEG_TILE), n - base);
     for (uint32_t j = t; j < tile_n; j += SEG_THREADS) {
       sm.keys[1 + j] = keys[base + j];
-      sm.vals[j] = vals[base + j];
+      const uint32_t v = vals[base + j];
+      if (v < n) {
+        if (aos_in) {  // columns 0..3 from the AoS copy: one sector per point
+          const float4 p = aos_in[v];
+          scol[0 * SEG_TILE + j] = p.x;
+          scol[1 * SEG_TILE + j] = p.y;
+          scol[2 * SEG_TILE + j] = p.z;
+          if (NC > 3) scol[3 * SEG_TILE + j] = p.w;
+#pragma unroll
+          for (int c = 4; c < NC; ++c) scol[c * SEG_TILE + j] = cols.in[c][v];
+        } else {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) scol[c * SEG_TILE + j] = cols.in[c][v];
+        }
+      } else {  // a consistent sort never produces this; never read out of bounds
+        atomicOr(&ctl->status, ST_INTERNAL);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) scol[c * SEG_TILE + j] = 0.0f;
+      }
     }
     if (t == 0) {
       sm.keys[0] = base > 0 ? keys[base - 1] : ~keys[0];
@@ -246,8 +284,9 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
     seg_base = sm.scratch[0];
     if (t == 0 && tile == num_tiles - 1) ctl->n_voxels = seg_base + tile_count;
 
-    // Short voxels: the owning thread reduces sequentially.  At most one
-    // voxel per thread (its last start) can be long or run past the tile.
+    // Short voxels: the owning thread reduces sequentially from shared memory.
+    // At most one voxel per thread (its last start) can be long or run past
+    // the tile.
     bool deferred = false;
     uint32_t def_pos = 0, def_seg = 0;
     uint32_t seg = seg_base + local;
@@ -263,15 +302,11 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
 #pragma unroll
         for (int c = 0; c < NC; ++c) s[c] = 0.0;
         for (uint32_t m = j; m < e; ++m) {
-          const uint32_t v = sm.vals[m];
-          if (v >= n) {  // a consistent sort never produces this; never read out of bounds
-            atomicOr(&ctl->status, ST_INTERNAL);
-            continue;
-          }
 #pragma unroll
-          for (int c = 0; c < NC; ++c) s[c] += double(cols.in[c][v]);
+          for (int c = 0; c < NC; ++c) s[c] += double(scol[c * SEG_TILE + m]);
         }
-        write_centroid<NC>(cols, s, e - j, seg, key, out_keys, out_counts, n, &ctl->status);
+        write_centroid<NC>(cols, s, e - j, seg, key, out_keys, out_counts, n, &ctl->status,
+                           aos_out);
       } else {
         deferred = true;
         def_pos = base + j;
@@ -279,7 +314,7 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
       }
       ++seg;
     }
-    // Long voxels: the whole warp finds the end and reduces.
+    // Long voxels: the whole warp finds the end and reduces from global memory.
     uint32_t pending = __ballot_sync(FULL_MASK, deferred);
     while (pending) {
       const uint32_t src_lane = __ffs(pending) - 1;
@@ -314,10 +349,30 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
       for (int c = 0; c < NC; ++c)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s[c] += __shfl_xor_sync(FULL_MASK, s[c], o);
-      if (lane == 0) write_centroid<NC>(cols, s, e - p, sg, key, out_keys, out_counts, n, &ctl->status);
+      if (lane == 0)
+        write_centroid<NC>(cols, s, e - p, sg, key, out_keys, out_counts, n, &ctl->status, aos_out);
     }
     __syncthreads();
   }
+}
+
+// Opts every k_voxel_segments<NC> instantiation into the shared memory it
+// needs (more than 48 KB for many attribute columns).
+template <int NC>
+inline cudaError_t configure_segments_nc() {
+  return cudaFuncSetAttribute(k_voxel_segments<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(segment_smem_bytes(NC)));
+}
+inline cudaError_t configure_segment_kernels() {
+  cudaError_t e = cudaSuccess;
+  const cudaError_t all[] = {configure_segments_nc<3>(),  configure_segments_nc<4>(),
+                             configure_segments_nc<5>(),  configure_segments_nc<6>(),
+                             configure_segments_nc<7>(),  configure_segments_nc<8>(),
+                             configure_segments_nc<9>(),  configure_segments_nc<10>(),
+                             configure_segments_nc<11>(), configure_segments_nc<12>()};
+  for (cudaError_t x : all)
+    if (x != cudaSuccess) e = x;
+  return e;
 }
 
 // Unpacks packed voxel keys into the reference's (ix, iy, iz) int64 triples.
