@@ -222,13 +222,13 @@ typedef enum srcu_kernel_id {
   SRCU_K_BEGIN = 0,      /* control-block reset */
   SRCU_K_BOUNDS,         /* per-axis min/max */
   SRCU_K_VOXEL_PLAN,     /* voxel-key packing plan */
-  SRCU_K_VOXEL_HIST,     /* digit histograms of the voxel keys */
-  SRCU_K_VOXEL_SORT,     /* onesweep passes over the voxel keys (8 launches) */
+  SRCU_K_VOXEL_HIST,     /* reserved: the histograms run inside SRCU_K_VOXEL_SORT */
+  SRCU_K_VOXEL_SORT,     /* persistent onesweep sort of the voxel keys (histograms + passes) */
   SRCU_K_VOXEL_SEGMENTS, /* fused voxel segmentation + FP64 centroid reduction */
   SRCU_K_UNPACK_KEYS,    /* packed key -> (ix, iy, iz) */
   SRCU_K_CELL_PLAN,      /* radius-grid plan */
-  SRCU_K_CELL_HIST,      /* digit histograms of the cell keys */
-  SRCU_K_CELL_SORT,      /* onesweep passes over the cell keys (8 launches) */
+  SRCU_K_CELL_HIST,      /* reserved: the histograms run inside SRCU_K_CELL_SORT */
+  SRCU_K_CELL_SORT,      /* persistent onesweep sort of the cell keys (histograms + passes) */
   SRCU_K_CELLS,          /* cell table + cell-sorted point records */
   SRCU_K_HASH,           /* cell hash table */
   SRCU_K_RANGES,         /* 3x3 neighbour column ranges */

@@ -64,9 +64,9 @@ srcu_status noalloc_setup(int device, NoallocDevice **out) {
       return SRCU_ERR_CUDA;
     }
     if (cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-        cudaFuncSetAttribute(k_onesweep<VoxelKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_sort<VoxelKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              sizeof(OnesweepSmem)) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_sort, k_onesweep<VoxelKeySrc>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_sort, k_sort<VoxelKeySrc>,
                                                       OS_THREADS, sizeof(OnesweepSmem)) != cudaSuccess ||
         configure_segment_kernels() != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_seg, k_voxel_segments<4>, SEG_THREADS,
@@ -92,7 +92,7 @@ void noalloc_segments(cudaStream_t s, uint32_t grid, Control *ctl, const SortBuf
     cols.out[c] = out[c];
   }
   k_voxel_segments<NC><<<grid, SEG_THREADS, segment_smem_bytes(NC), s>>>(
-      ctl, sb, &ctl->vsort_final, cols, vkeys, vcounts, sb.lookback + 0, nullptr, nullptr);
+      ctl, sb, &ctl->vsort, cols, vkeys, vcounts, sb.lookback + 0, nullptr, nullptr);
 }
 
 }  // namespace
@@ -156,14 +156,11 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
   src.x = in[0];
   src.y = in[1];
   src.z = in[2];
-  k_digit_hist<VoxelKeySrc>
-      <<<std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, HIST_THREADS * 8), sms * 4)),
-         HIST_THREADS, 0, s>>>(src, ctl, ctl->hist_v);
-  const uint32_t grid_s =
-      std::min<uint32_t>(std::max<uint32_t>(1, ceil_div(n, OS_TILE)), sms * uint32_t(dev->occ_sort));
-  for (int k = 0; k < MAX_DIGITS; ++k)
-    k_onesweep<VoxelKeySrc><<<grid_s, OS_THREADS, sizeof(OnesweepSmem), s>>>(
-        src, ctl, ctl->hist_v, sb, k, EP_VSORT, WK_VSORT, &ctl->vsort_final);
+  if (launch_sort_kernel(s, dev->num_sms, dev->occ_sort, src, ctl, ctl->hist_v, sb, EP_VSORT,
+                         WK_VSORT, &ctl->vsort, n) != cudaSuccess) {
+    cudaGetLastError();
+    return SRCU_ERR_CUDA;
+  }
   const uint32_t grid_g =
       std::min<uint32_t>(std::max<uint32_t>(1, ceil_div(n, SEG_TILE)), sms * uint32_t(dev->occ_seg));
   switch (nc) {

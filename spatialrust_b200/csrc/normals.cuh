@@ -71,10 +71,9 @@ struct CellKeySrc {
   __device__ __forceinline__ uint32_t count(const Control *ctl) const {
     return uint32_t(count_dev ? *count_dev : ctl->n_points);
   }
-  __device__ __forceinline__ uint32_t num_digits() const { return pl.num_digits; }
-  __device__ __forceinline__ void load(uint32_t i, uint64_t &k, uint32_t &v) const {
-    k = cell_pack(pl, x[i], y[i], z[i]);
-    v = i;
+  __device__ __forceinline__ uint32_t key_bits() const { return pl.total_bits; }
+  __device__ __forceinline__ uint64_t key(uint32_t i) const {
+    return cell_pack(pl, x[i], y[i], z[i]);
   }
 };
 
@@ -93,7 +92,7 @@ struct CellSmem {
 // offsets in the sorted order, cell keys; cell_start[U] = n) and records each
 // sorted point's cell number.
 __global__ void __launch_bounds__(CELL_THREADS) k_cells(Control *ctl, SortBuffers sort,
-                                                        const uint32_t *final_buf,
+                                                        const SortState *sort_state,
                                                         const unsigned long long *count_dev,
                                                         const float4 *aos, float4 *pts,
                                                         uint32_t *pt_cell, uint64_t *cell_key,
@@ -108,9 +107,7 @@ __global__ void __launch_bounds__(CELL_THREADS) k_cells(Control *ctl, SortBuffer
     }
     return;
   }
-  const uint32_t fb = *final_buf;
-  const uint64_t *keys = sort.keys[fb];
-  const uint32_t *vals = sort.vals[fb];
+  const SortedView sv = sorted_view(sort, *sort_state);
   const uint32_t epoch = ctl->epoch + EP_CELLS;
   const uint32_t num_tiles = (n + CELL_TILE - 1) / CELL_TILE;
   const uint32_t t = threadIdx.x;
@@ -122,8 +119,8 @@ __global__ void __launch_bounds__(CELL_THREADS) k_cells(Control *ctl, SortBuffer
     const uint32_t base = tile * CELL_TILE;
     const uint32_t tile_n = min(uint32_t(CELL_TILE), n - base);
     for (uint32_t j = t; j < tile_n; j += CELL_THREADS) {
-      sm.keys[1 + j] = keys[base + j];
-      const uint32_t v = vals[base + j];
+      sm.keys[1 + j] = sv.key(base + j);
+      const uint32_t v = sv.val(base + j);
       if (v < n) {
         const float4 p = aos[v];
         pts[base + j] = make_float4(p.x, p.y, p.z, __uint_as_float(v));
@@ -132,7 +129,7 @@ __global__ void __launch_bounds__(CELL_THREADS) k_cells(Control *ctl, SortBuffer
         atomicOr(&ctl->status, ST_INTERNAL);
       }
     }
-    if (t == 0) sm.keys[0] = base > 0 ? keys[base - 1] : ~keys[0];
+    if (t == 0) sm.keys[0] = base > 0 ? sv.key(base - 1) : ~sv.key(0);
     __syncthreads();
     const uint32_t j0 = t * CELL_ITEMS;
     uint32_t flags = 0;

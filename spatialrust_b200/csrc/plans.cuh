@@ -61,6 +61,19 @@ struct CellPlan {
   uint32_t pad;
 };
 
+// State of one sort: where the result is and how it is encoded, plus the
+// grid barrier of its persistent kernel.
+struct SortState {
+  uint32_t final_buf;  // ping-pong buffer holding the sorted items
+  uint32_t passes;     // digit passes that ran (non-trivial digits)
+  uint32_t packed;     // 1: items are (key << idx_bits) | index; 0: keys[] + vals[]
+  uint32_t idx_bits;
+  uint32_t key_bits;
+  uint32_t bar_count;
+  uint32_t bar_gen;
+  uint32_t pad;
+};
+
 struct NormalCounters {
   unsigned long long valid;
   unsigned long long invalid;
@@ -81,18 +94,11 @@ struct Control {
   VoxelPlan vplan;
   CellPlan cplan;
   NormalCounters ncount;
-  uint32_t vsort_final;  // ping-pong buffer holding the sorted voxel keys
-  uint32_t csort_final;  // ping-pong buffer holding the sorted cell keys
-  uint32_t vsort_passes; // digit passes that ran (non-trivial digits)
-  uint32_t csort_passes;
+  SortState vsort;  // voxel-key sort
+  SortState csort;  // cell-key sort
   uint32_t hist_v[MAX_DIGITS * RADIX_BINS];  // voxel-key digit histograms
   uint32_t hist_c[MAX_DIGITS * RADIX_BINS];  // cell-key digit histograms
 };
-
-static_assert(offsetof(Control, vsort_passes) == offsetof(Control, vsort_final) + 8,
-              "k_onesweep writes the pass count two words after the buffer index");
-static_assert(offsetof(Control, csort_passes) == offsetof(Control, csort_final) + 8,
-              "k_onesweep writes the pass count two words after the buffer index");
 
 constexpr uint32_t EPOCHS_PER_RUN = 64;
 // Epoch offsets (within a run) of each look-back user.

@@ -133,9 +133,9 @@ T *ptr(DevBuf &b) {
 uint32_t ceil_div(uint64_t a, uint64_t b) { return uint32_t((a + b - 1) / b); }
 
 const char *const kKernelNames[SRCU_K_COUNT] = {
-    "k_begin",          "k_bounds",        "k_voxel_plan",  "k_digit_hist<voxel>",
-    "k_onesweep<voxel>", "k_voxel_segments", "k_unpack_voxel_keys", "k_cell_plan",
-    "k_digit_hist<cell>", "k_onesweep<cell>", "k_cells",       "k_hash_insert",
+    "k_begin",          "k_bounds",        "k_voxel_plan",  "(in k_sort<voxel>)",
+    "k_sort<voxel>",    "k_voxel_segments", "k_unpack_voxel_keys", "k_cell_plan",
+    "(in k_sort<cell>)", "k_sort<cell>",    "k_cells",       "k_hash_insert",
     "k_ranges",         "k_normals"};
 
 // Counts the launches of one kernel group and, when its bit is set in
@@ -258,24 +258,32 @@ SortBuffers sort_buffers(srcu_ctx *ctx) {
   return sb;
 }
 
+// Launches the persistent cooperative sort (histogram + every needed digit
+// pass in one kernel).  The grid never exceeds the co-resident block count.
+template <class Src>
+cudaError_t launch_sort_kernel(cudaStream_t stream, int num_sms, int occ, const Src &src,
+                               Control *ctl, uint32_t *hist, const SortBuffers &sb,
+                               uint32_t epoch_off, int work_slot, SortState *st, uint64_t n_max) {
+  const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, OS_TILE));
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(tiles, uint32_t(num_sms) * uint32_t(occ)));
+  Src s = src;
+  Control *c = ctl;
+  uint32_t *h = hist;
+  SortBuffers b = sb;
+  uint32_t e = epoch_off;
+  int w = work_slot;
+  SortState *ss = st;
+  void *args[] = {&s, &c, &h, &b, &e, &w, &ss};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(&k_sort<Src>), dim3(grid),
+                                     dim3(OS_THREADS), args, sizeof(OnesweepSmem), stream);
+}
+
 template <class Src>
 srcu_status launch_sort(srcu_ctx *ctx, const Src &src, uint64_t n_max, uint32_t *hist,
-                        uint32_t epoch_off, int work_slot, uint32_t *final_buf, int occ,
-                        int hist_id, int sort_id) {
-  const uint32_t grid_h = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n_max, HIST_THREADS * 8),
-                                                                    uint32_t(ctx->num_sms) * 4));
-  {
-    Launch l(ctx, hist_id);
-    k_digit_hist<Src><<<grid_h, HIST_THREADS, 0, ctx->stream>>>(src, ctx->ctl, hist);
-  }
-  const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, OS_TILE));
-  const uint32_t grid_s = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(occ));
-  const SortBuffers sb = sort_buffers(ctx);
-  Launch l(ctx, sort_id, MAX_DIGITS);
-  for (int k = 0; k < MAX_DIGITS; ++k)
-    k_onesweep<Src><<<grid_s, OS_THREADS, sizeof(OnesweepSmem), ctx->stream>>>(
-        src, ctx->ctl, hist, sb, k, epoch_off, work_slot, final_buf);
-  CU_TRY(cudaGetLastError());
+                        uint32_t epoch_off, int work_slot, SortState *st, int occ, int sort_id) {
+  Launch l(ctx, sort_id);
+  CU_TRY(launch_sort_kernel(ctx->stream, ctx->num_sms, occ, src, ctx->ctl, hist, sort_buffers(ctx),
+                            epoch_off, work_slot, st, n_max));
   return SRCU_OK;
 }
 
@@ -287,7 +295,7 @@ void launch_segments_nc(srcu_ctx *ctx, const float **in, uint32_t grid) {
     cols.out[c] = ptr<float>(ctx->vout[c]);
   }
   k_voxel_segments<NC><<<grid, SEG_THREADS, segment_smem_bytes(NC), ctx->stream>>>(
-      ctx->ctl, sort_buffers(ctx), &ctx->ctl->vsort_final, cols, ptr<uint64_t>(ctx->vkeys),
+      ctx->ctl, sort_buffers(ctx), &ctx->ctl->vsort, cols, ptr<uint64_t>(ctx->vkeys),
       ptr<uint32_t>(ctx->vcounts), ptr<uint64_t>(ctx->lb_seg), ptr<const float4>(ctx->in_aos),
       ptr<float4>(ctx->vaos));
 }
@@ -312,8 +320,8 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
   src.x = in[0];
   src.y = in[1];
   src.z = in[2];
-  ST_TRY(launch_sort(ctx, src, n, ctx->ctl->hist_v, EP_VSORT, WK_VSORT, &ctx->ctl->vsort_final,
-                     ctx->occ_onesweep_v, SRCU_K_VOXEL_HIST, SRCU_K_VOXEL_SORT));
+  ST_TRY(launch_sort(ctx, src, n, ctx->ctl->hist_v, EP_VSORT, WK_VSORT, &ctx->ctl->vsort,
+                     ctx->occ_onesweep_v, SRCU_K_VOXEL_SORT));
   const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n, SEG_TILE));
   const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(ctx->occ_seg));
   Launch l(ctx, SRCU_K_VOXEL_SEGMENTS);
@@ -348,15 +356,14 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
   src.y = y;
   src.z = z;
   src.count_dev = count_dev;
-  ST_TRY(launch_sort(ctx, src, n_max, ctx->ctl->hist_c, EP_CSORT, WK_CSORT,
-                     &ctx->ctl->csort_final, ctx->occ_onesweep_c, SRCU_K_CELL_HIST,
-                     SRCU_K_CELL_SORT));
+  ST_TRY(launch_sort(ctx, src, n_max, ctx->ctl->hist_c, EP_CSORT, WK_CSORT, &ctx->ctl->csort,
+                     ctx->occ_onesweep_c, SRCU_K_CELL_SORT));
   const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, CELL_TILE));
   const uint32_t grid_c = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(ctx->occ_cells));
   {
     Launch l(ctx, SRCU_K_CELLS);
     k_cells<<<grid_c, CELL_THREADS, 0, ctx->stream>>>(
-        ctx->ctl, sort_buffers(ctx), &ctx->ctl->csort_final, count_dev, aos,
+        ctx->ctl, sort_buffers(ctx), &ctx->ctl->csort, count_dev, aos,
         ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint64_t>(ctx->cell_key),
         ptr<uint32_t>(ctx->cell_start), ptr<uint64_t>(ctx->lb_cells));
   }
@@ -516,15 +523,15 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
   if (cudaMemset(ctx->ctl, 0, sizeof(Control)) != cudaSuccess) return bail(SRCU_ERR_CUDA);
   if (cudaMallocHost(&ctx->ctl_host, sizeof(Control)) != cudaSuccess) return bail(SRCU_ERR_CUDA);
   // Kernels with more than 48 KB of dynamic shared memory opt in once.
-  if (cudaFuncSetAttribute(k_onesweep<VoxelKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(k_sort<VoxelKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            sizeof(OnesweepSmem)) != cudaSuccess ||
-      cudaFuncSetAttribute(k_onesweep<CellKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_sort<CellKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            sizeof(OnesweepSmem)) != cudaSuccess ||
       false)
     return bail(SRCU_ERR_CUDA);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_v, k_onesweep<VoxelKeySrc>,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_v, k_sort<VoxelKeySrc>,
                                                 OS_THREADS, sizeof(OnesweepSmem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_c, k_onesweep<CellKeySrc>,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_c, k_sort<CellKeySrc>,
                                                 OS_THREADS, sizeof(OnesweepSmem));
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals, k_normals, NM_THREADS, 0);
   if (configure_segment_kernels() != cudaSuccess) return bail(SRCU_ERR_CUDA);
@@ -742,8 +749,8 @@ srcu_status srcu_chain_info_get(srcu_ctx *ctx, srcu_chain_info *info) {
   info->cells = c.n_cells;
   info->voxel_key_bits = c.vplan.total_bits;
   info->cell_key_bits = c.cplan.total_bits;
-  info->voxel_sort_passes = c.vsort_passes;
-  info->cell_sort_passes = c.csort_passes;
+  info->voxel_sort_passes = c.vsort.passes;
+  info->cell_sort_passes = c.csort.passes;
   info->cell_size = c.cplan.h;
   return SRCU_OK;
 }

@@ -151,10 +151,9 @@ struct VoxelKeySrc {
   __device__ __forceinline__ uint32_t count(const Control *ctl) const {
     return uint32_t(ctl->n_points);
   }
-  __device__ __forceinline__ uint32_t num_digits() const { return pl.num_digits; }
-  __device__ __forceinline__ void load(uint32_t i, uint64_t &k, uint32_t &v) const {
-    k = voxel_pack(pl, x[i], y[i], z[i]);
-    v = i;
+  __device__ __forceinline__ uint32_t key_bits() const { return pl.total_bits; }
+  __device__ __forceinline__ uint64_t key(uint32_t i) const {
+    return voxel_pack(pl, x[i], y[i], z[i]);
   }
 };
 
@@ -213,7 +212,7 @@ __device__ __forceinline__ void write_centroid(const Columns<NC> &cols, const do
 // that runs past the tile end.
 template <int NC>
 __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, SortBuffers sort,
-                                                                 const uint32_t *final_buf,
+                                                                 const SortState *sort_state,
                                                                  Columns<NC> cols,
                                                                  uint64_t *out_keys,
                                                                  uint32_t *out_counts,
@@ -226,9 +225,7 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
   if (ld_relaxed_u32(&ctl->status)) return;
   const uint32_t n = uint32_t(ctl->n_points);
   if (n == 0) return;
-  const uint32_t fb = *final_buf;
-  const uint64_t *keys = sort.keys[fb];
-  const uint32_t *vals = sort.vals[fb];
+  const SortedView sv = sorted_view(sort, *sort_state);
   const uint32_t epoch = ctl->epoch + EP_VSEG;
   const uint32_t num_tiles = (n + SEG_TILE - 1) / SEG_TILE;
   const uint32_t t = threadIdx.x, lane = t & 31u;
@@ -241,8 +238,8 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
     const uint32_t base = tile * SEG_TILE;
     const uint32_t tile_n = min(uint32_t(SEG_TILE), n - base);
     for (uint32_t j = t; j < tile_n; j += SEG_THREADS) {
-      sm.keys[1 + j] = keys[base + j];
-      const uint32_t v = vals[base + j];
+      sm.keys[1 + j] = sv.key(base + j);
+      const uint32_t v = sv.val(base + j);
       if (v < n) {
         if (aos_in) {  // columns 0..3 from the AoS copy: one sector per point
           const float4 p = aos_in[v];
@@ -263,8 +260,8 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
       }
     }
     if (t == 0) {
-      sm.keys[0] = base > 0 ? keys[base - 1] : ~keys[0];
-      sm.keys[1 + tile_n] = base + tile_n < n ? keys[base + tile_n] : ~keys[n - 1];
+      sm.keys[0] = base > 0 ? sv.key(base - 1) : ~sv.key(0);
+      sm.keys[1 + tile_n] = base + tile_n < n ? sv.key(base + tile_n) : ~sv.key(n - 1);
     }
     __syncthreads();
 
@@ -321,11 +318,11 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
       pending &= pending - 1;
       const uint32_t p = __shfl_sync(FULL_MASK, def_pos, src_lane);
       const uint32_t sg = __shfl_sync(FULL_MASK, def_seg, src_lane);
-      const uint64_t key = keys[p];
+      const uint64_t key = sv.key(p);
       uint32_t e = p + 1;
       for (;;) {
         const uint32_t idx = e + lane;
-        const bool stop = idx >= n || keys[idx] != key;
+        const bool stop = idx >= n || sv.key(idx) != key;
         const uint32_t b = __ballot_sync(FULL_MASK, stop);
         if (b) {
           e += __ffs(b) - 1;
@@ -337,7 +334,7 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
 #pragma unroll
       for (int c = 0; c < NC; ++c) s[c] = 0.0;
       for (uint32_t m = p + lane; m < e; m += 32) {
-        const uint32_t v = vals[m];
+        const uint32_t v = sv.val(m);
         if (v >= n) {
           atomicOr(&ctl->status, ST_INTERNAL);
           continue;
