@@ -266,8 +266,9 @@ def run_gpu(args):
         step()
     torch.cuda.synchronize()
     infos = []
+    nstats = []
     for c in ctxs:
-        c.frame_check()
+        nstats.append(c.frame_check()[1])
         infos.append(c.chain_info())
 
     # untimed profile pass: which kernel group dominates
@@ -344,6 +345,9 @@ def run_gpu(args):
         vs_baseline=None, dtype="f32", data="synthetic",
         config=dict(workload=WORKLOAD, points=N_POINTS, leaves=list(LEAVES), radius=RADIUS,
                     voxels=[i["voxels"] for i in infos], cells=[i["cells"] for i in infos],
+                    sort_passes=[[i["voxel_sort_passes"], i["cell_sort_passes"]] for i in infos],
+                    normals=[{k: st[k] for k in ("valid_count", "invalid_count", "fp64_eigensolves")}
+                             for st in nstats],
                     l2="flushed by a 256 MB write before every timed step (outside the events)",
                     parallelism=f"replicas x{world}"),
         e2e=e2e, roofline=roofline, clocks=clock, gpu_launches=int(launches),

@@ -114,6 +114,60 @@ __device__ __forceinline__ uint32_t lookback_exclusive(uint64_t *words, size_t s
   return excl;
 }
 
+// Warp-cooperative decoupled look-back for one counter per tile: the whole
+// warp calls it with the same arguments; lane l inspects tile (j - l), so one
+// step covers 32 predecessors and the walk is 32x shorter than a one-word
+// walk.  Returns the exclusive prefix in every lane.  Bounded.
+__device__ __forceinline__ uint32_t lookback_exclusive_warp(uint64_t *words, uint32_t tile,
+                                                            uint32_t value, uint32_t epoch,
+                                                            uint32_t *status) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint64_t *mine = words + tile;
+  if (tile == 0) {
+    if (lane == 0) st_relaxed(mine, lb_pack(epoch, LB_INC, value));
+    return 0;
+  }
+  if (lane == 0) st_relaxed(mine, lb_pack(epoch, LB_AGG, value));
+  uint32_t excl = 0;
+  int64_t j = int64_t(tile) - 1;
+  uint32_t spins = 0;
+  while (j >= 0) {
+    const int64_t idx = j - int64_t(lane);
+    uint64_t w = lb_pack(epoch, LB_INC, 0);  // before tile 0: an inclusive zero
+    if (idx >= 0) w = ld_relaxed(words + idx);
+    const uint64_t flag = w & (3ull << 30);
+    const bool ready = uint32_t(w >> 32) == epoch && flag != 0;
+    const uint32_t not_ready = __ballot_sync(FULL_MASK, !ready);
+    const uint32_t inc = __ballot_sync(FULL_MASK, ready && flag == LB_INC);
+    // lanes [0, first not-ready) are usable; stop at the first inclusive among them
+    const uint32_t usable = not_ready ? (1u << (__ffs(not_ready) - 1)) - 1u : FULL_MASK;
+    const uint32_t inc_usable = inc & usable;
+    uint32_t take;  // lanes whose counts are added this step
+    if (inc_usable) {
+      const uint32_t first_inc = __ffs(inc_usable) - 1;
+      take = first_inc == 31 ? FULL_MASK : ((1u << (first_inc + 1)) - 1u);
+    } else {
+      take = usable;
+    }
+    uint32_t c = ((take >> lane) & 1u) ? (uint32_t(w) & LB_COUNT_MASK) : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(FULL_MASK, c, o);
+    excl += c;
+    if (inc_usable) break;
+    const uint32_t consumed = __popc(take);
+    j -= consumed;
+    if (consumed == 0) {
+      if (++spins > SPIN_LIMIT) {
+        if (lane == 0) atomicOr(status, ST_TIMEOUT);
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  if (lane == 0) st_relaxed(mine, lb_pack(epoch, LB_INC, excl + value));
+  return excl;
+}
+
 // Block-wide exclusive sum over 256 threads (8 warps).  `scratch` holds >= 8
 // words of shared memory.  Returns the exclusive prefix; *total = block sum.
 template <int THREADS>

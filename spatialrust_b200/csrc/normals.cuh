@@ -140,7 +140,10 @@ __global__ void __launch_bounds__(CELL_THREADS) k_cells(Control *ctl, SortBuffer
     }
     uint32_t tile_count;
     const uint32_t local = block_exclusive_sum<CELL_THREADS>(__popc(flags), sm.scratch, &tile_count);
-    if (t == 0) sm.scratch[0] = lookback_exclusive(lookback, 1, tile, tile_count, epoch, &ctl->status);
+    if (t < 32) {
+      const uint32_t cb = lookback_exclusive_warp(lookback, tile, tile_count, epoch, &ctl->status);
+      if (t == 0) sm.scratch[0] = cb;
+    }
     __syncthreads();
     const uint32_t cbase = sm.scratch[0];
     uint32_t c = cbase + local;

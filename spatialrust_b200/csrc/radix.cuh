@@ -34,6 +34,7 @@ constexpr int OS_ITEMS = 16;
 constexpr int OS_WARP_ITEMS = OS_ITEMS * 32;
 constexpr int OS_TILE = OS_THREADS * OS_ITEMS;  // 4096 keys per tile
 constexpr int HIST_COPIES = 2;                  // shared histogram copies (by warp parity)
+constexpr int LB_WIDTH = 8;                     // look-back words read per step
 
 struct OnesweepTileSmem {
   uint64_t keys[OS_TILE];
@@ -278,19 +279,31 @@ __global__ void __launch_bounds__(OS_THREADS, 2) k_sort(Src src, Control *ctl, u
           if (!packed) sm.u.tile.vals[pos] = v[i];
         }
       }
-      // Resolve the look-back for digit t.
+      // Resolve the look-back for digit t, LB_WIDTH predecessors per step
+      // (independent loads, one latency), stopping at the first inclusive.
       uint32_t excl = 0;
       if (tile > 0) {
         int64_t j = int64_t(tile) - 1;
         uint32_t spins = 0;
-        while (j >= 0) {
-          const uint64_t w = ld_relaxed(buf.lookback + size_t(j) * RADIX_BINS + t);
-          const uint64_t flag = w & (3ull << 30);
-          if (uint32_t(w >> 32) == epoch && flag != 0) {
-            excl += uint32_t(w) & LB_COUNT_MASK;
-            if (flag == LB_INC) break;
-            --j;
-          } else {
+        bool done = false;
+        while (!done && j >= 0) {
+          uint64_t w[LB_WIDTH];
+#pragma unroll
+          for (int q = 0; q < LB_WIDTH; ++q)
+            w[q] = (j - q >= 0) ? ld_relaxed(buf.lookback + size_t(j - q) * RADIX_BINS + t)
+                                : lb_pack(epoch, LB_INC, 0);
+          uint32_t consumed = 0;
+#pragma unroll
+          for (int q = 0; q < LB_WIDTH; ++q) {
+            if (done || consumed != uint32_t(q)) break;
+            const uint64_t flag = w[q] & (3ull << 30);
+            if (uint32_t(w[q] >> 32) != epoch || flag == 0) break;
+            excl += uint32_t(w[q]) & LB_COUNT_MASK;
+            ++consumed;
+            if (flag == LB_INC) done = true;
+          }
+          j -= consumed;
+          if (!done && consumed == 0) {
             if (++spins > SPIN_LIMIT) {
               atomicOr(&ctl->status, ST_TIMEOUT);
               break;

@@ -275,8 +275,10 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
     uint32_t tile_count;
     const uint32_t local = block_exclusive_sum<SEG_THREADS>(__popc(flags), sm.scratch, &tile_count);
     uint32_t seg_base = 0;
-    if (t == 0) seg_base = lookback_exclusive(lookback, 1, tile, tile_count, epoch, &ctl->status);
-    if (t == 0) sm.scratch[0] = seg_base;
+    if (t < 32) {
+      seg_base = lookback_exclusive_warp(lookback, tile, tile_count, epoch, &ctl->status);
+      if (t == 0) sm.scratch[0] = seg_base;
+    }
     __syncthreads();
     seg_base = sm.scratch[0];
     if (t == 0 && tile == num_tiles - 1) ctl->n_voxels = seg_base + tile_count;
