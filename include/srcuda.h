@@ -171,6 +171,25 @@ srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
                                const srcu_voxel_out *vout, const srcu_normal_out *nout,
                                uint64_t *out_voxels, srcu_normal_stats *stats);
 
+/* ---- many clouds in one chain ---------------------------------------------- */
+
+/* Enqueues voxel -> normals for `count` clouds in one chain: the clouds'
+ * points are concatenated in `points` (device-resident), cloud b owning
+ * points [offsets[b], offsets[b+1]) (host array, count + 1 entries, offsets[0]
+ * = 0, offsets[count] = points->n).  Each cloud has its own voxel and normal
+ * parameters (host arrays of count entries).  The cloud id rides above the
+ * per-cloud key bits, so one sort, one segment pass and one radius grid serve
+ * every cloud; neighbours never cross clouds.  Results stay on the device in
+ * cloud order (srcu_frame_view_get / srcu_frame_fetch); the voxel range of
+ * each cloud comes from srcu_batch_voxel_offsets.  Replaces a per-cloud loop
+ * of MvpPipeline::run (crates/spatialrust-pipeline/src/mvp.rs:193-226). */
+srcu_status srcu_batch_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *points,
+                                             const uint64_t *offsets, uint32_t count,
+                                             const srcu_voxel_params *vparams,
+                                             const srcu_normal_params *nparams);
+/* Synchronises and copies the count + 1 voxel offsets of the last batch. */
+srcu_status srcu_batch_voxel_offsets(srcu_ctx *ctx, uint64_t *voxel_offsets);
+
 /* ---- device-resident chain (GpuSpatialFrame, gpu_frame.rs:71-365) --------- */
 
 /* Enqueues the voxel -> normals chain on the context stream for a cloud

@@ -160,6 +160,10 @@ SIGNATURES = {
                           ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(SrcuNormalStats)],
                          ctypes.c_int),
     "srcu_chain_info_get": ([_P, ctypes.POINTER(SrcuChainInfo)], ctypes.c_int),
+    "srcu_batch_voxel_normals_enqueue": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(ctypes.c_uint64),
+                                          ctypes.c_uint32, ctypes.POINTER(SrcuVoxelParams),
+                                          ctypes.POINTER(SrcuNormalParams)], ctypes.c_int),
+    "srcu_batch_voxel_offsets": ([_P, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
     "srcu_profile_enable": ([_P, ctypes.c_uint64], ctypes.c_int),
     "srcu_voxel_centroid_noalloc": ([ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuVoxelParams),
                                      ctypes.POINTER(SrcuVoxelOut), ctypes.POINTER(ctypes.c_uint64),
@@ -403,6 +407,28 @@ class Context:
         np_ = _normal_params(radius, min_neighbors, viewpoint, include_self, count_shell)
         self._check(self._lib.srcu_voxel_normals_enqueue(self._h, ctypes.byref(cloud),
                                                          ctypes.byref(vp), ctypes.byref(np_)))
+
+    def batch_voxel_normals_enqueue(self, points: SrcuCloud, offsets, leaves, radii,
+                                    min_neighbors: int = 3, viewpoints=None,
+                                    include_self: bool = False, count_shell: bool = True,
+                                    origins=None):
+        """Voxel -> normals for many clouds concatenated in `points` (device)."""
+        count = len(offsets) - 1
+        offs = (ctypes.c_uint64 * (count + 1))(*[int(o) for o in offsets])
+        vps = (SrcuVoxelParams * count)(*[
+            _voxel_params(leaves[b], None if origins is None else origins[b]) for b in range(count)])
+        nps = (SrcuNormalParams * count)(*[
+            _normal_params(radii[b], min_neighbors, None if viewpoints is None else viewpoints[b],
+                           include_self, count_shell) for b in range(count)])
+        self._check(self._lib.srcu_batch_voxel_normals_enqueue(self._h, ctypes.byref(points), offs,
+                                                               count, vps, nps))
+        self._last_batch = count
+
+    def batch_voxel_offsets(self) -> np.ndarray:
+        count = getattr(self, "_last_batch", 1)
+        out = (ctypes.c_uint64 * (count + 1))()
+        self._check(self._lib.srcu_batch_voxel_offsets(self._h, out))
+        return np.frombuffer(out, dtype=np.uint64).astype(np.int64)
 
     def frame_view(self) -> SrcuFrameView:
         view = SrcuFrameView()

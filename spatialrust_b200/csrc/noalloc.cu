@@ -28,7 +28,14 @@ constexpr size_t NA_LB_SEG =
     NA_LB_SORT + na_align(((NA_MAX_POINTS + OS_TILE - 1) / OS_TILE) * RADIX_BINS * 8);
 constexpr size_t NA_VKEYS = NA_LB_SEG + na_align(((NA_MAX_POINTS + SEG_TILE - 1) / SEG_TILE) * 8);
 constexpr size_t NA_VCOUNTS = NA_VKEYS + na_align(NA_MAX_POINTS * 8);
-constexpr size_t NA_BYTES = NA_VCOUNTS + na_align(NA_MAX_POINTS * 4);
+constexpr size_t NA_BATCH = NA_VCOUNTS + na_align(NA_MAX_POINTS * 4);
+// one-cloud batch arrays: offsets[2], bounds, plan, parameters, voxel offsets[2]
+constexpr size_t NA_B_OFFSETS = NA_BATCH;
+constexpr size_t NA_B_BOUNDS = NA_B_OFFSETS + 256;
+constexpr size_t NA_B_VPLAN = NA_B_BOUNDS + na_align(sizeof(Bounds));
+constexpr size_t NA_B_VPARAMS = NA_B_VPLAN + na_align(sizeof(VoxelPlan));
+constexpr size_t NA_B_VOFF = NA_B_VPARAMS + na_align(sizeof(VoxelParamsDev));
+constexpr size_t NA_BYTES = NA_B_VOFF + 256;
 constexpr int NA_MAX_DEVICES = 64;
 
 }  // namespace
@@ -146,16 +153,30 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
     outc[3 + a] = out->attrs[a];
   }
   const uint32_t sms = uint32_t(dev->num_sms);
-  // k_begin zeroes the control block (all but the epoch) on every call.
-  k_begin<<<1, 256, 0, s>>>(ctl, n);
+  Batch bt;
+  bt.clouds = 1;
+  bt.offsets = reinterpret_cast<const uint32_t *>(b + NA_B_OFFSETS);
+  bt.bounds = reinterpret_cast<Bounds *>(b + NA_B_BOUNDS);
+  bt.vplans = reinterpret_cast<VoxelPlan *>(b + NA_B_VPLAN);
+  bt.cplans = nullptr;
+  bt.vparams = reinterpret_cast<const VoxelParamsDev *>(b + NA_B_VPARAMS);
+  bt.nparams = nullptr;
+  bt.voxel_offsets = reinterpret_cast<uint32_t *>(b + NA_B_VOFF);
+  VoxelParamsDev vp0{};
+  vp0.leaf = params->leaf_size;
+  vp0.has_origin = params->has_origin;
+  for (int a = 0; a < 3; ++a) vp0.origin[a] = params->origin[a];
+  // k_begin zeroes the control block (all but the epoch) and writes the
+  // cloud's offsets and parameters on every call.
+  k_begin<<<1, 256, 0, s>>>(ctl, n, bt, 0u, 1, vp0, NormalParamsDev{});
   k_bounds<<<std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4), sms * 8)),
-             BND_THREADS, 0, s>>>(in[0], in[1], in[2], ctl, nullptr, nullptr, nullptr);
-  k_voxel_plan<<<1, 32, 0, s>>>(ctl, params->leaf_size, params->has_origin, params->origin[0],
-                                params->origin[1], params->origin[2]);
+             BND_THREADS, 0, s>>>(in[0], in[1], in[2], ctl, nullptr, nullptr, nullptr, bt);
+  k_voxel_plans<<<1, 32, 0, s>>>(ctl, bt);
   VoxelKeySrc src;
   src.x = in[0];
   src.y = in[1];
   src.z = in[2];
+  src.bt = bt;
   if (launch_sort_kernel(s, dev->num_sms, dev->occ_sort, src, ctl, ctl->hist_v, sb, EP_VSORT,
                          WK_VSORT, &ctl->vsort, n) != cudaSuccess) {
     cudaGetLastError();
@@ -178,7 +199,7 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
   }
   if (out->keys)
     k_unpack_voxel_keys<<<std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, 256), sms * 8)), 256,
-                          0, s>>>(ctl, vkeys, out->keys);
+                          0, s>>>(ctl, vkeys, out->keys, bt);
   if (cudaGetLastError() != cudaSuccess) return SRCU_ERR_CUDA;
   // Read back the status word and V (two words of the control block).
   uint32_t status = 0;

@@ -17,24 +17,27 @@
 
 namespace srcu {
 
-// Cell plan from the bounds of the cloud (any box that contains every finite
-// point works).  h >= r (1 + 1e-5): points within r (f32 predicate) then
-// differ by at most one cell per axis even after the FP64 cell arithmetic.
-// h is also kept >= extent / 2^19 so every axis fits in 20 bits; larger
-// cells only add candidates, never drop neighbours.
-__global__ void k_cell_plan(Control *ctl, float radius) {
-  if (threadIdx.x != 0 || ld_relaxed_u32(&ctl->status)) return;
+// Cell plan of each cloud from its bounds (any box that contains every
+// finite point works).  h >= r (1 + 1e-5): points within r (f32 predicate)
+// then differ by at most one cell per axis even after the FP64 cell
+// arithmetic.  h is also kept >= extent / 2^19 so every axis fits in 20
+// bits; larger cells only add candidates, never drop neighbours.
+__global__ void k_cell_plans(Control *ctl, Batch bt) {
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bt.clouds) return;
+  const float radius = bt.nparams[b].radius;
   if (!(radius >= 0.0f) || isinf(radius)) {
     atomicOr(&ctl->status, ST_BAD_PARAMS);
     return;
   }
   CellPlan pl{};
-  const Bounds b = ctl->bounds;
+  const Bounds bd = bt.bounds[b];
   double lo[3], ext[3], max_ext = 0.0;
   for (int a = 0; a < 3; ++a) {
-    const bool any = b.mn[a] != 0xffffffffu;
-    lo[a] = any ? double(ord2f(b.mn[a])) : 0.0;
-    const double hi = any ? double(ord2f(b.mx[a])) : 0.0;
+    const bool any = bd.mn[a] != 0xffffffffu;
+    lo[a] = any ? double(ord2f(bd.mn[a])) : 0.0;
+    const double hi = any ? double(ord2f(bd.mx[a])) : 0.0;
     ext[a] = hi - lo[a];
     max_ext = fmax(max_ext, ext[a]);
   }
@@ -58,22 +61,39 @@ __global__ void k_cell_plan(Control *ctl, float radius) {
   pl.r2 = __fmul_rn(radius, radius);
   pl.shell_tol = __fmul_rn(1e-6f, pl.r2);
   pl.valid = 1;
-  ctl->cplan = pl;
+  bt.cplans[b] = pl;
+  atomicMax(&ctl->ckey_bits, total);
+  if (total + ctl->cloud_bits > 64) atomicOr(&ctl->status, ST_KEY_OVERFLOW);
 }
 
 // Key source for the cell sort over `count_dev` points (V for the chained
-// voxel -> normals path, n otherwise).
+// voxel -> normals path, n otherwise).  The cloud of point i comes from its
+// packed voxel key (chained path) or from the batch offsets.
 struct CellKeySrc {
   const float *x, *y, *z;
   const unsigned long long *count_dev;
-  CellPlan pl;
-  __device__ __forceinline__ void prepare(const Control *ctl) { pl = ctl->cplan; }
+  const uint64_t *voxel_keys;  // non-null: points are voxel centroids in key order
+  Batch bt;
+  CellPlan pl;  // the plan when there is one cloud
+  uint32_t local_bits, cloud_bits, voxel_local_bits;
+  __device__ __forceinline__ void prepare(const Control *ctl) {
+    local_bits = ctl->ckey_bits;
+    cloud_bits = ctl->cloud_bits;
+    voxel_local_bits = ctl->vkey_bits;
+    if (bt.clouds == 1) pl = bt.cplans[0];
+  }
   __device__ __forceinline__ uint32_t count(const Control *ctl) const {
     return uint32_t(count_dev ? *count_dev : ctl->n_points);
   }
-  __device__ __forceinline__ uint32_t key_bits() const { return pl.total_bits; }
+  __device__ __forceinline__ uint32_t key_bits() const { return local_bits + cloud_bits; }
+  __device__ __forceinline__ uint32_t cloud(uint32_t i) const {
+    if (voxel_keys) return voxel_local_bits >= 64 ? 0u : uint32_t(voxel_keys[i] >> voxel_local_bits);
+    return cloud_of(bt, i);
+  }
   __device__ __forceinline__ uint64_t key(uint32_t i) const {
-    return cell_pack(pl, x[i], y[i], z[i]);
+    if (bt.clouds == 1) return cell_pack(pl, x[i], y[i], z[i]);
+    const uint32_t b = cloud(i);
+    return with_cloud(cell_pack(bt.cplans[b], x[i], y[i], z[i]), b, local_bits);
   }
 };
 
@@ -225,17 +245,21 @@ __device__ __forceinline__ int32_t cell_lookup(const uint64_t *table, const uint
 // most three) cells are consecutive in key order, so each column is one
 // contiguous range: 9 ranges cover the 27-cell neighbourhood.
 __global__ void k_ranges(Control *ctl, const uint64_t *cell_key, const uint32_t *cell_start,
-                         const uint64_t *table, uint32_t log2cap, uint2 *ranges) {
+                         const uint64_t *table, uint32_t log2cap, uint2 *ranges, Batch bt) {
   if (ld_relaxed_u32(&ctl->status)) return;
-  const CellPlan pl = ctl->cplan;
   const uint64_t u_count = ctl->n_cells;
   const uint32_t epoch = ctl->epoch + EP_CELLS;
+  const uint32_t lb = ctl->ckey_bits;
+  const uint64_t local_mask = lb >= 64 ? ~0ull : ((1ull << lb) - 1);
   for (uint64_t w = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; w < u_count * 9;
        w += uint64_t(gridDim.x) * blockDim.x) {
     const uint64_t u = w / 9;
     const uint32_t col = uint32_t(w - u * 9);
+    const uint64_t full = cell_key[u];
+    const uint32_t b = (bt.clouds == 1 || lb >= 64) ? 0u : uint32_t(full >> lb);
+    const CellPlan &pl = bt.cplans[b < bt.clouds ? b : 0];
     uint32_t cx, cy, cz;
-    cell_unpack(pl, cell_key[u], cx, cy, cz);
+    cell_unpack(pl, full & local_mask, cx, cy, cz);
     const int64_t nx = int64_t(cx) + int64_t(col / 3) - 1;
     const int64_t ny = int64_t(cy) + int64_t(col % 3) - 1;
     uint2 rg = make_uint2(0, 0);
@@ -244,7 +268,8 @@ __global__ void k_ranges(Control *ctl, const uint64_t *cell_key, const uint32_t 
       for (int dz = -1; dz <= 1; ++dz) {
         const int64_t nz = int64_t(cz) + dz;
         if (nz < 0 || nz >= pl.dims[2]) continue;
-        const uint64_t key = (uint64_t(nx) << pl.shift_x) | (uint64_t(ny) << pl.shift_y) | uint64_t(nz);
+        const uint64_t key = with_cloud(
+            (uint64_t(nx) << pl.shift_x) | (uint64_t(ny) << pl.shift_y) | uint64_t(nz), b, lb);
         const int32_t f = cell_lookup(table, cell_key, key, log2cap, epoch);
         if (f >= 0) {
           if (first < 0) first = f;
@@ -256,14 +281,6 @@ __global__ void k_ranges(Control *ctl, const uint64_t *cell_key, const uint32_t 
     ranges[w] = rg;
   }
 }
-
-struct NormalParamsDev {
-  uint32_t min_neighbors;
-  int32_t include_self;
-  int32_t has_viewpoint;
-  int32_t count_shell;  // report points with a candidate on the radius shell
-  float vp[3];
-};
 
 constexpr int NM_THREADS = 256;
 constexpr int NM_FLUSH = 32;  // f32 partial moments are folded into FP64 every NM_FLUSH candidates
@@ -326,7 +343,8 @@ __device__ __noinline__ void moments_fp64(const float4 *pts, const uint2 *rg, fl
 // eigensolve are FP64.
 __global__ void __launch_bounds__(NM_THREADS, 3) k_normals(Control *ctl, const float4 *pts,
                                                            const uint32_t *pt_cell,
-                                                           const uint2 *ranges, NormalParamsDev prm,
+                                                           const uint2 *ranges,
+                                                           const uint64_t *cell_key, Batch bt,
                                                            const unsigned long long *count_dev,
                                                            float *nx, float *ny, float *nz,
                                                            float *curv, uint32_t *counts) {
@@ -334,8 +352,7 @@ __global__ void __launch_bounds__(NM_THREADS, 3) k_normals(Control *ctl, const f
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t n = uint32_t(count_dev ? *count_dev : ctl->n_points);
   const uint64_t u_count = ctl->n_cells;
-  const float r2 = ctl->cplan.r2;
-  const float shell_tol = ctl->cplan.shell_tol;
+  const uint32_t lb = ctl->ckey_bits;
   const uint32_t batches = (n + 31) / 32;
   const uint32_t warps = gridDim.x * (NM_THREADS / 32);
   unsigned long long n_valid = 0, n_invalid = 0, n_shell = 0, n_fp64 = 0;
@@ -350,6 +367,12 @@ __global__ void __launch_bounds__(NM_THREADS, 3) k_normals(Control *ctl, const f
       atomicOr(&ctl->status, ST_INTERNAL);
       continue;
     }
+    uint32_t cb = 0;  // the query's cloud
+    if (bt.clouds > 1 && lb < 64) cb = uint32_t(cell_key[u] >> lb);
+    if (cb >= bt.clouds) cb = 0;
+    const NormalParamsDev prm = bt.nparams[cb];
+    const float r2 = bt.cplans[cb].r2;
+    const float shell_tol = bt.cplans[cb].shell_tol;
     const uint2 *rg = ranges + size_t(u) * 9;
     float hits = 0.f;
     uint32_t shell = 0;

@@ -61,6 +61,53 @@ struct CellPlan {
   uint32_t pad;
 };
 
+// Per-cloud parameters on the device (srcu_voxel_params / srcu_normal_params).
+struct VoxelParamsDev {
+  float leaf;
+  int32_t has_origin;
+  float origin[3];
+};
+
+struct NormalParamsDev {
+  float radius;
+  uint32_t min_neighbors;
+  int32_t include_self;
+  int32_t has_viewpoint;
+  int32_t count_shell;  // report points with a candidate on the radius shell
+  float vp[3];
+};
+
+// Many clouds in one chain.  Points of cloud b are [offsets[b], offsets[b+1])
+// of the concatenated columns; its id sits above the per-cloud key bits of
+// every voxel and cell key, so one sort orders all clouds at once.  A single
+// cloud is the case clouds == 1.
+struct Batch {
+  uint32_t clouds;
+  const uint32_t *offsets;         // clouds + 1 point offsets
+  Bounds *bounds;                  // clouds
+  VoxelPlan *vplans;               // clouds
+  CellPlan *cplans;                // clouds
+  const VoxelParamsDev *vparams;   // clouds
+  const NormalParamsDev *nparams;  // clouds
+  uint32_t *voxel_offsets;         // clouds + 1, voxel ranges of each cloud
+};
+
+// Cloud owning concatenated point i: the largest b with offsets[b] <= i.
+__device__ __forceinline__ uint32_t cloud_of(const Batch &bt, uint32_t i) {
+  uint32_t lo = 0, hi = bt.clouds;  // invariant: offsets[lo] <= i < offsets[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(bt.offsets + mid) <= i) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__host__ __device__ __forceinline__ uint64_t with_cloud(uint64_t local_key, uint32_t cloud,
+                                                        uint32_t local_bits) {
+  return local_bits >= 64 ? local_key : (local_key | (uint64_t(cloud) << local_bits));
+}
+
 // State of one sort: where the result is and how it is encoded, plus the
 // grid barrier of its persistent kernel.
 struct SortState {
@@ -90,9 +137,10 @@ struct Control {
   unsigned long long n_voxels;  // V
   unsigned long long n_cells;   // U (occupied radius-grid cells)
   uint32_t work[64];            // per-kernel dynamic tile counters
-  Bounds bounds;
-  VoxelPlan vplan;
-  CellPlan cplan;
+  uint32_t clouds;              // B
+  uint32_t cloud_bits;          // bits of the cloud id above the per-cloud key bits
+  uint32_t vkey_bits;           // per-cloud voxel key bits (max over clouds)
+  uint32_t ckey_bits;           // per-cloud cell key bits (max over clouds)
   NormalCounters ncount;
   SortState vsort;  // voxel-key sort
   SortState csort;  // cell-key sort

@@ -49,6 +49,14 @@ struct srcu_ctx {
   DevBuf nout[4], ncounts;
   uint32_t last_attrs = 0;  // attribute count of the last enqueued chain
   const float *frame_attr_ptrs[MAX_COLS] = {};
+  // batch arrays (clouds of the last chain) and pinned staging for their parameters
+  DevBuf b_offsets, b_bounds, b_vplans, b_cplans, b_vparams, b_nparams, b_voff;
+  uint32_t batch_cap = 0;
+  uint32_t last_clouds = 1;
+  unsigned char *h_stage[2] = {nullptr, nullptr};
+  size_t h_stage_bytes[2] = {0, 0};
+  cudaEvent_t h_stage_ev[2] = {nullptr, nullptr};
+  int h_stage_next = 0;
   // launch accounting / CUDA-event timing per kernel group (srcu_profile_*)
   uint64_t prof_mask = 0;
   uint64_t launches[SRCU_K_COUNT] = {};
@@ -260,6 +268,91 @@ SortBuffers sort_buffers(srcu_ctx *ctx) {
 
 // Launches the persistent cooperative sort (histogram + every needed digit
 // pass in one kernel).  The grid never exceeds the co-resident block count.
+srcu_status reserve_batch(srcu_ctx *ctx, uint32_t clouds) {
+  const uint64_t b = std::max<uint32_t>(clouds, 1);
+  ST_TRY(ensure(ctx, ctx->b_offsets, (b + 1) * 4));
+  ST_TRY(ensure(ctx, ctx->b_bounds, b * sizeof(Bounds)));
+  ST_TRY(ensure(ctx, ctx->b_vplans, b * sizeof(VoxelPlan)));
+  ST_TRY(ensure(ctx, ctx->b_cplans, b * sizeof(CellPlan)));
+  ST_TRY(ensure(ctx, ctx->b_vparams, b * sizeof(VoxelParamsDev)));
+  ST_TRY(ensure(ctx, ctx->b_nparams, b * sizeof(NormalParamsDev)));
+  ST_TRY(ensure(ctx, ctx->b_voff, (b + 1) * 4));
+  ctx->batch_cap = std::max<uint32_t>(ctx->batch_cap, uint32_t(b));
+  return SRCU_OK;
+}
+
+Batch make_batch(srcu_ctx *ctx, uint32_t clouds) {
+  Batch bt;
+  bt.clouds = clouds;
+  bt.offsets = ptr<const uint32_t>(ctx->b_offsets);
+  bt.bounds = ptr<Bounds>(ctx->b_bounds);
+  bt.vplans = ptr<VoxelPlan>(ctx->b_vplans);
+  bt.cplans = ptr<CellPlan>(ctx->b_cplans);
+  bt.vparams = ptr<const VoxelParamsDev>(ctx->b_vparams);
+  bt.nparams = ptr<const NormalParamsDev>(ctx->b_nparams);
+  bt.voxel_offsets = ptr<uint32_t>(ctx->b_voff);
+  return bt;
+}
+
+VoxelParamsDev to_dev(const srcu_voxel_params *vp) {
+  VoxelParamsDev d{};
+  if (!vp) return d;
+  d.leaf = vp->leaf_size;
+  d.has_origin = vp->has_origin;
+  for (int a = 0; a < 3; ++a) d.origin[a] = vp->origin[a];
+  return d;
+}
+
+NormalParamsDev to_dev(const srcu_normal_params *np) {
+  NormalParamsDev d{};
+  if (!np) return d;
+  d.radius = np->radius;
+  d.min_neighbors = np->min_neighbors;
+  d.include_self = np->include_self;
+  d.has_viewpoint = np->has_viewpoint;
+  d.count_shell = np->count_shell;
+  for (int a = 0; a < 3; ++a) d.vp[a] = np->viewpoint[a];
+  return d;
+}
+
+uint32_t cloud_bits_for(uint32_t clouds) { return clouds > 1 ? bit_width_u64(clouds - 1) : 0; }
+
+// Copies the offsets and per-cloud parameters of a batch to the device
+// through a pinned staging slot (two slots alternate; a slot is reused only
+// after its previous copy has completed).
+srcu_status stage_batch(srcu_ctx *ctx, uint32_t clouds, const uint64_t *offsets,
+                        const srcu_voxel_params *vp, const srcu_normal_params *np) {
+  const size_t off_bytes = (size_t(clouds) + 1) * 4;
+  const size_t vp_bytes = size_t(clouds) * sizeof(VoxelParamsDev);
+  const size_t np_bytes = size_t(clouds) * sizeof(NormalParamsDev);
+  const size_t need = off_bytes + vp_bytes + np_bytes;
+  const int slot = ctx->h_stage_next;
+  ctx->h_stage_next ^= 1;
+  if (ctx->h_stage_ev[slot]) CU_TRY(cudaEventSynchronize(ctx->h_stage_ev[slot]));
+  if (ctx->h_stage_bytes[slot] < need) {
+    if (ctx->h_stage[slot]) CU_TRY(cudaFreeHost(ctx->h_stage[slot]));
+    ctx->h_stage[slot] = nullptr;
+    CU_TRY(cudaMallocHost(reinterpret_cast<void **>(&ctx->h_stage[slot]), need));
+    ctx->h_stage_bytes[slot] = need;
+  }
+  if (!ctx->h_stage_ev[slot])
+    CU_TRY(cudaEventCreateWithFlags(&ctx->h_stage_ev[slot], cudaEventDisableTiming));
+  unsigned char *h = ctx->h_stage[slot];
+  uint32_t *ho = reinterpret_cast<uint32_t *>(h);
+  for (uint32_t b = 0; b <= clouds; ++b) ho[b] = uint32_t(offsets[b]);
+  VoxelParamsDev *hv = reinterpret_cast<VoxelParamsDev *>(h + off_bytes);
+  NormalParamsDev *hn = reinterpret_cast<NormalParamsDev *>(h + off_bytes + vp_bytes);
+  for (uint32_t b = 0; b < clouds; ++b) {
+    hv[b] = to_dev(vp ? &vp[b] : nullptr);
+    hn[b] = to_dev(np ? &np[b] : nullptr);
+  }
+  CU_TRY(cudaMemcpyAsync(ctx->b_offsets.p, ho, off_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CU_TRY(cudaMemcpyAsync(ctx->b_vparams.p, hv, vp_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CU_TRY(cudaMemcpyAsync(ctx->b_nparams.p, hn, np_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CU_TRY(cudaEventRecord(ctx->h_stage_ev[slot], ctx->stream));
+  return SRCU_OK;
+}
+
 template <class Src>
 cudaError_t launch_sort_kernel(cudaStream_t stream, int num_sms, int occ, const Src &src,
                                Control *ctl, uint32_t *hist, const SortBuffers &sb,
@@ -302,24 +395,24 @@ void launch_segments_nc(srcu_ctx *ctx, const float **in, uint32_t grid) {
 
 // Voxel stage: bounds -> plan -> sort -> fused segment/centroid reduction.
 srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t n,
-                          const srcu_voxel_params *vp) {
+                          const Batch &bt) {
   const uint32_t grid_b = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4),
                                                                     uint32_t(ctx->num_sms) * 8));
   {
     Launch l(ctx, SRCU_K_BOUNDS);
     k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(in[0], in[1], in[2], ctx->ctl, nullptr,
                                                        nc > 3 ? in[3] : nullptr,
-                                                       ptr<float4>(ctx->in_aos));
+                                                       ptr<float4>(ctx->in_aos), bt);
   }
   {
     Launch l(ctx, SRCU_K_VOXEL_PLAN);
-    k_voxel_plan<<<1, 32, 0, ctx->stream>>>(ctx->ctl, vp->leaf_size, vp->has_origin,
-                                            vp->origin[0], vp->origin[1], vp->origin[2]);
+    k_voxel_plans<<<ceil_div(bt.clouds, 128), 128, 0, ctx->stream>>>(ctx->ctl, bt);
   }
   VoxelKeySrc src;
   src.x = in[0];
   src.y = in[1];
   src.z = in[2];
+  src.bt = bt;
   ST_TRY(launch_sort(ctx, src, n, ctx->ctl->hist_v, EP_VSORT, WK_VSORT, &ctx->ctl->vsort,
                      ctx->occ_onesweep_v, SRCU_K_VOXEL_SORT));
   const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n, SEG_TILE));
@@ -338,6 +431,8 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
     case 12: launch_segments_nc<12>(ctx, in, grid); break;
     default: return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "unsupported column count %u", nc);
   }
+  k_voxel_offsets<<<ceil_div(bt.clouds + 1, 128), 128, 0, ctx->stream>>>(
+      ctx->ctl, ptr<uint64_t>(ctx->vkeys), bt);
   CU_TRY(cudaGetLastError());
   return SRCU_OK;
 }
@@ -346,16 +441,18 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
 // or ctl->n_points when count_dev is null; n_max bounds the grid sizes.
 srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const float *z,
                             const float4 *aos, const unsigned long long *count_dev, uint64_t n_max,
-                            const srcu_normal_params *np) {
+                            const Batch &bt, const uint64_t *voxel_keys) {
   {
     Launch l(ctx, SRCU_K_CELL_PLAN);
-    k_cell_plan<<<1, 32, 0, ctx->stream>>>(ctx->ctl, np->radius);
+    k_cell_plans<<<ceil_div(bt.clouds, 128), 128, 0, ctx->stream>>>(ctx->ctl, bt);
   }
   CellKeySrc src;
   src.x = x;
   src.y = y;
   src.z = z;
   src.count_dev = count_dev;
+  src.voxel_keys = voxel_keys;
+  src.bt = bt;
   ST_TRY(launch_sort(ctx, src, n_max, ctx->ctl->hist_c, EP_CSORT, WK_CSORT, &ctx->ctl->csort,
                      ctx->occ_onesweep_c, SRCU_K_CELL_SORT));
   const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, CELL_TILE));
@@ -381,29 +478,27 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
     k_ranges<<<grid_r, 256, 0, ctx->stream>>>(ctx->ctl, ptr<uint64_t>(ctx->cell_key),
                                               ptr<uint32_t>(ctx->cell_start),
                                               ptr<uint64_t>(ctx->table), ctx->table_log2,
-                                              ptr<uint2>(ctx->ranges));
+                                              ptr<uint2>(ctx->ranges), bt);
   }
-  NormalParamsDev prm;
-  prm.min_neighbors = np->min_neighbors;
-  prm.include_self = np->include_self;
-  prm.has_viewpoint = np->has_viewpoint;
-  prm.count_shell = np->count_shell;
-  prm.vp[0] = np->viewpoint[0];
-  prm.vp[1] = np->viewpoint[1];
-  prm.vp[2] = np->viewpoint[2];
   const uint32_t grid_n = uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals);
   Launch l(ctx, SRCU_K_NORMALS);
   k_normals<<<grid_n, NM_THREADS, 0, ctx->stream>>>(
       ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint2>(ctx->ranges),
-      prm, count_dev, ptr<float>(ctx->nout[0]), ptr<float>(ctx->nout[1]), ptr<float>(ctx->nout[2]),
-      ptr<float>(ctx->nout[3]), ptr<uint32_t>(ctx->ncounts));
+      ptr<uint64_t>(ctx->cell_key), bt, count_dev, ptr<float>(ctx->nout[0]),
+      ptr<float>(ctx->nout[1]), ptr<float>(ctx->nout[2]), ptr<float>(ctx->nout[3]),
+      ptr<uint32_t>(ctx->ncounts));
   CU_TRY(cudaGetLastError());
   return SRCU_OK;
 }
 
-void begin_chain(srcu_ctx *ctx, uint64_t n) {
+// Starts a chain over one cloud (parameters written by k_begin itself) or
+// a staged batch (single == 0).
+void begin_chain(srcu_ctx *ctx, uint64_t n, const Batch &bt, int single,
+                 const srcu_voxel_params *vp, const srcu_normal_params *np) {
   Launch l(ctx, SRCU_K_BEGIN);
-  k_begin<<<1, 256, 0, ctx->stream>>>(ctx->ctl, n);
+  k_begin<<<1, 256, 0, ctx->stream>>>(ctx->ctl, n, bt, cloud_bits_for(bt.clouds), single,
+                                      to_dev(vp), to_dev(np));
+  ctx->last_clouds = bt.clouds;
 }
 
 srcu_status read_control(srcu_ctx *ctx) {
@@ -482,7 +577,8 @@ srcu_status unpack_keys(srcu_ctx *ctx, uint64_t n) {
   const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, 256), ctx->num_sms * 8));
   Launch l(ctx, SRCU_K_UNPACK_KEYS);
   k_unpack_voxel_keys<<<grid, 256, 0, ctx->stream>>>(ctx->ctl, ptr<uint64_t>(ctx->vkeys),
-                                                     ptr<int64_t>(ctx->vkeys3));
+                                                     ptr<int64_t>(ctx->vkeys3),
+                                                     make_batch(ctx, ctx->last_clouds));
   CU_TRY(cudaGetLastError());
   return SRCU_OK;
 }
@@ -560,6 +656,13 @@ void srcu_destroy(srcu_ctx *ctx) {
   for (auto &b : ctx->in) release(ctx, b);
   for (auto &b : ctx->vout) release(ctx, b);
   for (auto &b : ctx->nout) release(ctx, b);
+  DevBuf *batch[] = {&ctx->b_offsets, &ctx->b_bounds, &ctx->b_vplans, &ctx->b_cplans,
+                     &ctx->b_vparams, &ctx->b_nparams, &ctx->b_voff};
+  for (DevBuf *b : batch) release(ctx, *b);
+  for (int slot = 0; slot < 2; ++slot) {
+    if (ctx->h_stage_ev[slot]) cudaEventDestroy(ctx->h_stage_ev[slot]);
+    if (ctx->h_stage[slot]) cudaFreeHost(ctx->h_stage[slot]);
+  }
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->ctl) cudaFree(ctx->ctl);
   if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
@@ -595,11 +698,13 @@ srcu_status srcu_voxel_centroid(srcu_ctx *ctx, const srcu_cloud *cloud,
   if (n == 0) return SRCU_OK;  // voxel.rs:257-259: empty input is returned unchanged
   const uint32_t nc = 3 + cloud->n_attrs;
   ST_TRY(reserve(ctx, n, nc, !cloud->on_device, true, false));
+  ST_TRY(reserve_batch(ctx, 1));
   if (out && out->keys) ST_TRY(ensure(ctx, ctx->vkeys3, n * 24));
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, cloud, cols));
-  begin_chain(ctx, n);
-  ST_TRY(enqueue_voxel(ctx, cols, nc, n, params));
+  const Batch bt = make_batch(ctx, 1);
+  begin_chain(ctx, n, bt, 1, params, nullptr);
+  ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
   if (out && out->keys) ST_TRY(unpack_keys(ctx, n));
   ST_TRY(read_control(ctx));
   const uint64_t v = ctx->ctl_host->n_voxels;
@@ -620,20 +725,22 @@ srcu_status srcu_radius_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
   const uint64_t n = cloud->n;
   if (n == 0) return SRCU_OK;  // normal.rs:106-108
   ST_TRY(reserve(ctx, n, 3, !cloud->on_device, false, true));
+  ST_TRY(reserve_batch(ctx, 1));
   srcu_cloud xyz = *cloud;
   xyz.n_attrs = 0;
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, &xyz, cols));
-  begin_chain(ctx, n);
+  const Batch bt = make_batch(ctx, 1);
+  begin_chain(ctx, n, bt, 1, nullptr, params);
   const uint32_t grid_b = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4),
                                                                     uint32_t(ctx->num_sms) * 8));
   {
     Launch l(ctx, SRCU_K_BOUNDS);
     k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(cols[0], cols[1], cols[2], ctx->ctl, nullptr,
-                                                       nullptr, ptr<float4>(ctx->in_aos));
+                                                       nullptr, ptr<float4>(ctx->in_aos), bt);
   }
   ST_TRY(enqueue_normals(ctx, cols[0], cols[1], cols[2], ptr<const float4>(ctx->in_aos), nullptr, n,
-                         params));
+                         bt, nullptr));
   ST_TRY(read_control(ctx));
   ST_TRY(fetch_normals(ctx, out, n, stats));
   CU_TRY(cudaStreamSynchronize(ctx->stream));
@@ -655,15 +762,17 @@ srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
   if (n == 0) return SRCU_OK;
   const uint32_t nc = 3 + cloud->n_attrs;
   ST_TRY(reserve(ctx, n, nc, !cloud->on_device, true, true));
+  ST_TRY(reserve_batch(ctx, 1));
   if (vout && vout->keys) ST_TRY(ensure(ctx, ctx->vkeys3, n * 24));
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, cloud, cols));
-  begin_chain(ctx, n);
-  ST_TRY(enqueue_voxel(ctx, cols, nc, n, vparams));
+  const Batch bt = make_batch(ctx, 1);
+  begin_chain(ctx, n, bt, 1, vparams, nparams);
+  ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
   // Normals on the centroids (mvp.rs:220-222); the input bounds contain them.
   ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
                          ptr<float>(ctx->vout[2]), ptr<const float4>(ctx->vaos),
-                         &ctx->ctl->n_voxels, n, nparams));
+                         &ctx->ctl->n_voxels, n, bt, ptr<uint64_t>(ctx->vkeys)));
   if (vout && vout->keys) ST_TRY(unpack_keys(ctx, n));
   ST_TRY(read_control(ctx));
   const uint64_t v = ctx->ctl_host->n_voxels;
@@ -686,17 +795,69 @@ srcu_status srcu_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
   const uint64_t n = cloud->n;
   const uint32_t nc = 3 + cloud->n_attrs;
   ST_TRY(reserve(ctx, n, nc, false, true, true));
+  ST_TRY(reserve_batch(ctx, 1));
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, cloud, cols));
-  begin_chain(ctx, n);
+  const Batch bt = make_batch(ctx, 1);
+  begin_chain(ctx, n, bt, 1, vparams, nparams);
   if (n > 0) {
-    ST_TRY(enqueue_voxel(ctx, cols, nc, n, vparams));
+    ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
     ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
                            ptr<float>(ctx->vout[2]), ptr<const float4>(ctx->vaos),
-                         &ctx->ctl->n_voxels, n, nparams));
+                           &ctx->ctl->n_voxels, n, bt, ptr<uint64_t>(ctx->vkeys)));
   }
   ctx->last_attrs = cloud->n_attrs;
   CU_TRY(cudaGetLastError());
+  return SRCU_OK;
+}
+
+srcu_status srcu_batch_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *points,
+                                             const uint64_t *offsets, uint32_t count,
+                                             const srcu_voxel_params *vparams,
+                                             const srcu_normal_params *nparams) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  ST_TRY(check_cloud(ctx, points));
+  if (!points->on_device)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "batch enqueue needs device-resident points");
+  if (count == 0 || !offsets || !vparams || !nparams)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "a batch needs count >= 1, offsets and parameters");
+  if (offsets[0] != 0 || offsets[count] != points->n)
+    return fail(ctx, SRCU_ERR_LENGTH_MISMATCH, "offsets must run from 0 to the point count %llu",
+                (unsigned long long)points->n);
+  for (uint32_t b = 0; b < count; ++b) {
+    if (offsets[b + 1] < offsets[b])
+      return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing (cloud %u)", b);
+    ST_TRY(check_voxel_params(ctx, &vparams[b]));
+    ST_TRY(check_normal_params(ctx, &nparams[b]));
+  }
+  const uint64_t n = points->n;
+  const uint32_t nc = 3 + points->n_attrs;
+  ST_TRY(reserve(ctx, n, nc, false, true, true));
+  ST_TRY(reserve_batch(ctx, count));
+  const float *cols[MAX_COLS];
+  ST_TRY(stage_input(ctx, points, cols));
+  ST_TRY(stage_batch(ctx, count, offsets, vparams, nparams));
+  const Batch bt = make_batch(ctx, count);
+  begin_chain(ctx, n, bt, 0, nullptr, nullptr);
+  if (n > 0) {
+    ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
+    ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
+                           ptr<float>(ctx->vout[2]), ptr<const float4>(ctx->vaos),
+                           &ctx->ctl->n_voxels, n, bt, ptr<uint64_t>(ctx->vkeys)));
+  }
+  ctx->last_attrs = points->n_attrs;
+  CU_TRY(cudaGetLastError());
+  return SRCU_OK;
+}
+
+srcu_status srcu_batch_voxel_offsets(srcu_ctx *ctx, uint64_t *voxel_offsets) {
+  if (!ctx || !voxel_offsets) return SRCU_ERR_INVALID_ARGUMENT;
+  const uint32_t count = ctx->last_clouds;
+  std::vector<uint32_t> tmp(count + 1);
+  CU_TRY(cudaMemcpyAsync(tmp.data(), ctx->b_voff.p, (count + 1) * 4, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+  ST_TRY(read_control(ctx));
+  for (uint32_t b = 0; b <= count; ++b) voxel_offsets[b] = tmp[b];
   return SRCU_OK;
 }
 
@@ -747,11 +908,13 @@ srcu_status srcu_chain_info_get(srcu_ctx *ctx, srcu_chain_info *info) {
   info->points = c.n_points;
   info->voxels = c.n_voxels;
   info->cells = c.n_cells;
-  info->voxel_key_bits = c.vplan.total_bits;
-  info->cell_key_bits = c.cplan.total_bits;
+  info->voxel_key_bits = c.vkey_bits + c.cloud_bits;
+  info->cell_key_bits = c.ckey_bits + c.cloud_bits;
   info->voxel_sort_passes = c.vsort.passes;
   info->cell_sort_passes = c.csort.passes;
-  info->cell_size = c.cplan.h;
+  CellPlan first{};
+  CU_TRY(cudaMemcpy(&first, ctx->b_cplans.p, sizeof(CellPlan), cudaMemcpyDeviceToHost));
+  info->cell_size = first.h;
   return SRCU_OK;
 }
 

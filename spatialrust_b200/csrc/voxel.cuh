@@ -8,119 +8,186 @@ namespace srcu {
 
 constexpr int BND_THREADS = 256;
 
-// k_begin: zeroes the control block for a new chain and advances the epoch.
-__global__ void k_begin(Control *ctl, unsigned long long n_points) {
+// k_begin: zeroes the control block for a new chain, advances the epoch and
+// resets the per-cloud bounds.  For a single cloud it also writes the batch
+// arrays (offsets {0, n} and the cloud's parameters) so that no host copy is
+// needed.
+__global__ void k_begin(Control *ctl, unsigned long long n_points, Batch bt, uint32_t cloud_bits,
+                        int single, VoxelParamsDev vp0, NormalParamsDev np0) {
   const uint32_t t = threadIdx.x;
+  if (single && t == 0) {
+    uint32_t *off = const_cast<uint32_t *>(bt.offsets);
+    off[0] = 0;
+    off[1] = uint32_t(n_points);
+    if (bt.vparams) *const_cast<VoxelParamsDev *>(bt.vparams) = vp0;
+    if (bt.nparams) *const_cast<NormalParamsDev *>(bt.nparams) = np0;
+  }
   uint32_t *w = reinterpret_cast<uint32_t *>(ctl);
   const uint32_t words = sizeof(Control) / 4;
   // word 0 is the epoch
   for (uint32_t i = 1 + t; i < words; i += blockDim.x) w[i] = 0;
+  for (uint32_t b = t; b < bt.clouds; b += blockDim.x) {
+    Bounds z;
+    for (int a = 0; a < 3; ++a) {
+      z.mn[a] = 0xffffffffu;  // atomicMin target
+      z.mx[a] = 0u;
+    }
+    z.flags = 0;
+    z.pad = 0;
+    bt.bounds[b] = z;
+  }
   __syncthreads();
   if (t == 0) {
     ctl->epoch += EPOCHS_PER_RUN;
     ctl->n_points = n_points;
-    for (int a = 0; a < 3; ++a) {
-      ctl->bounds.mn[a] = 0xffffffffu;  // f2ord(+max) sentinel: atomicMin target
-      ctl->bounds.mx[a] = 0u;
-    }
+    ctl->clouds = bt.clouds;
+    ctl->cloud_bits = cloud_bits;
   }
 }
 
-// Per-axis min/max over finite coordinates plus NaN / inf flags
-// (compute_bounds, voxel.rs:1067-1079, ignores NaN through f32::min/max).
-// Reads the point count from *count_dev when non-null, else ctl->n_points.
-__global__ void __launch_bounds__(BND_THREADS) k_bounds(const float *x, const float *y,
-                                                        const float *z, Control *ctl,
-                                                        const unsigned long long *count_dev,
-                                                        const float *a0, float4 *aos) {
-  if (ld_relaxed_u32(&ctl->status)) return;
-  const uint64_t n = count_dev ? *count_dev : ctl->n_points;
-  uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0, 0, 0};
-  uint32_t flags = 0;
-  const float *cols[3] = {x, y, z};
-  for (uint64_t i = blockIdx.x * uint64_t(BND_THREADS) + threadIdx.x; i < n;
-       i += uint64_t(gridDim.x) * BND_THREADS) {
-    // Optional AoS copy (x, y, z, first attribute): later gathers by point
-    // index then touch one 32-byte sector per point instead of one per column.
-    if (aos) aos[i] = make_float4(x[i], y[i], z[i], a0 ? a0[i] : 0.0f);
+struct BoundsAcc {
+  uint32_t mn[3], mx[3], flags;
+  __device__ __forceinline__ void reset() {
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = 0xffffffffu;
+      mx[a] = 0u;
+    }
+    flags = 0;
+  }
+  __device__ __forceinline__ void add(float x, float y, float z) {
+    const float v[3] = {x, y, z};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float v = cols[a][i];
-      if (isnan(v)) {
+      if (isnan(v[a])) {
         flags |= 1u << a;
-      } else if (isinf(v)) {
+      } else if (isinf(v[a])) {
         flags |= 8u << a;
       } else {
-        const uint32_t o = f2ord(v);
+        const uint32_t o = f2ord(v[a]);
         mn[a] = min(mn[a], o);
         mx[a] = max(mx[a], o);
       }
     }
   }
+  __device__ __forceinline__ void flush(Bounds &b) const {
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      mn[a] = min(mn[a], __shfl_xor_sync(FULL_MASK, mn[a], o));
-      mx[a] = max(mx[a], __shfl_xor_sync(FULL_MASK, mx[a], o));
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) flags |= __shfl_xor_sync(FULL_MASK, flags, o);
-  __shared__ uint32_t s[BND_THREADS / 32][7];
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  if (lane == 0) {
     for (int a = 0; a < 3; ++a) {
-      s[warp][a] = mn[a];
-      s[warp][3 + a] = mx[a];
+      if (mn[a] != 0xffffffffu) atomicMin(&b.mn[a], mn[a]);
+      if (mx[a] != 0u) atomicMax(&b.mx[a], mx[a]);
     }
-    s[warp][6] = flags;
+    if (flags) atomicOr(&b.flags, flags);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < BND_THREADS / 32; ++w) {
-      for (int a = 0; a < 3; ++a) {
-        s[0][a] = min(s[0][a], s[w][a]);
-        s[0][3 + a] = max(s[0][3 + a], s[w][3 + a]);
+};
+
+constexpr uint32_t BND_CHUNK = 16;  // consecutive points per thread in the multi-cloud case
+
+// Per-cloud min/max over finite coordinates plus NaN / inf flags
+// (compute_bounds, voxel.rs:1067-1079, ignores NaN through f32::min/max).
+// The point count comes from *count_dev when non-null, else ctl->n_points.
+// Optionally writes an AoS copy (x, y, z, first attribute) so that later
+// gathers by point index touch one 32-byte sector per point.
+__global__ void __launch_bounds__(BND_THREADS) k_bounds(const float *x, const float *y,
+                                                        const float *z, Control *ctl,
+                                                        const unsigned long long *count_dev,
+                                                        const float *a0, float4 *aos, Batch bt) {
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint64_t n = count_dev ? *count_dev : ctl->n_points;
+  if (bt.clouds == 1) {
+    BoundsAcc acc;
+    acc.reset();
+    for (uint64_t i = blockIdx.x * uint64_t(BND_THREADS) + threadIdx.x; i < n;
+         i += uint64_t(gridDim.x) * BND_THREADS) {
+      const float xi = x[i], yi = y[i], zi = z[i];
+      if (aos) aos[i] = make_float4(xi, yi, zi, a0 ? a0[i] : 0.0f);
+      acc.add(xi, yi, zi);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        acc.mn[a] = min(acc.mn[a], __shfl_xor_sync(FULL_MASK, acc.mn[a], o));
+        acc.mx[a] = max(acc.mx[a], __shfl_xor_sync(FULL_MASK, acc.mx[a], o));
       }
-      s[0][6] |= s[w][6];
     }
-    for (int a = 0; a < 3; ++a) {
-      if (s[0][a] != 0xffffffffu) atomicMin(&ctl->bounds.mn[a], s[0][a]);
-      if (s[0][3 + a] != 0u) atomicMax(&ctl->bounds.mx[a], s[0][3 + a]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc.flags |= __shfl_xor_sync(FULL_MASK, acc.flags, o);
+    // one flush per block: warp results meet in shared memory first
+    __shared__ uint32_t sred[BND_THREADS / 32][7];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+      for (int a = 0; a < 3; ++a) {
+        sred[warp][a] = acc.mn[a];
+        sred[warp][3 + a] = acc.mx[a];
+      }
+      sred[warp][6] = acc.flags;
     }
-    if (s[0][6]) atomicOr(&ctl->bounds.flags, s[0][6]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (uint32_t w = 1; w < BND_THREADS / 32; ++w) {
+        for (int a = 0; a < 3; ++a) {
+          acc.mn[a] = min(acc.mn[a], sred[w][a]);
+          acc.mx[a] = max(acc.mx[a], sred[w][3 + a]);
+        }
+        acc.flags |= sred[w][6];
+      }
+      acc.flush(bt.bounds[0]);
+    }
+    return;
+  }
+  // Many clouds: each thread walks BND_CHUNK consecutive points and flushes
+  // its running bounds whenever the cloud changes.
+  const uint64_t chunks = (n + BND_CHUNK - 1) / BND_CHUNK;
+  for (uint64_t c = blockIdx.x * uint64_t(BND_THREADS) + threadIdx.x; c < chunks;
+       c += uint64_t(gridDim.x) * BND_THREADS) {
+    const uint32_t i0 = uint32_t(c * BND_CHUNK);
+    const uint64_t end = c * BND_CHUNK + BND_CHUNK;
+    const uint32_t i1 = uint32_t(end < n ? end : n);
+    uint32_t b = cloud_of(bt, i0);
+    uint32_t next = __ldg(bt.offsets + b + 1);
+    BoundsAcc acc;
+    acc.reset();
+    for (uint32_t i = i0; i < i1; ++i) {
+      while (i >= next) {  // crossed into a later cloud (skipping empty ones)
+        acc.flush(bt.bounds[b]);
+        acc.reset();
+        ++b;
+        next = __ldg(bt.offsets + b + 1);
+      }
+      const float xi = x[i], yi = y[i], zi = z[i];
+      if (aos) aos[i] = make_float4(xi, yi, zi, a0 ? a0[i] : 0.0f);
+      acc.add(xi, yi, zi);
+    }
+    acc.flush(bt.bounds[b]);
   }
 }
 
-// Builds the voxel-key plan from the bounds (filter_internal, voxel.rs:266-275).
-__global__ void k_voxel_plan(Control *ctl, float leaf, int has_origin, float ox, float oy,
-                             float oz) {
-  if (threadIdx.x != 0 || ld_relaxed_u32(&ctl->status)) return;
+// One voxel-key plan per cloud from its bounds and parameters
+// (filter_internal, voxel.rs:266-275).  The per-cloud key widths are reduced
+// to their maximum (ctl->vkey_bits); a cloud whose key plus the cloud id does
+// not fit in 64 bits stops the chain with ST_KEY_OVERFLOW.
+__global__ void k_voxel_plans(Control *ctl, Batch bt) {
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bt.clouds) return;
+  const VoxelParamsDev prm = bt.vparams[b];
   VoxelPlan pl{};
-  pl.inv_leaf = __fdiv_rn(1.0f, leaf);  // f32 IEEE division, voxel.rs:267
-  pl.floor_mode = has_origin ? 1 : 0;
-  const Bounds b = ctl->bounds;
+  pl.inv_leaf = __fdiv_rn(1.0f, prm.leaf);  // f32 IEEE division, voxel.rs:267
+  pl.floor_mode = prm.has_origin ? 1 : 0;
+  const Bounds bd = bt.bounds[b];
   float lo[3], hi[3];
   for (int a = 0; a < 3; ++a) {
-    const bool any = b.mn[a] != 0xffffffffu;
-    lo[a] = any ? ord2f(b.mn[a]) : __int_as_float(0x7fc00000);  // all-NaN axis -> NaN
-    hi[a] = any ? ord2f(b.mx[a]) : __int_as_float(0x7fc00000);
+    const bool any = bd.mn[a] != 0xffffffffu;
+    lo[a] = any ? ord2f(bd.mn[a]) : __int_as_float(0x7fc00000);  // all-NaN axis -> NaN
+    hi[a] = any ? ord2f(bd.mx[a]) : __int_as_float(0x7fc00000);
   }
-  if (has_origin) {
-    pl.origin[0] = ox;
-    pl.origin[1] = oy;
-    pl.origin[2] = oz;
-  } else {
-    for (int a = 0; a < 3; ++a) pl.origin[a] = lo[a];
-  }
-  bool ok = (b.flags & (7u << 3)) == 0;  // an infinite coordinate saturates the key
+  for (int a = 0; a < 3; ++a) pl.origin[a] = prm.has_origin ? prm.origin[a] : lo[a];
+  bool ok = (bd.flags & (7u << 3)) == 0;  // an infinite coordinate saturates the key
   uint32_t total = 0;
   for (int a = 0; a < 3; ++a) {
     int64_t k0 = voxel_axis_key(lo[a], pl.origin[a], pl.inv_leaf, pl.floor_mode);
     int64_t k1 = voxel_axis_key(hi[a], pl.origin[a], pl.inv_leaf, pl.floor_mode);
     if (isnan(lo[a])) k0 = k1 = 0;
-    if (b.flags & (1u << a)) {  // NaN coordinates get key 0 (saturating cast)
+    if (bd.flags & (1u << a)) {  // NaN coordinates get key 0 (saturating cast)
       k0 = min(k0, int64_t(0));
       k1 = max(k1, int64_t(0));
     }
@@ -133,27 +200,38 @@ __global__ void k_voxel_plan(Control *ctl, float leaf, int has_origin, float ox,
   pl.shift_x = pl.bits[1] + pl.bits[2];
   pl.total_bits = total;
   pl.num_digits = total == 0 ? 1u : (total + RADIX_BITS - 1) / RADIX_BITS;
-  if (total > 64) ok = false;
+  if (total + ctl->cloud_bits > 64) ok = false;
   if (ctl->n_points > LB_MAX_COUNT) {
     atomicOr(&ctl->status, ST_TOO_MANY_POINTS);
     ok = false;
   }
   pl.valid = ok ? 1u : 0u;
-  ctl->vplan = pl;
+  bt.vplans[b] = pl;
+  atomicMax(&ctl->vkey_bits, total);
   if (!ok) atomicOr(&ctl->status, ST_KEY_OVERFLOW);
 }
 
-// Key source for the voxel sort: packs the reference's voxel key of point i.
+// Key source for the voxel sort: the reference's voxel key of point i,
+// packed, with its cloud id above the per-cloud key bits.
 struct VoxelKeySrc {
   const float *x, *y, *z;
-  VoxelPlan pl;
-  __device__ __forceinline__ void prepare(const Control *ctl) { pl = ctl->vplan; }
+  Batch bt;
+  VoxelPlan pl;  // the plan when there is one cloud
+  uint32_t local_bits;
+  uint32_t cloud_bits;
+  __device__ __forceinline__ void prepare(const Control *ctl) {
+    local_bits = ctl->vkey_bits;
+    cloud_bits = ctl->cloud_bits;
+    if (bt.clouds == 1) pl = bt.vplans[0];
+  }
   __device__ __forceinline__ uint32_t count(const Control *ctl) const {
     return uint32_t(ctl->n_points);
   }
-  __device__ __forceinline__ uint32_t key_bits() const { return pl.total_bits; }
+  __device__ __forceinline__ uint32_t key_bits() const { return local_bits + cloud_bits; }
   __device__ __forceinline__ uint64_t key(uint32_t i) const {
-    return voxel_pack(pl, x[i], y[i], z[i]);
+    if (bt.clouds == 1) return voxel_pack(pl, x[i], y[i], z[i]);
+    const uint32_t b = cloud_of(bt, i);
+    return with_cloud(voxel_pack(bt.vplans[b], x[i], y[i], z[i]), b, local_bits);
   }
 };
 
@@ -375,18 +453,44 @@ inline cudaError_t configure_segment_kernels() {
 }
 
 // Unpacks packed voxel keys into the reference's (ix, iy, iz) int64 triples.
-__global__ void k_unpack_voxel_keys(const Control *ctl, const uint64_t *packed, int64_t *out) {
+__global__ void k_unpack_voxel_keys(const Control *ctl, const uint64_t *packed, int64_t *out,
+                                    Batch bt) {
   if (ctl->status) return;
-  const VoxelPlan pl = ctl->vplan;
   const uint64_t v = ctl->n_voxels;
+  const uint32_t lb = ctl->vkey_bits;
+  const uint64_t mask = lb >= 64 ? ~0ull : ((1ull << lb) - 1);
   for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < v;
        i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t key = packed[i];
+    const uint32_t b = lb >= 64 ? 0u : uint32_t(key >> lb);
     int64_t k[3];
-    voxel_unpack(pl, packed[i], k);
+    voxel_unpack(bt.vplans[b < bt.clouds ? b : 0], key & mask, k);
     out[3 * i] = k[0];
     out[3 * i + 1] = k[1];
     out[3 * i + 2] = k[2];
   }
+}
+
+// Voxel range of every cloud in the key-ordered output: voxel_offsets[b] is
+// the first voxel whose key carries cloud id >= b (binary search).
+__global__ void k_voxel_offsets(const Control *ctl, const uint64_t *packed, Batch bt) {
+  if (ctl->status) return;
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > bt.clouds) return;
+  const uint64_t v = ctl->n_voxels;
+  const uint32_t lb = ctl->vkey_bits;
+  uint64_t lo = 0, hi = v;
+  if (b == 0) hi = 0;
+  else if (b == bt.clouds) lo = v;
+  else {
+    const uint64_t target = uint64_t(b) << lb;  // lb < 64 whenever there are 2+ clouds
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (packed[mid] < target) lo = mid + 1;
+      else hi = mid;
+    }
+  }
+  bt.voxel_offsets[b] = uint32_t(lo);
 }
 
 }  // namespace srcu
