@@ -418,14 +418,11 @@ def run_batched(args, torch, dev, stream):
                plain_mpts=n / ms_plain / 1e3, batched_mpts=n / ms_batched / 1e3,
                speedup=ms_plain / ms_batched)
     try:  # the same batched chain replayed from a CUDA graph
-        g = torch.cuda.CUDAGraph()
-        torch.cuda.synchronize()
-        with torch.cuda.graph(g, stream=stream):
-            batched()
-        ms_graph = timed(g.replay, 3)
+        g = ctx.chain_graph(allc, leaves.tolist(), radii.tolist(), offsets=offsets, viewpoints=vps)
+        ms_graph = timed(g.launch, 3)
         out.update(graph_ms=ms_graph, graph_mpts=n / ms_graph / 1e3, graph_speedup=ms_plain / ms_graph)
-        del g
-    except Exception as e:  # capture support depends on the driver
+        g.close()
+    except Exception as e:
         out["graph_error"] = str(e)[:200]
     ctx.frame_check()
     ctx.close()

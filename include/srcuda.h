@@ -190,6 +190,23 @@ srcu_status srcu_batch_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *po
 /* Synchronises and copies the count + 1 voxel offsets of the last batch. */
 srcu_status srcu_batch_voxel_offsets(srcu_ctx *ctx, uint64_t *voxel_offsets);
 
+/* ---- CUDA graphs ---------------------------------------------------------- */
+
+typedef struct srcu_graph srcu_graph;
+
+/* Captures the voxel -> normals chain for these exact inputs (a batch when
+ * offsets is non-NULL, else one cloud) as a CUDA graph on the context
+ * stream.  Runs the chain once uncaptured first (sizing buffers and staging
+ * parameters), then captures only the kernels.  Replays read the same input
+ * pointers and write the context's result buffers; the context must not run
+ * other chains while the graph is in use. */
+srcu_status srcu_chain_graph_create(srcu_ctx *ctx, const srcu_cloud *points,
+                                    const uint64_t *offsets, uint32_t count,
+                                    const srcu_voxel_params *vparams,
+                                    const srcu_normal_params *nparams, srcu_graph **out);
+srcu_status srcu_graph_launch(srcu_ctx *ctx, srcu_graph *graph);
+void srcu_graph_destroy(srcu_graph *graph);
+
 /* ---- device-resident chain (GpuSpatialFrame, gpu_frame.rs:71-365) --------- */
 
 /* Enqueues the voxel -> normals chain on the context stream for a cloud

@@ -164,6 +164,12 @@ SIGNATURES = {
                                           ctypes.c_uint32, ctypes.POINTER(SrcuVoxelParams),
                                           ctypes.POINTER(SrcuNormalParams)], ctypes.c_int),
     "srcu_batch_voxel_offsets": ([_P, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+    "srcu_chain_graph_create": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(ctypes.c_uint64),
+                                 ctypes.c_uint32, ctypes.POINTER(SrcuVoxelParams),
+                                 ctypes.POINTER(SrcuNormalParams), ctypes.POINTER(ctypes.c_void_p)],
+                                ctypes.c_int),
+    "srcu_graph_launch": ([_P, _P], ctypes.c_int),
+    "srcu_graph_destroy": ([_P], None),
     "srcu_profile_enable": ([_P, ctypes.c_uint64], ctypes.c_int),
     "srcu_voxel_centroid_noalloc": ([ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuVoxelParams),
                                      ctypes.POINTER(SrcuVoxelOut), ctypes.POINTER(ctypes.c_uint64),
@@ -424,6 +430,21 @@ class Context:
                                                                count, vps, nps))
         self._last_batch = count
 
+    def chain_graph(self, points: SrcuCloud, leaves, radii, offsets=None, min_neighbors=3,
+                    viewpoints=None, count_shell=False) -> "ChainGraph":
+        """Captures the chain (a batch when offsets is given) as a CUDA graph."""
+        count = len(offsets) - 1 if offsets is not None else 1
+        offs = (ctypes.c_uint64 * (count + 1))(*[int(o) for o in offsets]) if offsets is not None else None
+        vps = (SrcuVoxelParams * count)(*[_voxel_params(leaves[b], None) for b in range(count)])
+        nps = (SrcuNormalParams * count)(*[
+            _normal_params(radii[b], min_neighbors, None if viewpoints is None else viewpoints[b],
+                           False, count_shell) for b in range(count)])
+        h = ctypes.c_void_p()
+        self._check(self._lib.srcu_chain_graph_create(self._h, ctypes.byref(points), offs, count, vps,
+                                                      nps, ctypes.byref(h)))
+        self._last_batch = count
+        return ChainGraph(self, h)
+
     def batch_voxel_offsets(self) -> np.ndarray:
         count = getattr(self, "_last_batch", 1)
         out = (ctypes.c_uint64 * (count + 1))()
@@ -460,6 +481,28 @@ class Context:
         return dict(columns=[c[:v] for c in vcols], counts=counts[:v], nx=nouts[0][:v],
                     ny=nouts[1][:v], nz=nouts[2][:v], curvature=nouts[3][:v],
                     neighbor_counts=ncounts[:v], stats=_stats(stats))
+
+
+class ChainGraph:
+    """A captured voxel -> normals chain (srcu_chain_graph_create)."""
+
+    def __init__(self, ctx: Context, handle: ctypes.c_void_p):
+        self._ctx = ctx
+        self._h = handle
+
+    def launch(self):
+        self._ctx._check(self._ctx._lib.srcu_graph_launch(self._ctx.handle, self._h))
+
+    def close(self):
+        if self._h:
+            self._ctx._lib.srcu_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _voxel_params(leaf, origin) -> SrcuVoxelParams:

@@ -811,10 +811,9 @@ srcu_status srcu_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
   return SRCU_OK;
 }
 
-srcu_status srcu_batch_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *points,
-                                             const uint64_t *offsets, uint32_t count,
-                                             const srcu_voxel_params *vparams,
-                                             const srcu_normal_params *nparams) {
+static srcu_status batch_enqueue(srcu_ctx *ctx, const srcu_cloud *points, const uint64_t *offsets,
+                                 uint32_t count, const srcu_voxel_params *vparams,
+                                 const srcu_normal_params *nparams, bool stage) {
   if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
   ST_TRY(check_cloud(ctx, points));
   if (!points->on_device)
@@ -836,7 +835,7 @@ srcu_status srcu_batch_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *po
   ST_TRY(reserve_batch(ctx, count));
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, points, cols));
-  ST_TRY(stage_batch(ctx, count, offsets, vparams, nparams));
+  if (stage) ST_TRY(stage_batch(ctx, count, offsets, vparams, nparams));
   const Batch bt = make_batch(ctx, count);
   begin_chain(ctx, n, bt, 0, nullptr, nullptr);
   if (n > 0) {
@@ -848,6 +847,77 @@ srcu_status srcu_batch_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *po
   ctx->last_attrs = points->n_attrs;
   CU_TRY(cudaGetLastError());
   return SRCU_OK;
+}
+
+srcu_status srcu_batch_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *points,
+                                             const uint64_t *offsets, uint32_t count,
+                                             const srcu_voxel_params *vparams,
+                                             const srcu_normal_params *nparams) {
+  return batch_enqueue(ctx, points, offsets, count, vparams, nparams, true);
+}
+
+struct srcu_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint32_t clouds = 1;
+  uint32_t attrs = 0;
+};
+
+srcu_status srcu_chain_graph_create(srcu_ctx *ctx, const srcu_cloud *points,
+                                    const uint64_t *offsets, uint32_t count,
+                                    const srcu_voxel_params *vparams,
+                                    const srcu_normal_params *nparams, srcu_graph **out) {
+  if (!ctx || !out) return SRCU_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (ctx->stream == ctx->own_stream || ctx->stream == nullptr) {
+    // capture needs a stream; the context's own stream is fine
+  }
+  const uint64_t single_off[2] = {0, points ? points->n : 0};
+  const uint64_t *off = offsets ? offsets : single_off;
+  const uint32_t cnt = offsets ? count : 1;
+  // 1) one uncaptured run sizes every buffer and stages the parameters
+  ST_TRY(batch_enqueue(ctx, points, off, cnt, vparams, nparams, true));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  ST_TRY(read_control(ctx));
+  // 2) capture the kernels only (the staged parameters stay in the batch arrays)
+  srcu_graph *g = new srcu_graph();
+  g->clouds = cnt;
+  g->attrs = points->n_attrs;
+  const uint64_t mask = ctx->prof_mask;
+  ctx->prof_mask = 0;  // no timing events inside a graph
+  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  srcu_status st = SRCU_OK;
+  if (e == cudaSuccess) {
+    st = batch_enqueue(ctx, points, off, cnt, vparams, nparams, false);
+    e = cudaStreamEndCapture(ctx->stream, &g->graph);
+  }
+  ctx->prof_mask = mask;
+  if (e == cudaSuccess && st == SRCU_OK) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (e != cudaSuccess || st != SRCU_OK) {
+    cudaGetLastError();
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    if (st != SRCU_OK) return st;
+    return fail(ctx, SRCU_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  }
+  *out = g;
+  return SRCU_OK;
+}
+
+srcu_status srcu_graph_launch(srcu_ctx *ctx, srcu_graph *g) {
+  if (!ctx || !g) return SRCU_ERR_INVALID_ARGUMENT;
+  CU_TRY(cudaGraphLaunch(g->exec, ctx->stream));
+  ctx->last_clouds = g->clouds;
+  ctx->last_attrs = g->attrs;
+  return SRCU_OK;
+}
+
+void srcu_graph_destroy(srcu_graph *g) {
+  if (!g) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
 }
 
 srcu_status srcu_batch_voxel_offsets(srcu_ctx *ctx, uint64_t *voxel_offsets) {

@@ -97,3 +97,39 @@ def test_batch_rejects_bad_offsets(cuda_ctx):
         cuda_ctx.batch_voxel_normals_enqueue(pts, [0, 500], [1.0], [2.0])
     with pytest.raises(_native.InvalidArgument):
         cuda_ctx.batch_voxel_normals_enqueue(pts, [0, 600, 500, 1000], [1.0] * 3, [2.0] * 3)
+
+
+def test_chain_graph_replays_match_enqueue():
+    import torch
+    ctx = _native.Context(0)
+    clouds = [synthetic.georef_scan(20_000, seed=21), synthetic.georef_scan(7_000, seed=22)]
+    leaves, radii = [0.1, 0.2], [0.5, 1.0]
+    dev, offsets = device_concat(torch, clouds)
+    keep = _native._Keep()
+    pts = _native.make_cloud(dev[0], dev[1], dev[2], [dev[3]], keep)
+    n = int(offsets[-1])
+    ctx.batch_voxel_normals_enqueue(pts, offsets, leaves, radii, count_shell=False)
+    ref = ctx.frame_fetch(n, n_attrs=1)
+    ref_off = ctx.batch_voxel_offsets()
+    g = ctx.chain_graph(pts, leaves, radii, offsets=offsets)
+    for _ in range(3):
+        g.launch()
+    got = ctx.frame_fetch(n, n_attrs=1)
+    assert np.array_equal(ctx.batch_voxel_offsets(), ref_off)
+    for a, b in zip(got["columns"], ref["columns"]):
+        assert np.array_equal(a, b)
+    for k in ("nx", "nz", "curvature", "neighbor_counts"):
+        assert np.array_equal(got[k], ref[k], equal_nan=True)
+    g.close()
+    # single cloud
+    single = _native.make_cloud(dev[0][:clouds[0].n], dev[1][:clouds[0].n], dev[2][:clouds[0].n],
+                                [dev[3][:clouds[0].n]], keep)
+    g1 = ctx.chain_graph(single, [0.1], [0.5])
+    g1.launch()
+    got1 = ctx.frame_fetch(clouds[0].n, n_attrs=1)
+    ref1 = ctx.voxel_normals(clouds[0].x, clouds[0].y, clouds[0].z, [clouds[0].intensity], leaf=0.1,
+                             radius=0.5)
+    assert np.array_equal(got1["columns"][0], ref1["columns"][0])
+    assert np.array_equal(got1["nx"], ref1["nx"], equal_nan=True)
+    g1.close()
+    ctx.close()
