@@ -56,6 +56,11 @@ def parse():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the many-clouds (batched vs per-cloud loop) measurement")
     ap.add_argument("--batched-clouds", type=int, default=256)
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the serving-loop (Poisson arrivals) measurement")
+    ap.add_argument("--serving-rates", default="100,500,1000,2000",
+                    help="offered request rates (req/s) of the serving measurement")
+    ap.add_argument("--serving-seconds", type=float, default=2.0)
     return ap.parse_args()
 
 
@@ -357,6 +362,8 @@ def run_gpu(args):
     )
     if not args.no_batched:
         line["batched"] = run_batched(args, torch, dev, stream)
+    if not args.no_serving:
+        line["serving"] = run_serving(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cloud)
     if world > 1:
@@ -426,6 +433,107 @@ def run_batched(args, torch, dev, stream):
         out["graph_error"] = str(e)[:200]
     ctx.frame_check()
     ctx.close()
+    return out
+
+
+def run_serving(args, device):
+    """The serving loop (srcu_server_*) under open-loop Poisson arrivals.
+
+    Requests: spinning-LiDAR frames (64 beams x 2048 azimuths = 131,072
+    points, ray-cast against ground + 100 boxes, max range 120 m, N(0, 0.02)
+    range noise) and, with probability 0.1, map chunks of 1-4M points (the
+    scan mixture); each runs voxel 0.2 m -> radius normals 0.6 m.  Frames and
+    chunks arrive as two independent Poisson streams (0.9 and 0.1 of the
+    offered rate, i.e. one Poisson stream whose requests are chunks with
+    probability 0.1), each submitted by its own host thread; a third thread
+    polls results.  Latency = submit -> results in pinned host memory."""
+    import threading
+
+    from spatialrust_b200 import _native, synthetic
+    scene = synthetic.lidar_scene(seed=4)
+    frames = [synthetic.lidar_frame(seed=i, scene=scene) for i in range(4)]
+    chunks = [synthetic.map_chunk(n, seed=50 + i)
+              for i, n in enumerate((1_000_000, 2_500_000, 4_000_000))]
+    srv = _native.Server(device, hbm_budget_bytes=40 << 30)
+    leaf, radius = 0.2, 0.6
+    next_id = [0]
+    id_lock = threading.Lock()
+
+    def submit(c):
+        with id_lock:
+            rid = next_id[0]
+            next_id[0] += 1
+        while not srv.submit(rid, c.x, c.y, c.z, c.intensity, leaf=leaf, radius=radius):
+            time.sleep(0.0005)  # queue full: back off (counted as rejected by the server)
+
+    def drain(count):
+        got = 0
+        while got < count:
+            if srv.poll(wait_us=5000, fetch=False) is not None:
+                got += 1
+
+    # warm-up: every frame and chunk once, then a short burst
+    for c in frames + chunks:
+        submit(c)
+    drain(len(frames) + len(chunks))
+    out = dict(workload="LiDAR frames 64x2048 (131,072 pts) + 10% map chunks 1M/2.5M/4M pts; "
+                        "voxel 0.2 m -> normals r 0.6 m; Poisson arrivals; HBM budget 40 GB; "
+                        "3 batch slots (<= 1M pts per batched chain) + 1 bulk slot",
+               rates=[])
+    for rate in [float(r) for r in args.serving_rates.split(",") if r]:
+        srv.reset_stats()
+        done = threading.Event()
+        counts = {"frames": 0, "chunks": 0, "points": 0}
+
+        def stream_of(pool, share, key, seed):
+            rng = np.random.default_rng(seed)
+            t_next = time.perf_counter()
+            end = t_next + args.serving_seconds
+            k = 0
+            while True:
+                t_next += rng.exponential(1.0 / (rate * share))
+                if t_next >= end:
+                    break
+                while True:
+                    dt = t_next - time.perf_counter()
+                    if dt <= 0:
+                        break
+                    time.sleep(dt if dt > 0.002 else 0)
+                c = pool[k % len(pool)]
+                k += 1
+                submit(c)
+                counts[key] += 1
+                counts["points"] += c.n
+
+        t0 = time.perf_counter()
+        ths = [threading.Thread(target=stream_of, args=(frames, 0.9, "frames", int(rate))),
+               threading.Thread(target=stream_of, args=(chunks, 0.1, "chunks", int(rate) + 7))]
+        for t in ths:
+            t.start()
+        poller_count = [0]
+
+        def poller():
+            while not (done.is_set() and poller_count[0] >= counts["frames"] + counts["chunks"]):
+                if srv.poll(wait_us=2000, fetch=False) is not None:
+                    poller_count[0] += 1
+
+        pt = threading.Thread(target=poller)
+        pt.start()
+        for t in ths:
+            t.join()
+        done.set()
+        pt.join()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        n_req = counts["frames"] + counts["chunks"]
+        out["rates"].append(dict(
+            offered_req_s=rate, requests=n_req, frames=counts["frames"], chunks=counts["chunks"],
+            achieved_req_s=n_req / wall, mpts_s=counts["points"] / wall / 1e6,
+            frame_p50_ms=st["frame_p50_ms"], frame_p99_ms=st["frame_p99_ms"],
+            chunk_p50_ms=st["bulk_p50_ms"], chunk_p99_ms=st["bulk_p99_ms"],
+            all_p50_ms=st["all_p50_ms"], all_p99_ms=st["all_p99_ms"], batches=st["batches"],
+            rejected_submits=st["rejected"], failed=st["failed"], wall_s=wall))
+    srv.close()
     return out
 
 

@@ -251,6 +251,68 @@ srcu_status srcu_chain_info_get(srcu_ctx *ctx, srcu_chain_info *info);
 srcu_status srcu_frame_fetch(srcu_ctx *ctx, const srcu_voxel_out *vout, const srcu_normal_out *nout,
                              uint64_t *out_voxels, srcu_normal_stats *stats);
 
+/* ---- serving loop ------------------------------------------------------------ */
+
+/* A request loop that admits frames and map chunks of different sizes as they
+ * arrive and runs voxel -> normals on them with continuous batching: small
+ * requests waiting when a batch slot frees up are packed into one batched
+ * chain (srcu_batch_voxel_normals_enqueue) on that slot's stream, large
+ * requests run on their own slots so they never hold small ones back, and
+ * several slots overlap on the device.  Admission is gated by the pending
+ * queue (max_pending_points) and by the HBM budget that sizes the slots.
+ * One worker thread owns all device work; submit / poll / release may be
+ * called from any threads. */
+typedef struct srcu_server srcu_server;
+
+typedef struct srcu_server_config {
+  int device;
+  uint64_t hbm_budget_bytes;      /* device memory for all slots (0: 40 GB) */
+  uint32_t frame_slots;           /* concurrent batches of small requests (0: 3) */
+  uint32_t bulk_slots;            /* concurrent large requests (0: 1) */
+  uint64_t frame_batch_points;    /* most points packed into one small-request batch (0: 1M) */
+  uint64_t bulk_threshold_points; /* requests with at least this many points use bulk slots (0: 500k) */
+  uint64_t bulk_max_points;       /* largest admissible request (0: 4.5M) */
+  uint64_t max_pending_points;    /* beyond this queued total, submit returns SRCU_ERR_BUSY (0: 64M) */
+  uint64_t host_arena_bytes;      /* pinned host memory for queued inputs and unreleased
+                                     results; submit returns SRCU_ERR_BUSY when full (0: 2 GB) */
+} srcu_server_config;
+
+typedef struct srcu_request_result {
+  uint64_t req_id;
+  srcu_status status;
+  uint64_t points;
+  uint64_t voxels;
+  const float *x, *y, *z, *intensity;      /* centroids (intensity NULL without it) */
+  const float *nx, *ny, *nz, *curvature;  /* normals of each centroid */
+  const uint32_t *counts;                 /* points per voxel */
+  double latency_ms;                      /* submit -> results ready */
+} srcu_request_result;
+
+typedef struct srcu_server_stats {
+  uint64_t submitted, rejected, completed, failed, batches, points;
+  double frame_p50_ms, frame_p99_ms;      /* requests below bulk_threshold_points */
+  double bulk_p50_ms, bulk_p99_ms;        /* the others */
+  double all_p50_ms, all_p99_ms;
+  double elapsed_s;                       /* since the first submit */
+} srcu_server_stats;
+
+srcu_status srcu_server_create(const srcu_server_config *config, srcu_server **out);
+void srcu_server_destroy(srcu_server *server);
+/* Copies the request (host columns: x, y, z and at most one attribute) into
+ * pinned memory and queues it.  SRCU_ERR_BUSY: the queue or the pinned arena
+ * is full -- retry later. */
+srcu_status srcu_server_submit(srcu_server *server, uint64_t req_id, const srcu_cloud *cloud,
+                               const srcu_voxel_params *vparams,
+                               const srcu_normal_params *nparams);
+/* Returns one finished request, waiting up to wait_us; SRCU_ERR_BUSY if
+ * none.  Its result columns live in the pinned arena until
+ * srcu_server_release(req_id); unreleased results hold arena space. */
+srcu_status srcu_server_poll(srcu_server *server, srcu_request_result *out, uint32_t wait_us);
+srcu_status srcu_server_release(srcu_server *server, uint64_t req_id);
+srcu_status srcu_server_stats_get(srcu_server *server, srcu_server_stats *stats);
+/* Discards the latency history (e.g. after a warm-up phase). */
+srcu_status srcu_server_stats_reset(srcu_server *server);
+
 /* ---- launch accounting and kernel timing ---------------------------------- */
 
 /* Kernel groups of the chain, in launch order. */

@@ -126,6 +126,30 @@ class SrcuKernelStat(ctypes.Structure):
                 ("timed_regions", ctypes.c_uint64), ("total_ms", ctypes.c_double)]
 
 
+class SrcuServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_uint64),
+                ("frame_slots", ctypes.c_uint32), ("bulk_slots", ctypes.c_uint32),
+                ("frame_batch_points", ctypes.c_uint64), ("bulk_threshold_points", ctypes.c_uint64),
+                ("bulk_max_points", ctypes.c_uint64), ("max_pending_points", ctypes.c_uint64),
+                ("host_arena_bytes", ctypes.c_uint64)]
+
+
+class SrcuRequestResult(ctypes.Structure):
+    _fields_ = [("req_id", ctypes.c_uint64), ("status", ctypes.c_int), ("points", ctypes.c_uint64),
+                ("voxels", ctypes.c_uint64), ("x", ctypes.c_void_p), ("y", ctypes.c_void_p),
+                ("z", ctypes.c_void_p), ("intensity", ctypes.c_void_p), ("nx", ctypes.c_void_p),
+                ("ny", ctypes.c_void_p), ("nz", ctypes.c_void_p), ("curvature", ctypes.c_void_p),
+                ("counts", ctypes.c_void_p), ("latency_ms", ctypes.c_double)]
+
+
+class SrcuServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in
+                ("submitted", "rejected", "completed", "failed", "batches", "points")] + [
+                (k, ctypes.c_double) for k in
+                ("frame_p50_ms", "frame_p99_ms", "bulk_p50_ms", "bulk_p99_ms", "all_p50_ms",
+                 "all_p99_ms", "elapsed_s")]
+
+
 KERNEL_IDS = ["begin", "bounds", "voxel_plan", "voxel_hist", "voxel_sort", "voxel_segments",
               "unpack_keys", "cell_plan", "cell_hist", "cell_sort", "cells", "hash", "ranges",
               "normals"]
@@ -176,6 +200,16 @@ SIGNATURES = {
                                      _P], ctypes.c_int),
     "srcu_profile_read": ([_P, ctypes.POINTER(SrcuKernelStat), ctypes.c_int, ctypes.c_int],
                           ctypes.c_int),
+    "srcu_server_create": ([ctypes.POINTER(SrcuServerConfig), ctypes.POINTER(ctypes.c_void_p)],
+                           ctypes.c_int),
+    "srcu_server_destroy": ([_P], None),
+    "srcu_server_submit": ([_P, ctypes.c_uint64, ctypes.POINTER(SrcuCloud),
+                            ctypes.POINTER(SrcuVoxelParams), ctypes.POINTER(SrcuNormalParams)],
+                           ctypes.c_int),
+    "srcu_server_poll": ([_P, ctypes.POINTER(SrcuRequestResult), ctypes.c_uint32], ctypes.c_int),
+    "srcu_server_release": ([_P, ctypes.c_uint64], ctypes.c_int),
+    "srcu_server_stats_get": ([_P, ctypes.POINTER(SrcuServerStats)], ctypes.c_int),
+    "srcu_server_stats_reset": ([_P], ctypes.c_int),
 }
 
 _lib = None
@@ -503,6 +537,92 @@ class ChainGraph:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """The continuous-batching request loop (srcu_server_*): frames and map
+    chunks are submitted from host memory, run as voxel -> normals chains
+    (small requests packed into batched chains, large ones on bulk slots) and
+    polled back with their latency."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, frame_slots: int = 0,
+                 bulk_slots: int = 0, frame_batch_points: int = 0, bulk_threshold_points: int = 0,
+                 bulk_max_points: int = 0, max_pending_points: int = 0, host_arena_bytes: int = 0):
+        self._lib = load()
+        cfg = SrcuServerConfig(device, hbm_budget_bytes, frame_slots, bulk_slots, frame_batch_points,
+                               bulk_threshold_points, bulk_max_points, max_pending_points,
+                               host_arena_bytes)
+        h = ctypes.c_void_p()
+        st = self._lib.srcu_server_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != SRCU_OK:
+            _raise(st, f"srcu_server_create(device={device}) failed")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.srcu_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, req_id: int, x, y, z, intensity=None, *, leaf: float, radius: float,
+               min_neighbors: int = 3, viewpoint=None, origin=None, include_self: bool = False,
+               count_shell: bool = False) -> bool:
+        """Queues one request; False when the pending queue is full (retry later)."""
+        keep = _Keep()
+        cloud = make_cloud(x, y, z, [] if intensity is None else [intensity], keep)
+        vp = _voxel_params(leaf, origin)
+        np_ = _normal_params(radius, min_neighbors, viewpoint, include_self, count_shell)
+        st = self._lib.srcu_server_submit(self._h, int(req_id), ctypes.byref(cloud), ctypes.byref(vp),
+                                          ctypes.byref(np_))
+        if st == SRCU_ERR_BUSY:
+            return False
+        if st != SRCU_OK:
+            _raise(st, f"srcu_server_submit(req_id={req_id}) failed")
+        return True
+
+    def poll(self, wait_us: int = 0, fetch: bool = True) -> dict | None:
+        """One finished request (its columns copied out when fetch, then
+        released), or None."""
+        r = SrcuRequestResult()
+        st = self._lib.srcu_server_poll(self._h, ctypes.byref(r), int(wait_us))
+        if st == SRCU_ERR_BUSY:
+            return None
+        if st != SRCU_OK:
+            _raise(st, "srcu_server_poll failed")
+        v = int(r.voxels)
+        if not fetch:
+            self._lib.srcu_server_release(self._h, r.req_id)
+            return dict(req_id=int(r.req_id), status=int(r.status), points=int(r.points), voxels=v,
+                        latency_ms=float(r.latency_ms))
+
+        def col(ptr, ctype, dtype):
+            if not ptr or v == 0:
+                return np.zeros(0, dtype=dtype)
+            return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctype)), (v,)).copy()
+
+        out = dict(req_id=int(r.req_id), status=int(r.status), points=int(r.points), voxels=v,
+                   latency_ms=float(r.latency_ms))
+        for k in ("x", "y", "z", "nx", "ny", "nz", "curvature"):
+            out[k] = col(getattr(r, k), ctypes.c_float, np.float32)
+        out["intensity"] = col(r.intensity, ctypes.c_float, np.float32) if r.intensity else None
+        out["counts"] = col(r.counts, ctypes.c_uint32, np.uint32)
+        self._lib.srcu_server_release(self._h, r.req_id)
+        return out
+
+    def stats(self) -> dict:
+        s = SrcuServerStats()
+        st = self._lib.srcu_server_stats_get(self._h, ctypes.byref(s))
+        if st != SRCU_OK:
+            _raise(st, "srcu_server_stats_get failed")
+        return {k: getattr(s, k) for k, _ in SrcuServerStats._fields_}
+
+    def reset_stats(self):
+        self._lib.srcu_server_stats_reset(self._h)
 
 
 def _voxel_params(leaf, origin) -> SrcuVoxelParams:

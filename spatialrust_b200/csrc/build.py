@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libsrcuda.so")
-SOURCES = [os.path.join(HERE, "srcuda.cu")]
+SOURCES = [os.path.join(HERE, "srcuda.cu"), os.path.join(HERE, "server.cu")]
 HEADERS = [os.path.join(HERE, f) for f in os.listdir(HERE) if f.endswith((".cuh", "noalloc.cu"))] + [
     os.path.join(ROOT, "include", "srcuda.h")]
 
@@ -24,6 +24,7 @@ NVCC_FLAGS = [
     "-prec-div=true", "-prec-sqrt=true", "-fmad=true",
     "-Xcompiler", "-fPIC", "-shared",
     "-I", os.path.join(ROOT, "include"),
+    "-lpthread",
 ]
 
 

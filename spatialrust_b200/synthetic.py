@@ -177,6 +177,62 @@ def batched_uneven(count: int = 256, lo: int = 10_000, hi: int = 1_000_000, seed
     return clouds, leaves, (leaves * np.float32(5.0)).astype(np.float32)
 
 
+def lidar_scene(seed: int = 4, n_boxes: int = 100, extent: float = 120.0):
+    """Seeded scene for ray-cast LiDAR frames: the ground plane z = 0 plus
+    n_boxes axis-aligned boxes (sides U[0.5, 8] m, standing on the ground,
+    centres uniform within +-extent m).  Returns (lo, hi) box corners."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.uniform(0.5, 8.0, (n_boxes, 3))
+    centers = np.stack([rng.uniform(-extent, extent, n_boxes), rng.uniform(-extent, extent, n_boxes),
+                        sizes[:, 2] / 2.0], axis=1)
+    return centers - sizes / 2.0, centers + sizes / 2.0
+
+
+def lidar_frame(seed: int = 0, scene=None, beams: int = 64, azimuths: int = 2048,
+                elev_deg=(-25.0, 15.0), max_range: float = 120.0, noise: float = 0.02,
+                sensor_height: float = 1.8) -> Cloud:
+    """One spinning-LiDAR frame (beams x azimuths points, sensor frame): each
+    ray's range is its first hit on the scene (ground or box, slab test), or
+    max_range when nothing is hit, plus N(0, noise) range noise, clipped to
+    (0, max_range]; intensity U[0, 1).  The sensor sits at a seeded position
+    and yaw, sensor_height m above the ground, outside every box."""
+    lo, hi = scene if scene is not None else lidar_scene()
+    rng = np.random.default_rng(seed)
+    for _ in range(1000):
+        pos = np.array([rng.uniform(-60, 60), rng.uniform(-60, 60), sensor_height])
+        if not np.any(np.all((pos >= lo - 0.5) & (pos <= hi + 0.5), axis=1)):
+            break
+    yaw = rng.uniform(0.0, 2.0 * np.pi)
+    el = np.deg2rad(np.linspace(elev_deg[0], elev_deg[1], beams))
+    az = yaw + np.arange(azimuths) * (2.0 * np.pi / azimuths)
+    ce, se = np.cos(el)[:, None], np.sin(el)[:, None]
+    d = np.stack([np.broadcast_to(ce * np.cos(az), (beams, azimuths)),
+                  np.broadcast_to(ce * np.sin(az), (beams, azimuths)),
+                  np.broadcast_to(se, (beams, azimuths))], axis=-1).reshape(-1, 3)
+    t = np.full(d.shape[0], max_range)
+    down = d[:, 2] < -1e-9
+    t[down] = np.minimum(t[down], -pos[2] / d[down, 2])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = 1.0 / d
+        for b in range(lo.shape[0]):
+            t1 = (lo[b] - pos) * inv
+            t2 = (hi[b] - pos) * inv
+            tn = np.nanmax(np.minimum(t1, t2), axis=1)
+            tf = np.nanmin(np.maximum(t1, t2), axis=1)
+            hit = (tn <= tf) & (tn > 0.0) & (tn < t)
+            t[hit] = tn[hit]
+    r = np.clip(t + rng.normal(0.0, noise, t.shape[0]), 1e-3, max_range)
+    pts = (d * r[:, None]).astype(np.float32)
+    inten = rng.random(pts.shape[0], dtype=np.float32)
+    return Cloud(np.ascontiguousarray(pts[:, 0]), np.ascontiguousarray(pts[:, 1]),
+                 np.ascontiguousarray(pts[:, 2] + np.float32(sensor_height)), inten, np.zeros(3))
+
+
+def map_chunk(n: int, seed: int) -> Cloud:
+    """A map-chunk request: the georeferenced scan mixture with n points."""
+    return georef_scan(n, seed=seed)
+
+
 def unit_plane_grid(nx: int, ny: int, step: float, z: float = 0.0, x0: float = 0.0,
                     y0: float = 0.0) -> Cloud:
     """Regular grid in the plane z = const (the reference's planar test clouds)."""

@@ -52,11 +52,13 @@ def test_struct_layouts_match_c(tmp_path):
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "srcuda.h"\n'
         "int main(void){\n"
-        'printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(srcu_cloud), sizeof(srcu_voxel_params),'
+        'printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(srcu_cloud), sizeof(srcu_voxel_params),'
         " sizeof(srcu_voxel_out), sizeof(srcu_normal_params), sizeof(srcu_normal_out),"
-        " sizeof(srcu_normal_stats), sizeof(srcu_frame_view));\n"
-        'printf("%zu %zu %zu\\n", offsetof(srcu_cloud, n), offsetof(srcu_normal_params, include_self),'
-        " offsetof(srcu_frame_view, n_attrs));\n"
+        " sizeof(srcu_normal_stats), sizeof(srcu_frame_view), sizeof(srcu_server_config),"
+        " sizeof(srcu_request_result), sizeof(srcu_server_stats));\n"
+        'printf("%zu %zu %zu %zu %zu\\n", offsetof(srcu_cloud, n),'
+        " offsetof(srcu_normal_params, include_self), offsetof(srcu_frame_view, n_attrs),"
+        " offsetof(srcu_request_result, points), offsetof(srcu_server_stats, frame_p50_ms));\n"
         "return 0;}\n")
     exe = tmp_path / "sizes"
     subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)])
@@ -65,9 +67,11 @@ def test_struct_layouts_match_c(tmp_path):
     offs = [int(v) for v in lines[1].split()]
     assert sizes == [ctypes.sizeof(t) for t in (
         _native.SrcuCloud, _native.SrcuVoxelParams, _native.SrcuVoxelOut, _native.SrcuNormalParams,
-        _native.SrcuNormalOut, _native.SrcuNormalStats, _native.SrcuFrameView)]
+        _native.SrcuNormalOut, _native.SrcuNormalStats, _native.SrcuFrameView,
+        _native.SrcuServerConfig, _native.SrcuRequestResult, _native.SrcuServerStats)]
     assert offs == [_native.SrcuCloud.n.offset, _native.SrcuNormalParams.include_self.offset,
-                    _native.SrcuFrameView.n_attrs.offset]
+                    _native.SrcuFrameView.n_attrs.offset, _native.SrcuRequestResult.points.offset,
+                    _native.SrcuServerStats.frame_p50_ms.offset]
 
 
 def test_header_compiles_as_c_and_cxx(tmp_path):
@@ -88,3 +92,23 @@ def test_create_without_device_reports_no_device(lib):
     assert st == _native.SRCU_ERR_NO_DEVICE
     assert not h.value
     assert lib.srcu_last_error(None) == b"no context"
+
+
+def test_server_without_device_or_budget(lib):
+    """The serving loop refuses cleanly: slots larger than the HBM budget, bad
+    size relations, and (here) no device."""
+    import torch
+    cfg = _native.SrcuServerConfig()
+    h = ctypes.c_void_p()
+    cfg.hbm_budget_bytes = 1 << 20
+    assert lib.srcu_server_create(ctypes.byref(cfg), ctypes.byref(h)) == _native.SRCU_ERR_OUT_OF_BUDGET
+    cfg.hbm_budget_bytes = 0
+    cfg.bulk_threshold_points = 2_000_000  # above frame_batch_points (1M default)
+    assert (lib.srcu_server_create(ctypes.byref(cfg), ctypes.byref(h))
+            == _native.SRCU_ERR_INVALID_ARGUMENT)
+    assert lib.srcu_server_create(None, None) == _native.SRCU_ERR_INVALID_ARGUMENT
+    if torch.cuda.is_available():
+        return
+    with pytest.raises(_native.NoDevice):
+        _native.Server(0)
+    assert not h.value
