@@ -47,7 +47,7 @@ L2_FLUSH_BYTES = 256 << 20
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the many-clouds (batched vs per-cloud loop) measurement")
     ap.add_argument("--batched-clouds", type=int, default=256)
+    ap.add_argument("--no-shapes", action="store_true",
+                    help="skip the 5M-point shapes radius-normals measurement")
     ap.add_argument("--no-serving", action="store_true",
                     help="skip the serving-loop (Poisson arrivals) measurement")
     ap.add_argument("--serving-rates", default="100,500,1000,2000",
@@ -155,6 +157,25 @@ def run_reference(args):
         e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0),
     )
     print(json.dumps(line), flush=True)
+
+
+# ---- multi-rank plumbing (replicas: no data-path collective) ---------------
+
+def max_over_ranks(x: float, device=None) -> float:
+    """The max of x over all ranks (the job's time is its slowest rank's)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mpts(world: int, points_per_rank: int, ms_per_step: float) -> float:
+    """Whole-job throughput: every rank processes its own replica of the
+    workload each step; the step takes the slowest rank's time."""
+    return world * points_per_rank / (ms_per_step / 1e3) / 1e6
 
 
 # ---- GPU --------------------------------------------------------------------
@@ -324,12 +345,9 @@ def run_gpu(args):
     dom_ms = sum(p[dominant]["total_ms"] for p in prof)
     dom_regions = sum(p[dominant]["timed_regions"] for p in prof)
     dom_bytes = sum(algorithmic_bytes(dominant, info) for info in infos) / len(infos)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = max_over_ranks(total_ms, dev)
     ms_per_step = max_ms / args.steps
-    value = world * N_POINTS / (ms_per_step / 1e3) / 1e6
+    value = job_mpts(world, N_POINTS, ms_per_step)
 
     # end to end through the C ABI with pinned host buffers
     e2e = run_e2e(ctxs[0], cloud, args, torch, dev, stream)
@@ -362,6 +380,8 @@ def run_gpu(args):
     )
     if not args.no_batched:
         line["batched"] = run_batched(args, torch, dev, stream)
+    if not args.no_shapes:
+        line["shapes"] = run_shapes(args, torch, dev, stream)
     if not args.no_serving:
         line["serving"] = run_serving(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -419,11 +439,22 @@ def run_batched(args, torch, dev, stream):
     ms_plain = timed(plain, 2)
     ms_batched = timed(batched, 3)
     voxels = int(ctx.batch_voxel_offsets()[-1])
+    info = ctx.chain_info()
+    # where the batched chain spends its time (an untimed, event-bracketed pass)
+    ctx.profile_read(reset=True)
+    ctx.profile_enable(_native.KERNEL_IDS)
+    batched()
+    torch.cuda.synchronize()
+    prof = ctx.profile_read(reset=True)
+    ctx.profile_enable([])
+    groups = {g: round(p["total_ms"], 3) for g, p in prof.items() if p["total_ms"] > 0}
     out = dict(workload=f"{len(clouds)} clouds, {n} points, log-uniform 10k-1M, leaf 0.05/0.1/0.2, "
                         "r = 5 x leaf", points=n, voxels=voxels,
                plain_ms=ms_plain, batched_ms=ms_batched,
                plain_mpts=n / ms_plain / 1e3, batched_mpts=n / ms_batched / 1e3,
-               speedup=ms_plain / ms_batched)
+               speedup=ms_plain / ms_batched, cells=info["cells"],
+               sort_passes=[info["voxel_sort_passes"], info["cell_sort_passes"]],
+               key_bits=[info["voxel_key_bits"], info["cell_key_bits"]], group_ms=groups)
     try:  # the same batched chain replayed from a CUDA graph
         g = ctx.chain_graph(allc, leaves.tolist(), radii.tolist(), offsets=offsets, viewpoints=vps)
         ms_graph = timed(g.launch, 3)
@@ -434,6 +465,53 @@ def run_batched(args, torch, dev, stream):
     ctx.frame_check()
     ctx.close()
     return out
+
+
+def run_shapes(args, torch, dev, stream):
+    """Radius normals at scale: 5,000,000 points on 50 spheres, 30 planar
+    patches and 20 cylinders with N(0, 0.005) surface noise, r = 0.3 m,
+    uncapped neighbourhoods; device-resident input and output, one
+    srcu_radius_normals call per step.  Reports the neighbour-count
+    distribution the shapes actually give."""
+    from spatialrust_b200 import _native, synthetic
+    lib = _native.load()
+    cloud = synthetic.shapes_scene(5_000_000, seed=2)
+    n = cloud.n
+    cols = [torch.from_numpy(a).to(dev) for a in (cloud.x, cloud.y, cloud.z)]
+    outs = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(4)]
+    counts = torch.empty(n, dtype=torch.int32, device=dev)
+    keep = _native._Keep()
+    dcloud = _native.make_cloud(cols[0], cols[1], cols[2], [], keep)
+    nout = _native.SrcuNormalOut(*[o.data_ptr() for o in outs], counts.data_ptr(), 1)
+    params = _native._normal_params(0.3, 3, None, False, count_shell=True)
+    stats = _native.SrcuNormalStats()
+    ctx = _native.Context(dev.index)
+    ctx.set_stream(stream.cuda_stream)
+
+    def step():
+        ctx._check(lib.srcu_radius_normals(ctx.handle, ctypes.byref(dcloud), ctypes.byref(params),
+                                           ctypes.byref(nout), ctypes.byref(stats)))
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    reps = 5
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    nb = counts.cpu().numpy()
+    pct = np.percentile(nb, [5, 25, 50, 75, 95]).tolist()
+    info = ctx.chain_info()
+    ctx.close()
+    return dict(workload="shapes 5M (spheres/planes/cylinders, noise 0.005), radius normals r 0.3",
+                points=n, ms=ms, mpts_s=n / ms / 1e3, cells=info["cells"],
+                neighbours=dict(mean=float(nb.mean()), p5=pct[0], p25=pct[1], p50=pct[2],
+                                p75=pct[3], p95=pct[4], max=int(nb.max())),
+                stats=_native._stats(stats))
 
 
 def run_serving(args, device):

@@ -197,16 +197,37 @@ __device__ __forceinline__ uint32_t cell_hash(uint64_t key, uint32_t log2cap) {
   return uint32_t((key * 0x9E3779B97F4A7C15ull) >> (64 - log2cap));
 }
 
-__global__ void k_hash_insert(Control *ctl, const uint64_t *cell_key, uint64_t *table,
-                              uint32_t log2cap) {
+// Column of a cell key: the key with its z field cleared, so the cloud id and
+// the x, y fields name the column.  The cells of one column are consecutive
+// in key order, sorted by z.
+__device__ __forceinline__ uint64_t column_mask(const Batch &bt, uint32_t b) {
+  return ~((1ull << bt.cplans[b < bt.clouds ? b : 0].bits[2]) - 1ull);
+}
+
+__device__ __forceinline__ uint32_t cloud_of_key(uint64_t full, const Batch &bt, uint32_t lb) {
+  return (bt.clouds == 1 || lb >= 64) ? 0u : uint32_t(full >> lb);
+}
+
+// Hashes every occupied column to its first cell: one insert per column head
+// (a cell whose predecessor lies in another column).  Slots hold
+// [epoch:32][first cell:32]; the column key itself is read back from
+// cell_key[first], so a slot is 8 bytes and the table never needs clearing.
+__global__ void k_column_insert(Control *ctl, const uint64_t *cell_key, uint64_t *table,
+                                uint32_t log2cap, Batch bt) {
   if (ld_relaxed_u32(&ctl->status)) return;
   const uint64_t u_count = ctl->n_cells;
   const uint32_t epoch = ctl->epoch + EP_CELLS;
+  const uint32_t lb = ctl->ckey_bits;
   const uint32_t mask = (1u << log2cap) - 1u;
   for (uint64_t u = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; u < u_count;
        u += uint64_t(gridDim.x) * blockDim.x) {
-    const uint64_t key = cell_key[u];
-    uint32_t h = cell_hash(key, log2cap);
+    const uint64_t full = cell_key[u];
+    const uint64_t col = full & column_mask(bt, cloud_of_key(full, bt, lb));
+    if (u > 0) {
+      const uint64_t prev = cell_key[u - 1];
+      if ((prev & column_mask(bt, cloud_of_key(prev, bt, lb))) == col) continue;
+    }
+    uint32_t h = cell_hash(col, log2cap);
     const uint64_t mine = (uint64_t(epoch) << 32) | u;
     bool done = false;
     for (uint32_t probe = 0; probe <= mask && !done; ++probe) {
@@ -226,15 +247,18 @@ __global__ void k_hash_insert(Control *ctl, const uint64_t *cell_key, uint64_t *
   }
 }
 
-__device__ __forceinline__ int32_t cell_lookup(const uint64_t *table, const uint64_t *cell_key,
-                                               uint64_t key, uint32_t log2cap, uint32_t epoch) {
+// First cell of column `col` (cloud b), or -1 when the column is empty.
+__device__ __forceinline__ int64_t column_lookup(const uint64_t *table, const uint64_t *cell_key,
+                                                 uint64_t col, uint64_t cmask, uint32_t log2cap,
+                                                 uint32_t epoch) {
   const uint32_t mask = (1u << log2cap) - 1u;
-  uint32_t h = cell_hash(key, log2cap);
+  uint32_t h = cell_hash(col, log2cap);
   for (uint32_t probe = 0; probe <= mask; ++probe) {
     const uint64_t w = table[h];
     if (uint32_t(w >> 32) != epoch) return -1;
-    const uint32_t u = uint32_t(w);
-    if (cell_key[u] == key) return int32_t(u);
+    const uint32_t f = uint32_t(w);
+    // a head of another cloud differs in the cloud bits, which cmask keeps
+    if ((cell_key[f] & cmask) == col) return f;
     h = (h + 1) & mask;
   }
   return -1;
@@ -243,7 +267,10 @@ __device__ __forceinline__ int32_t cell_lookup(const uint64_t *table, const uint
 // For every occupied cell and each of the 3x3 neighbouring columns, the range
 // of cell-sorted points in cells (cx+dx, cy+dy, cz-1 .. cz+1).  Those (at
 // most three) cells are consecutive in key order, so each column is one
-// contiguous range: 9 ranges cover the 27-cell neighbourhood.
+// contiguous range: 9 ranges cover the 27-cell neighbourhood.  The centre
+// column holds the cell itself (its z neighbours are its key-order
+// neighbours); another column is found through the column hash and searched
+// from its first cell by galloping over the sorted cell keys.
 __global__ void k_ranges(Control *ctl, const uint64_t *cell_key, const uint32_t *cell_start,
                          const uint64_t *table, uint32_t log2cap, uint2 *ranges, Batch bt) {
   if (ld_relaxed_u32(&ctl->status)) return;
@@ -256,27 +283,49 @@ __global__ void k_ranges(Control *ctl, const uint64_t *cell_key, const uint32_t 
     const uint64_t u = w / 9;
     const uint32_t col = uint32_t(w - u * 9);
     const uint64_t full = cell_key[u];
-    const uint32_t b = (bt.clouds == 1 || lb >= 64) ? 0u : uint32_t(full >> lb);
+    const uint32_t b = cloud_of_key(full, bt, lb);
     const CellPlan &pl = bt.cplans[b < bt.clouds ? b : 0];
     uint32_t cx, cy, cz;
     cell_unpack(pl, full & local_mask, cx, cy, cz);
     const int64_t nx = int64_t(cx) + int64_t(col / 3) - 1;
     const int64_t ny = int64_t(cy) + int64_t(col % 3) - 1;
     uint2 rg = make_uint2(0, 0);
-    if (nx >= 0 && ny >= 0 && nx < pl.dims[0] && ny < pl.dims[1]) {
-      int32_t first = -1, last = -1;
-      for (int dz = -1; dz <= 1; ++dz) {
-        const int64_t nz = int64_t(cz) + dz;
-        if (nz < 0 || nz >= pl.dims[2]) continue;
-        const uint64_t key = with_cloud(
-            (uint64_t(nx) << pl.shift_x) | (uint64_t(ny) << pl.shift_y) | uint64_t(nz), b, lb);
-        const int32_t f = cell_lookup(table, cell_key, key, log2cap, epoch);
-        if (f >= 0) {
-          if (first < 0) first = f;
-          last = f;
+    if (col == 4) {
+      uint64_t first = u, last = u;
+      if (cz > 0 && u > 0 && cell_key[u - 1] == full - 1) first = u - 1;
+      if (cz + 1 < pl.dims[2] && u + 1 < u_count && cell_key[u + 1] == full + 1) last = u + 1;
+      rg = make_uint2(cell_start[first], cell_start[last + 1]);
+    } else if (nx >= 0 && ny >= 0 && nx < pl.dims[0] && ny < pl.dims[1]) {
+      const uint64_t cmask = column_mask(bt, b);
+      const uint64_t ckey =
+          with_cloud((uint64_t(nx) << pl.shift_x) | (uint64_t(ny) << pl.shift_y), b, lb);
+      const int64_t f = column_lookup(table, cell_key, ckey, cmask, log2cap, epoch);
+      if (f >= 0) {
+        const uint64_t lo_key = ckey | (cz > 0 ? cz - 1 : 0);
+        const uint64_t hi_key = ckey | (cz + 1 < pl.dims[2] ? cz + 1 : cz);
+        // first cell with key >= lo_key at or after the column head
+        uint64_t c = uint64_t(f);
+        if (cell_key[c] < lo_key) {
+          uint64_t step = 1;
+          while (c + step < u_count && cell_key[c + step] < lo_key) {
+            c += step;
+            step <<= 1;
+          }
+          // cell_key[c] < lo_key <= cell_key[hi] (or hi == u_count)
+          uint64_t hi = c + step < u_count ? c + step : u_count;
+          while (hi - c > 1) {
+            const uint64_t mid = c + ((hi - c) >> 1);
+            if (cell_key[mid] < lo_key) c = mid;
+            else hi = mid;
+          }
+          c = hi;
+        }
+        if (c < u_count && cell_key[c] <= hi_key) {
+          uint64_t last = c;
+          while (last + 1 < u_count && cell_key[last + 1] <= hi_key) ++last;
+          rg = make_uint2(cell_start[c], cell_start[last + 1]);
         }
       }
-      if (first >= 0) rg = make_uint2(cell_start[first], cell_start[last + 1]);
     }
     ranges[w] = rg;
   }

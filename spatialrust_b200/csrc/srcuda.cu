@@ -143,7 +143,7 @@ uint32_t ceil_div(uint64_t a, uint64_t b) { return uint32_t((a + b - 1) / b); }
 const char *const kKernelNames[SRCU_K_COUNT] = {
     "k_begin",          "k_bounds",        "k_voxel_plan",  "(in k_sort<voxel>)",
     "k_sort<voxel>",    "k_voxel_segments", "k_unpack_voxel_keys", "k_cell_plan",
-    "(in k_sort<cell>)", "k_sort<cell>",    "k_cells",       "k_hash_insert",
+    "(in k_sort<cell>)", "k_sort<cell>",    "k_cells",       "k_column_insert",
     "k_ranges",         "k_normals"};
 
 // Counts the launches of one kernel group and, when its bit is set in
@@ -468,8 +468,8 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
                                                                     uint32_t(ctx->num_sms) * 8));
   {
     Launch l(ctx, SRCU_K_HASH);
-    k_hash_insert<<<grid_g, 256, 0, ctx->stream>>>(ctx->ctl, ptr<uint64_t>(ctx->cell_key),
-                                                   ptr<uint64_t>(ctx->table), ctx->table_log2);
+    k_column_insert<<<grid_g, 256, 0, ctx->stream>>>(ctx->ctl, ptr<uint64_t>(ctx->cell_key),
+                                                     ptr<uint64_t>(ctx->table), ctx->table_log2, bt);
   }
   const uint32_t grid_r = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n_max * 9, 256),
                                                                     uint32_t(ctx->num_sms) * 16));

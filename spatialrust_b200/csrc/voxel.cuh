@@ -79,7 +79,7 @@ struct BoundsAcc {
   }
 };
 
-constexpr uint32_t BND_CHUNK = 16;  // consecutive points per thread in the multi-cloud case
+constexpr uint32_t BND_CHUNK = 16;  // points per lane of a warp span in the multi-cloud case
 
 // Per-cloud min/max over finite coordinates plus NaN / inf flags
 // (compute_bounds, voxel.rs:1067-1079, ignores NaN through f32::min/max).
@@ -134,30 +134,55 @@ __global__ void __launch_bounds__(BND_THREADS) k_bounds(const float *x, const fl
     }
     return;
   }
-  // Many clouds: each thread walks BND_CHUNK consecutive points and flushes
-  // its running bounds whenever the cloud changes.
-  const uint64_t chunks = (n + BND_CHUNK - 1) / BND_CHUNK;
-  for (uint64_t c = blockIdx.x * uint64_t(BND_THREADS) + threadIdx.x; c < chunks;
-       c += uint64_t(gridDim.x) * BND_THREADS) {
-    const uint32_t i0 = uint32_t(c * BND_CHUNK);
-    const uint64_t end = c * BND_CHUNK + BND_CHUNK;
-    const uint32_t i1 = uint32_t(end < n ? end : n);
-    uint32_t b = cloud_of(bt, i0);
-    uint32_t next = __ldg(bt.offsets + b + 1);
+  // Many clouds: each warp owns a span of 32 * BND_CHUNK consecutive points,
+  // read coalesced.  A span inside one cloud (all but at most one span per
+  // cloud boundary) reduces across the warp and flushes once; a span that
+  // crosses a boundary flushes per lane whenever its cloud changes.
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t span = 32ull * BND_CHUNK;
+  const uint64_t spans = (n + span - 1) / span;
+  const uint64_t warps = uint64_t(gridDim.x) * (BND_THREADS / 32);
+  for (uint64_t sp = blockIdx.x * uint64_t(BND_THREADS / 32) + (threadIdx.x >> 5); sp < spans;
+       sp += warps) {
+    const uint64_t s0 = sp * span;
+    const uint64_t s1 = s0 + span < n ? s0 + span : n;
+    const uint32_t b0 = cloud_of(bt, uint32_t(s0));
+    const uint32_t b1 = cloud_of(bt, uint32_t(s1 - 1));
     BoundsAcc acc;
     acc.reset();
-    for (uint32_t i = i0; i < i1; ++i) {
-      while (i >= next) {  // crossed into a later cloud (skipping empty ones)
-        acc.flush(bt.bounds[b]);
-        acc.reset();
-        ++b;
-        next = __ldg(bt.offsets + b + 1);
+    if (b0 == b1) {
+      for (uint64_t i = s0 + lane; i < s1; i += 32) {
+        const float xi = x[i], yi = y[i], zi = z[i];
+        if (aos) aos[i] = make_float4(xi, yi, zi, a0 ? a0[i] : 0.0f);
+        acc.add(xi, yi, zi);
       }
-      const float xi = x[i], yi = y[i], zi = z[i];
-      if (aos) aos[i] = make_float4(xi, yi, zi, a0 ? a0[i] : 0.0f);
-      acc.add(xi, yi, zi);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          acc.mn[a] = min(acc.mn[a], __shfl_xor_sync(FULL_MASK, acc.mn[a], o));
+          acc.mx[a] = max(acc.mx[a], __shfl_xor_sync(FULL_MASK, acc.mx[a], o));
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc.flags |= __shfl_xor_sync(FULL_MASK, acc.flags, o);
+      if (lane == 0) acc.flush(bt.bounds[b0]);
+    } else {
+      uint32_t b = b0;
+      uint32_t next = __ldg(bt.offsets + b + 1);
+      for (uint64_t i = s0 + lane; i < s1; i += 32) {
+        while (i >= next) {  // crossed into a later cloud (skipping empty ones)
+          acc.flush(bt.bounds[b]);
+          acc.reset();
+          ++b;
+          next = __ldg(bt.offsets + b + 1);
+        }
+        const float xi = x[i], yi = y[i], zi = z[i];
+        if (aos) aos[i] = make_float4(xi, yi, zi, a0 ? a0[i] : 0.0f);
+        acc.add(xi, yi, zi);
+      }
+      acc.flush(bt.bounds[b]);
     }
-    acc.flush(bt.bounds[b]);
   }
 }
 
