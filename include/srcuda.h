@@ -73,12 +73,25 @@ typedef struct srcu_cloud {
   uint64_t n;
 } srcu_cloud;
 
-/* VoxelGridDownsampleConfig for Centroid + Average
- * (crates/spatialrust-filtering/src/voxel.rs:112-183). */
+/* VoxelAggregationMode (voxel.rs:68-76) and AttributeAggregation (voxel.rs:78-86). */
+#define SRCU_VOXEL_CENTROID 0          /* mean of every point of the voxel */
+#define SRCU_VOXEL_APPROXIMATE_FIRST 1 /* the voxel's first point (input order) */
+#define SRCU_ATTRIBUTE_AVERAGE 0
+#define SRCU_ATTRIBUTE_FIRST 1
+
+/* VoxelGridDownsampleConfig (crates/spatialrust-filtering/src/voxel.rs:112-183).
+ * Centroid + Average is the reference's fast path (voxel.rs:464-540:
+ * (sum * (1/count)) as f32 for every field).  The other combinations follow
+ * its general path (voxel.rs:1122-1160): Centroid + First averages the
+ * positions as (sum / count) as f32 and takes the other fields from the
+ * voxel's first point; ApproximateFirst takes every field from the first
+ * point, whatever the attribute policy.  Zero-initialised = Centroid + Average. */
 typedef struct srcu_voxel_params {
   float leaf_size;  /* must be > 0 (NaN passes, as in voxel.rs:260) */
   int32_t has_origin;
   float origin[3];  /* used when has_origin != 0: floor keys; else origin = min corner, truncated keys */
+  int32_t mode;             /* SRCU_VOXEL_CENTROID or SRCU_VOXEL_APPROXIMATE_FIRST */
+  int32_t attribute_policy; /* SRCU_ATTRIBUTE_AVERAGE or SRCU_ATTRIBUTE_FIRST */
 } srcu_voxel_params;
 
 /* Voxel output.  Each column needs capacity >= input n (the voxel count is

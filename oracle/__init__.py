@@ -47,6 +47,9 @@ def _load():
     lib.oracle_voxel_centroid.argtypes = [P, P, P, P, ctypes.c_int, ctypes.c_size_t, ctypes.c_float,
                                           ctypes.c_int, P, ctypes.c_int, P, P, P, P]
     lib.oracle_voxel_centroid.restype = ctypes.c_int
+    lib.oracle_voxel_general.argtypes = [P, P, P, P, ctypes.c_int, ctypes.c_size_t, ctypes.c_float,
+                                         ctypes.c_int, P, ctypes.c_int, ctypes.c_int, P, P, P, P]
+    lib.oracle_voxel_general.restype = ctypes.c_int
     lib.oracle_radius_normals_ref.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float,
                                               ctypes.c_uint32, ctypes.c_int, P, ctypes.c_int, P, P,
                                               P, P, P, P, P]
@@ -119,6 +122,35 @@ def voxel_centroid(x, y, z, attrs=(), leaf=1.0, origin=None, plain_xyz=False) ->
                                    ctypes.byref(nv))
     if rc != 0:
         raise OracleError(f"oracle_voxel_centroid failed: {rc}")
+    v = nv.value
+    return VoxelResult([o[:v].copy() for o in outs], keys[:v].copy(), counts[:v].copy())
+
+
+def voxel_general(x, y, z, attrs=(), leaf=1.0, origin=None, approximate=False,
+                  attribute_first=False) -> VoxelResult:
+    """Reference CPU general voxel path (voxel.rs:703-716, 1122-1171): the
+    modes other than Centroid + Average.  approximate: ApproximateFirst (every
+    field from the voxel's first point); else Centroid with positions
+    (sum / count) and attributes first (attribute_first) or (sum / count)."""
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    attrs = [_f32(a) for a in attrs]
+    n = x.shape[0]
+    cap = max(n, 1)
+    outs = [np.empty(cap, np.float32) for _ in range(3 + len(attrs))]
+    keys = np.empty((cap, 3), np.int64)
+    counts = np.empty(cap, np.uint32)
+    attr_ptrs = (ctypes.c_void_p * max(len(attrs), 1))(*[a.ctypes.data for a in attrs])
+    out_ptrs = (ctypes.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
+    org = np.asarray(origin if origin is not None else (0, 0, 0), np.float32)
+    nv = ctypes.c_size_t(0)
+    rc = lib.oracle_voxel_general(_ptr(x), _ptr(y), _ptr(z), ctypes.cast(attr_ptrs, ctypes.c_void_p),
+                                  len(attrs), n, ctypes.c_float(leaf), int(origin is not None),
+                                  _ptr(org), int(bool(approximate)), int(bool(attribute_first)),
+                                  ctypes.cast(out_ptrs, ctypes.c_void_p), _ptr(keys), _ptr(counts),
+                                  ctypes.byref(nv))
+    if rc != 0:
+        raise OracleError(f"oracle_voxel_general failed: {rc}")
     v = nv.value
     return VoxelResult([o[:v].copy() for o in outs], keys[:v].copy(), counts[:v].copy())
 

@@ -322,6 +322,101 @@ nomem:
   return OR_ERR_NOMEM;
 }
 
+/* General voxel path: build_voxel_cells_cpu (voxel.rs:703-716: floor keys,
+ * point indices per cell in input order), cells sorted by key (voxel.rs:
+ * 352-353), append_voxel_point (voxel.rs:1122-1160): with approximate != 0
+ * every field is the cell's first point; otherwise positions are
+ * average_field (voxel.rs:1162-1171: f64 sum over the indices in order,
+ * divided by the count, cast to f32) and the other fields are the first
+ * point's (attribute_first) or average_field (attribute average).  The
+ * reference only reaches this path for modes other than Centroid + Average
+ * on its CPU policies. */
+int oracle_voxel_general(const float *x, const float *y, const float *z, const float *const *attrs,
+                         int n_attrs, size_t n, float leaf, int has_origin, const float *origin,
+                         int approximate, int attribute_first, float *const *out_fields,
+                         int64_t *out_keys, uint32_t *out_counts, size_t *out_v) {
+  *out_v = 0;
+  if (n == 0) return OR_OK;
+  if (leaf <= 0.0f) return OR_ERR_INVALID;
+  const float inv_leaf = 1.0f / leaf;
+  float o[3];
+  if (has_origin) {
+    o[0] = origin[0];
+    o[1] = origin[1];
+    o[2] = origin[2];
+  } else {
+    float mx[3];
+    oracle_compute_bounds(x, y, z, n, o, mx);
+  }
+  const int nf = 3 + n_attrs;
+  cell_map map;
+  if (cell_map_init(&map, 64) != OR_OK) return OR_ERR_NOMEM;
+  size_t cap_cells = 1024;
+  int64_t *keys = (int64_t *)malloc(cap_cells * 3 * sizeof(int64_t));
+  uint32_t *counts = (uint32_t *)malloc(cap_cells * sizeof(uint32_t));
+  size_t *first = (size_t *)malloc(cap_cells * sizeof(size_t));
+  double *sums = (double *)malloc(cap_cells * nf * sizeof(double));
+  size_t ncells = 0;
+  for (size_t i = 0; i < n; ++i) {
+    int64_t k[3];
+    voxel_key_floor(x[i], y[i], z[i], o, inv_leaf, k);
+    uint32_t id;
+    int inserted;
+    if (cell_map_get_or_insert(&map, k, (uint32_t)ncells, &id, &inserted) != OR_OK) goto nomem;
+    if (inserted) {
+      if (ncells == cap_cells) {
+        cap_cells *= 2;
+        keys = (int64_t *)realloc(keys, cap_cells * 3 * sizeof(int64_t));
+        counts = (uint32_t *)realloc(counts, cap_cells * sizeof(uint32_t));
+        first = (size_t *)realloc(first, cap_cells * sizeof(size_t));
+        sums = (double *)realloc(sums, cap_cells * nf * sizeof(double));
+      }
+      memcpy(&keys[3 * ncells], k, 3 * sizeof(int64_t));
+      counts[ncells] = 0;
+      first[ncells] = i;
+      for (int f = 0; f < nf; ++f) sums[ncells * nf + f] = 0.0;
+      ncells++;
+    }
+    counts[id] += 1;
+    double *sm = &sums[(size_t)id * nf];
+    sm[0] += (double)x[i];
+    sm[1] += (double)y[i];
+    sm[2] += (double)z[i];
+    for (int a = 0; a < n_attrs; ++a) sm[3 + a] += (double)attrs[a][i];
+  }
+  uint32_t *order = (uint32_t *)malloc(ncells * sizeof(uint32_t));
+  for (size_t c = 0; c < ncells; ++c) order[c] = (uint32_t)c;
+  g_sort_keys = keys;
+  qsort(order, ncells, sizeof(uint32_t), cmp_cell_ids);
+  for (size_t r = 0; r < ncells; ++r) {
+    const uint32_t id = order[r];
+    const size_t rep = first[id];
+    for (int f = 0; f < nf; ++f) {
+      const float rep_value = f == 0 ? x[rep] : f == 1 ? y[rep] : f == 2 ? z[rep] : attrs[f - 3][rep];
+      const int take_first = approximate || (f >= 3 && attribute_first);
+      out_fields[f][r] =
+          take_first ? rep_value : (float)(sums[(size_t)id * nf + f] / (double)counts[id]);
+    }
+    if (out_keys) memcpy(&out_keys[3 * r], &keys[3 * (size_t)id], 3 * sizeof(int64_t));
+    if (out_counts) out_counts[r] = counts[id];
+  }
+  *out_v = ncells;
+  free(order);
+  free(keys);
+  free(counts);
+  free(first);
+  free(sums);
+  cell_map_free(&map);
+  return OR_OK;
+nomem:
+  free(keys);
+  free(counts);
+  free(first);
+  free(sums);
+  cell_map_free(&map);
+  return OR_ERR_NOMEM;
+}
+
 /* ------------------------------------------------------------------------ */
 /* KD-tree (crates/spatialrust-search/src/kdtree.rs)                         */
 /* ------------------------------------------------------------------------ */

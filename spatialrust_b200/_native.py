@@ -78,9 +78,15 @@ class SrcuCloud(ctypes.Structure):
                 ("on_device", ctypes.c_int32), ("n", ctypes.c_uint64)]
 
 
+SRCU_VOXEL_CENTROID = 0
+SRCU_VOXEL_APPROXIMATE_FIRST = 1
+SRCU_ATTRIBUTE_AVERAGE = 0
+SRCU_ATTRIBUTE_FIRST = 1
+
+
 class SrcuVoxelParams(ctypes.Structure):
     _fields_ = [("leaf_size", ctypes.c_float), ("has_origin", ctypes.c_int32),
-                ("origin", c_float3)]
+                ("origin", c_float3), ("mode", ctypes.c_int32), ("attribute_policy", ctypes.c_int32)]
 
 
 class SrcuVoxelOut(ctypes.Structure):
@@ -372,8 +378,11 @@ class Context:
     # ---- one cloud --------------------------------------------------------
 
     def voxel_centroid(self, x, y, z, attrs=(), leaf: float = 1.0, origin=None,
-                       want_keys: bool = False):
-        """Returns (columns [x, y, z, attrs...], keys (V,3) int64 or None, counts) as numpy."""
+                       want_keys: bool = False, approximate: bool = False,
+                       attribute_first: bool = False):
+        """Returns (columns [x, y, z, attrs...], keys (V,3) int64 or None, counts) as numpy.
+        approximate / attribute_first select the reference's ApproximateFirst mode
+        and First attribute policy (srcu_voxel_params)."""
         keep = _Keep()
         cloud = make_cloud(x, y, z, attrs, keep)
         n = int(cloud.n)
@@ -385,7 +394,7 @@ class Context:
         vout = SrcuVoxelOut(outs[0].ctypes.data, outs[1].ctypes.data, outs[2].ctypes.data,
                             ctypes.cast(attr_out, ctypes.c_void_p),
                             keys.ctypes.data if keys is not None else 0, counts.ctypes.data, 0)
-        vp = _voxel_params(leaf, origin)
+        vp = _voxel_params(leaf, origin, approximate, attribute_first)
         nv = ctypes.c_uint64(0)
         self._check(self._lib.srcu_voxel_centroid(self._h, ctypes.byref(cloud), ctypes.byref(vp),
                                                   ctypes.byref(vout), ctypes.byref(nv)))
@@ -451,12 +460,15 @@ class Context:
     def batch_voxel_normals_enqueue(self, points: SrcuCloud, offsets, leaves, radii,
                                     min_neighbors: int = 3, viewpoints=None,
                                     include_self: bool = False, count_shell: bool = True,
-                                    origins=None):
-        """Voxel -> normals for many clouds concatenated in `points` (device)."""
+                                    origins=None, modes=None):
+        """Voxel -> normals for many clouds concatenated in `points` (device).
+        modes: per cloud (approximate, attribute_first), default Centroid + Average."""
         count = len(offsets) - 1
         offs = (ctypes.c_uint64 * (count + 1))(*[int(o) for o in offsets])
         vps = (SrcuVoxelParams * count)(*[
-            _voxel_params(leaves[b], None if origins is None else origins[b]) for b in range(count)])
+            _voxel_params(leaves[b], None if origins is None else origins[b],
+                          *((False, False) if modes is None else modes[b]))
+            for b in range(count)])
         nps = (SrcuNormalParams * count)(*[
             _normal_params(radii[b], min_neighbors, None if viewpoints is None else viewpoints[b],
                            include_self, count_shell) for b in range(count)])
@@ -625,11 +637,14 @@ class Server:
         self._lib.srcu_server_stats_reset(self._h)
 
 
-def _voxel_params(leaf, origin) -> SrcuVoxelParams:
+def _voxel_params(leaf, origin, approximate: bool = False,
+                  attribute_first: bool = False) -> SrcuVoxelParams:
+    mode = SRCU_VOXEL_APPROXIMATE_FIRST if approximate else SRCU_VOXEL_CENTROID
+    policy = SRCU_ATTRIBUTE_FIRST if attribute_first else SRCU_ATTRIBUTE_AVERAGE
     if origin is None:
-        return SrcuVoxelParams(float(leaf), 0, c_float3(0, 0, 0))
+        return SrcuVoxelParams(float(leaf), 0, c_float3(0, 0, 0), mode, policy)
     o = [float(v) for v in origin]
-    return SrcuVoxelParams(float(leaf), 1, c_float3(*o))
+    return SrcuVoxelParams(float(leaf), 1, c_float3(*o), mode, policy)
 
 
 def _normal_params(radius, min_neighbors, viewpoint, include_self,

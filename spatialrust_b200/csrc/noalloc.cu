@@ -92,14 +92,15 @@ srcu_status noalloc_setup(int device, NoallocDevice **out) {
 
 template <int NC>
 void noalloc_segments(cudaStream_t s, uint32_t grid, Control *ctl, const SortBuffers &sb,
-                      const float **in, float *const *out, uint64_t *vkeys, uint32_t *vcounts) {
+                      const float **in, float *const *out, uint64_t *vkeys, uint32_t *vcounts,
+                      const Batch &bt) {
   Columns<NC> cols;
   for (int c = 0; c < NC; ++c) {
     cols.in[c] = in[c];
     cols.out[c] = out[c];
   }
   k_voxel_segments<NC><<<grid, SEG_THREADS, segment_smem_bytes(NC), s>>>(
-      ctl, sb, &ctl->vsort, cols, vkeys, vcounts, sb.lookback + 0, nullptr, nullptr);
+      ctl, sb, &ctl->vsort, cols, vkeys, vcounts, sb.lookback + 0, nullptr, nullptr, bt, -1);
 }
 
 }  // namespace
@@ -114,6 +115,10 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
   if (cloud->n_attrs > MAX_COLS - 3) return SRCU_ERR_INVALID_ARGUMENT;
   if (!cloud->on_device || !out->on_device) return SRCU_ERR_INVALID_ARGUMENT;
   if (params->leaf_size <= 0.0f) return SRCU_ERR_INVALID_ARGUMENT;  // voxel.rs:260-264
+  if ((params->mode != SRCU_VOXEL_CENTROID && params->mode != SRCU_VOXEL_APPROXIMATE_FIRST) ||
+      (params->attribute_policy != SRCU_ATTRIBUTE_AVERAGE &&
+       params->attribute_policy != SRCU_ATTRIBUTE_FIRST))
+    return SRCU_ERR_INVALID_ARGUMENT;
   const uint64_t n = cloud->n;
   if (n == 0) return SRCU_OK;
   if (!cloud->x || !cloud->y || !cloud->z || !out->x || !out->y || !out->z)
@@ -166,6 +171,9 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
   vp0.leaf = params->leaf_size;
   vp0.has_origin = params->has_origin;
   for (int a = 0; a < 3; ++a) vp0.origin[a] = params->origin[a];
+  vp0.agg = params->mode == SRCU_VOXEL_APPROXIMATE_FIRST ? AGG_FIRST
+            : params->attribute_policy == SRCU_ATTRIBUTE_FIRST ? AGG_CENTROID_FIRST
+                                                               : AGG_FAST;
   // k_begin zeroes the control block (all but the epoch) and writes the
   // cloud's offsets and parameters on every call.
   k_begin<<<1, 256, 0, s>>>(ctl, n, bt, 0u, 1, vp0, NormalParamsDev{});
@@ -185,16 +193,16 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
   const uint32_t grid_g =
       std::min<uint32_t>(std::max<uint32_t>(1, ceil_div(n, SEG_TILE)), sms * uint32_t(dev->occ_seg));
   switch (nc) {
-    case 3: noalloc_segments<3>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
-    case 4: noalloc_segments<4>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
-    case 5: noalloc_segments<5>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
-    case 6: noalloc_segments<6>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
-    case 7: noalloc_segments<7>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
-    case 8: noalloc_segments<8>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
-    case 9: noalloc_segments<9>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
-    case 10: noalloc_segments<10>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
-    case 11: noalloc_segments<11>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
-    case 12: noalloc_segments<12>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts); break;
+    case 3: noalloc_segments<3>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts, bt); break;
+    case 4: noalloc_segments<4>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts, bt); break;
+    case 5: noalloc_segments<5>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts, bt); break;
+    case 6: noalloc_segments<6>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts, bt); break;
+    case 7: noalloc_segments<7>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts, bt); break;
+    case 8: noalloc_segments<8>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts, bt); break;
+    case 9: noalloc_segments<9>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts, bt); break;
+    case 10: noalloc_segments<10>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts, bt); break;
+    case 11: noalloc_segments<11>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts, bt); break;
+    case 12: noalloc_segments<12>(s, grid_g, ctl, seg, in, outc, vkeys, vcounts, bt); break;
     default: return SRCU_ERR_INVALID_ARGUMENT;
   }
   if (out->keys)

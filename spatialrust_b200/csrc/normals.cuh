@@ -278,10 +278,20 @@ __global__ void k_ranges(Control *ctl, const uint64_t *cell_key, const uint32_t 
   const uint32_t epoch = ctl->epoch + EP_CELLS;
   const uint32_t lb = ctl->ckey_bits;
   const uint64_t local_mask = lb >= 64 ? ~0ull : ((1ull << lb) - 1);
-  for (uint64_t w = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; w < u_count * 9;
+  const uint64_t total = u_count * 9;
+  const bool narrow = total <= 0xFFFFFFFFull;  // 32-bit index math (no 64-bit divide)
+  for (uint64_t w = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; w < total;
        w += uint64_t(gridDim.x) * blockDim.x) {
-    const uint64_t u = w / 9;
-    const uint32_t col = uint32_t(w - u * 9);
+    uint64_t u;
+    uint32_t col;
+    if (narrow) {
+      const uint32_t u32 = uint32_t(w) / 9u;
+      u = u32;
+      col = uint32_t(w) - u32 * 9u;
+    } else {
+      u = w / 9;
+      col = uint32_t(w - u * 9);
+    }
     const uint64_t full = cell_key[u];
     const uint32_t b = cloud_of_key(full, bt, lb);
     const CellPlan &pl = bt.cplans[b < bt.clouds ? b : 0];
@@ -428,36 +438,58 @@ __global__ void __launch_bounds__(NM_THREADS, 3) k_normals(Control *ctl, const f
     double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // sx sy sz sxx syy szz sxy sxz syz
     float F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     uint32_t since = 0;
+    // One candidate: the reference's f32 predicate ((dx^2 + dy^2) + dz^2 <= r^2,
+    // kdtree.rs:544-549) and the f32 partial moments of the hits.
+    auto visit = [&](const float4 c) {
+      const float dx = __fsub_rn(c.x, qp.x);
+      const float dy = __fsub_rn(c.y, qp.y);
+      const float dz = __fsub_rn(c.z, qp.z);
+      const float xx = __fmul_rn(dx, dx), yy = __fmul_rn(dy, dy), zz = __fmul_rn(dz, dz);
+      const float d2 = __fadd_rn(__fadd_rn(xx, yy), zz);
+      if (d2 <= r2) {
+        hits += 1.f;
+        F[0] += dx;
+        F[1] += dy;
+        F[2] += dz;
+        F[3] += xx;
+        F[4] += yy;
+        F[5] += zz;
+        F[6] = fmaf(dx, dy, F[6]);
+        F[7] = fmaf(dx, dz, F[7]);
+        F[8] = fmaf(dy, dz, F[8]);
+      }
+      if (prm.count_shell && d2 != 0.f && fabsf(__fsub_rn(d2, r2)) <= shell_tol) shell = 1;
+    };
+    auto flush = [&]() {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        S[k] += double(F[k]);
+        F[k] = 0.f;
+      }
+    };
+    uint2 next = rg[0];
 #pragma unroll 1
     for (int r = 0; r < 9; ++r) {
-      const uint2 range = rg[r];
-      for (uint32_t j = range.x; j < range.y; ++j) {
-        const float4 c = __ldg(pts + j);
-        const float dx = __fsub_rn(c.x, qp.x);
-        const float dy = __fsub_rn(c.y, qp.y);
-        const float dz = __fsub_rn(c.z, qp.z);
-        const float xx = __fmul_rn(dx, dx), yy = __fmul_rn(dy, dy), zz = __fmul_rn(dz, dz);
-        const float d2 = __fadd_rn(__fadd_rn(xx, yy), zz);
-        if (d2 <= r2) {
-          hits += 1.f;
-          F[0] += dx;
-          F[1] += dy;
-          F[2] += dz;
-          F[3] += xx;
-          F[4] += yy;
-          F[5] += zz;
-          F[6] = fmaf(dx, dy, F[6]);
-          F[7] = fmaf(dx, dz, F[7]);
-          F[8] = fmaf(dy, dz, F[8]);
-        }
-        if (prm.count_shell && d2 != 0.f && fabsf(__fsub_rn(d2, r2)) <= shell_tol) shell = 1;
-        if (++since == NM_FLUSH) {
+      const uint2 range = next;
+      if (r < 8) next = rg[r + 1];  // the next column's range loads under this one
+      uint32_t j = range.x;
+      // two independent candidate loads in flight per step
+      for (; j + 2 <= range.y; j += 2) {
+        const float4 c0 = __ldg(pts + j);
+        const float4 c1 = __ldg(pts + j + 1);
+        visit(c0);
+        visit(c1);
+        since += 2;
+        if (since >= NM_FLUSH) {
           since = 0;
-#pragma unroll
-          for (int k = 0; k < 9; ++k) {
-            S[k] += double(F[k]);
-            F[k] = 0.f;
-          }
+          flush();
+        }
+      }
+      if (j < range.y) {
+        visit(__ldg(pts + j));
+        if (++since >= NM_FLUSH) {
+          since = 0;
+          flush();
         }
       }
     }

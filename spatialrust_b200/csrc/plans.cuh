@@ -62,10 +62,16 @@ struct CellPlan {
 };
 
 // Per-cloud parameters on the device (srcu_voxel_params / srcu_normal_params).
+// Per-voxel emission (srcu_voxel_params mode / attribute_policy).
+constexpr int32_t AGG_FAST = 0;            // Centroid + Average: (sum * (1/count)) for every field
+constexpr int32_t AGG_CENTROID_FIRST = 1;  // positions (sum / count), other fields first point
+constexpr int32_t AGG_FIRST = 2;           // ApproximateFirst: every field from the first point
+
 struct VoxelParamsDev {
   float leaf;
   int32_t has_origin;
   float origin[3];
+  int32_t agg;  // AGG_*
 };
 
 struct NormalParamsDev {

@@ -53,6 +53,7 @@ struct srcu_ctx {
   DevBuf b_offsets, b_bounds, b_vplans, b_cplans, b_vparams, b_nparams, b_voff;
   uint32_t batch_cap = 0;
   uint32_t last_clouds = 1;
+  int32_t agg_all = AGG_FAST;  // the chain's voxel aggregation when every cloud shares it, else -1
   unsigned char *h_stage[2] = {nullptr, nullptr};
   size_t h_stage_bytes[2] = {0, 0};
   cudaEvent_t h_stage_ev[2] = {nullptr, nullptr};
@@ -300,6 +301,9 @@ VoxelParamsDev to_dev(const srcu_voxel_params *vp) {
   d.leaf = vp->leaf_size;
   d.has_origin = vp->has_origin;
   for (int a = 0; a < 3; ++a) d.origin[a] = vp->origin[a];
+  d.agg = vp->mode == SRCU_VOXEL_APPROXIMATE_FIRST ? AGG_FIRST
+          : vp->attribute_policy == SRCU_ATTRIBUTE_FIRST ? AGG_CENTROID_FIRST
+                                                         : AGG_FAST;
   return d;
 }
 
@@ -381,7 +385,7 @@ srcu_status launch_sort(srcu_ctx *ctx, const Src &src, uint64_t n_max, uint32_t 
 }
 
 template <int NC>
-void launch_segments_nc(srcu_ctx *ctx, const float **in, uint32_t grid) {
+void launch_segments_nc(srcu_ctx *ctx, const float **in, uint32_t grid, const Batch &bt) {
   Columns<NC> cols;
   for (int c = 0; c < NC; ++c) {
     cols.in[c] = in[c];
@@ -390,7 +394,7 @@ void launch_segments_nc(srcu_ctx *ctx, const float **in, uint32_t grid) {
   k_voxel_segments<NC><<<grid, SEG_THREADS, segment_smem_bytes(NC), ctx->stream>>>(
       ctx->ctl, sort_buffers(ctx), &ctx->ctl->vsort, cols, ptr<uint64_t>(ctx->vkeys),
       ptr<uint32_t>(ctx->vcounts), ptr<uint64_t>(ctx->lb_seg), ptr<const float4>(ctx->in_aos),
-      ptr<float4>(ctx->vaos));
+      ptr<float4>(ctx->vaos), bt, ctx->agg_all);
 }
 
 // Voxel stage: bounds -> plan -> sort -> fused segment/centroid reduction.
@@ -419,16 +423,16 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
   const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(ctx->occ_seg));
   Launch l(ctx, SRCU_K_VOXEL_SEGMENTS);
   switch (nc) {
-    case 3: launch_segments_nc<3>(ctx, in, grid); break;
-    case 4: launch_segments_nc<4>(ctx, in, grid); break;
-    case 5: launch_segments_nc<5>(ctx, in, grid); break;
-    case 6: launch_segments_nc<6>(ctx, in, grid); break;
-    case 7: launch_segments_nc<7>(ctx, in, grid); break;
-    case 8: launch_segments_nc<8>(ctx, in, grid); break;
-    case 9: launch_segments_nc<9>(ctx, in, grid); break;
-    case 10: launch_segments_nc<10>(ctx, in, grid); break;
-    case 11: launch_segments_nc<11>(ctx, in, grid); break;
-    case 12: launch_segments_nc<12>(ctx, in, grid); break;
+    case 3: launch_segments_nc<3>(ctx, in, grid, bt); break;
+    case 4: launch_segments_nc<4>(ctx, in, grid, bt); break;
+    case 5: launch_segments_nc<5>(ctx, in, grid, bt); break;
+    case 6: launch_segments_nc<6>(ctx, in, grid, bt); break;
+    case 7: launch_segments_nc<7>(ctx, in, grid, bt); break;
+    case 8: launch_segments_nc<8>(ctx, in, grid, bt); break;
+    case 9: launch_segments_nc<9>(ctx, in, grid, bt); break;
+    case 10: launch_segments_nc<10>(ctx, in, grid, bt); break;
+    case 11: launch_segments_nc<11>(ctx, in, grid, bt); break;
+    case 12: launch_segments_nc<12>(ctx, in, grid, bt); break;
     default: return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "unsupported column count %u", nc);
   }
   k_voxel_offsets<<<ceil_div(bt.clouds + 1, 128), 128, 0, ctx->stream>>>(
@@ -499,6 +503,7 @@ void begin_chain(srcu_ctx *ctx, uint64_t n, const Batch &bt, int single,
   k_begin<<<1, 256, 0, ctx->stream>>>(ctx->ctl, n, bt, cloud_bits_for(bt.clouds), single,
                                       to_dev(vp), to_dev(np));
   ctx->last_clouds = bt.clouds;
+  if (single) ctx->agg_all = to_dev(vp).agg;
 }
 
 srcu_status read_control(srcu_ctx *ctx) {
@@ -533,6 +538,10 @@ srcu_status check_voxel_params(srcu_ctx *ctx, const srcu_voxel_params *vp) {
   if (!vp) return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "voxel params are NULL");
   if (vp->leaf_size <= 0.0f)  // voxel.rs:260-264 (a NaN leaf is not rejected there either)
     return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "leaf_size must be greater than zero");
+  if ((vp->mode != SRCU_VOXEL_CENTROID && vp->mode != SRCU_VOXEL_APPROXIMATE_FIRST) ||
+      (vp->attribute_policy != SRCU_ATTRIBUTE_AVERAGE && vp->attribute_policy != SRCU_ATTRIBUTE_FIRST))
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "unknown voxel aggregation mode %d / policy %d",
+                vp->mode, vp->attribute_policy);
   return SRCU_OK;
 }
 
@@ -838,6 +847,9 @@ static srcu_status batch_enqueue(srcu_ctx *ctx, const srcu_cloud *points, const 
   if (stage) ST_TRY(stage_batch(ctx, count, offsets, vparams, nparams));
   const Batch bt = make_batch(ctx, count);
   begin_chain(ctx, n, bt, 0, nullptr, nullptr);
+  ctx->agg_all = to_dev(&vparams[0]).agg;
+  for (uint32_t b = 1; b < count; ++b)
+    if (to_dev(&vparams[b]).agg != ctx->agg_all) ctx->agg_all = -1;
   if (n > 0) {
     ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
     ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),

@@ -283,8 +283,25 @@ __host__ __device__ constexpr size_t segment_smem_bytes(int nc) {
   return sizeof(SegmentSmemHead) + size_t(nc) * SEG_TILE * sizeof(float);
 }
 
-template <int NC>
+// Aggregation of the voxel whose packed key is `key`: agg_all when the host
+// knows every cloud of the chain shares one, else the voxel's cloud's mode.
+__device__ __forceinline__ int32_t voxel_agg(const Batch &bt, uint64_t key, uint32_t vkey_bits,
+                                             int32_t agg_all) {
+  if (agg_all >= 0) return agg_all;
+  const uint32_t b = (bt.clouds == 1 || vkey_bits >= 64) ? 0u : uint32_t(key >> vkey_bits);
+  return bt.vparams[b < bt.clouds ? b : 0].agg;
+}
+
+// Writes one voxel.  s: FP64 sums of every column in ascending point order;
+// first(c): column c of the voxel's first point, read only by the modes that
+// use it (so the default mode keeps no extra registers live).
+//   AGG_FAST            (sum * (1.0 / count)) as f32, voxel.rs:531-536
+//   AGG_CENTROID_FIRST  positions (sum / count) as f32 (average_field,
+//                       voxel.rs:1162-1171), other fields from the first point
+//   AGG_FIRST           every field from the first point (voxel.rs:1135-1146)
+template <int NC, class First>
 __device__ __forceinline__ void write_centroid(const Columns<NC> &cols, const double (&s)[NC],
+                                               First first, int32_t agg,
                                                uint32_t cnt, uint32_t seg, uint64_t key,
                                                uint64_t *out_keys, uint32_t *out_counts,
                                                uint32_t n, uint32_t *status, float4 *aos_out) {
@@ -292,12 +309,14 @@ __device__ __forceinline__ void write_centroid(const Columns<NC> &cols, const do
     atomicOr(status, ST_INTERNAL);
     return;
   }
-  // (sum * (1.0 / count)) as f32, voxel.rs:531-536
   const double inv = 1.0 / double(cnt);
   float o[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
-    o[c] = __double2float_rn(__dmul_rn(s[c], inv));
+    if (agg == AGG_FAST) o[c] = __double2float_rn(__dmul_rn(s[c], inv));
+    else if (agg == AGG_CENTROID_FIRST && c < 3)
+      o[c] = __double2float_rn(__ddiv_rn(s[c], double(cnt)));
+    else o[c] = first(c);
     cols.out[c][seg] = o[c];
   }
   if (aos_out) aos_out[seg] = make_float4(o[0], o[1], o[2], 0.0f);
@@ -314,14 +333,15 @@ __device__ __forceinline__ void write_centroid(const Columns<NC> &cols, const do
 // reference's order, voxel.rs:502-520), one warp per long voxel or per voxel
 // that runs past the tile end.
 template <int NC>
-__global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, SortBuffers sort,
+__global__ void __launch_bounds__(SEG_THREADS, 5) k_voxel_segments(Control *ctl, SortBuffers sort,
                                                                  const SortState *sort_state,
                                                                  Columns<NC> cols,
                                                                  uint64_t *out_keys,
                                                                  uint32_t *out_counts,
                                                                  uint64_t *lookback,
                                                                  const float4 *aos_in,
-                                                                 float4 *aos_out) {
+                                                                 float4 *aos_out, Batch bt,
+                                                                 int32_t agg_all) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SegmentSmemHead &sm = *reinterpret_cast<SegmentSmemHead *>(smem_raw);
   float *scol = reinterpret_cast<float *>(smem_raw + sizeof(SegmentSmemHead));  // [NC][SEG_TILE]
@@ -407,8 +427,9 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
 #pragma unroll
           for (int c = 0; c < NC; ++c) s[c] += double(scol[c * SEG_TILE + m]);
         }
-        write_centroid<NC>(cols, s, e - j, seg, key, out_keys, out_counts, n, &ctl->status,
-                           aos_out);
+        write_centroid<NC>(cols, s, [&](int c) { return scol[c * SEG_TILE + j]; },
+                           voxel_agg(bt, key, ctl->vkey_bits, agg_all), e - j, seg, key, out_keys,
+                           out_counts, n, &ctl->status, aos_out);
       } else {
         deferred = true;
         def_pos = base + j;
@@ -451,8 +472,15 @@ __global__ void __launch_bounds__(SEG_THREADS) k_voxel_segments(Control *ctl, So
       for (int c = 0; c < NC; ++c)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s[c] += __shfl_xor_sync(FULL_MASK, s[c], o);
-      if (lane == 0)
-        write_centroid<NC>(cols, s, e - p, sg, key, out_keys, out_counts, n, &ctl->status, aos_out);
+      if (lane == 0) {
+        // the voxel's first point is the first sorted item (stable sort)
+        auto first = [&](int c) {
+          const uint32_t v0 = sv.val(p);
+          return v0 < n ? cols.in[c][v0] : 0.0f;
+        };
+        write_centroid<NC>(cols, s, first, voxel_agg(bt, key, ctl->vkey_bits, agg_all), e - p, sg,
+                           key, out_keys, out_counts, n, &ctl->status, aos_out);
+      }
     }
     __syncthreads();
   }

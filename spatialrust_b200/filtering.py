@@ -131,13 +131,14 @@ class VoxelGridDownsample:
             return input.clone()
         if cfg.leaf_size <= 0.0:
             raise InvalidArgument("leaf_size must be greater than zero")
-        if cfg.mode != VoxelAggregationMode.Centroid or cfg.attribute_policy != AttributeAggregation.Average:
-            raise InvalidArgument("the CUDA arm implements Centroid + Average voxel downsampling")
         x, y, z = input.positions3()
         attr_fields = [f for f in input.schema.fields if f.semantic not in POSITION_SEMANTICS]
         attrs = [_widen(input.columns[f.name]) for f in attr_fields]
         ctx = _native.shared_context(self._device)
-        cols, _, _ = ctx.voxel_centroid(x, y, z, attrs, leaf=cfg.leaf_size, origin=cfg.origin)
+        cols, _, _ = ctx.voxel_centroid(
+            x, y, z, attrs, leaf=cfg.leaf_size, origin=cfg.origin,
+            approximate=cfg.mode == VoxelAggregationMode.ApproximateFirst,
+            attribute_first=cfg.attribute_policy == AttributeAggregation.First)
         out = {}
         pos_names = {f.semantic: f.name for f in input.schema.fields if f.semantic in POSITION_SEMANTICS}
         out[pos_names[FieldSemantic.PositionX]] = cols[0]

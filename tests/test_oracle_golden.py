@@ -95,6 +95,43 @@ def test_generic_path_sorted_by_key_and_fp64_means():
         assert r.x[row] == expect
 
 
+def test_approximate_keeps_first_point_in_voxel():
+    # voxel.rs:1329-1339: approximate(1.0) on two points in one voxel keeps the first
+    x = np.array([0.0, 0.1], F)
+    zero = np.zeros(2, F)
+    r = oracle.voxel_general(x, zero, zero, [np.array([0.2, 0.9], F)], leaf=1.0, approximate=True)
+    assert len(r.x) == 1 and r.fields[3][0] == F(0.2) and r.x[0] == F(0.0)
+
+
+def test_approximate_first_four_points():
+    # voxel.rs:1446-1471 (CPU side): approximate(0.5), x = 0, 0.1, 1.0, 1.1, i = 0.2, 0.9, 10, 20
+    x = np.array([0.0, 0.1, 1.0, 1.1], F)
+    zero = np.zeros(4, F)
+    inten = np.array([0.2, 0.9, 10.0, 20.0], F)
+    r = oracle.voxel_general(x, zero, zero, [inten], leaf=0.5, approximate=True)
+    assert r.x.tolist() == [0.0, 1.0]
+    assert r.fields[3].tolist() == [F(0.2), F(10.0)]
+    assert r.counts.tolist() == [2, 2]
+
+
+def test_centroid_first_policy_divides_and_keeps_first_attribute():
+    # voxel.rs:1122-1171: Centroid + First: positions (f64 sum / count) as f32,
+    # attributes from the first point; the key set is the fast path's
+    rng = np.random.default_rng(9)
+    pts = (rng.random((3000, 3), dtype=np.float32) * F(7)).astype(np.float32)
+    inten = rng.random(3000, dtype=np.float32)
+    g = oracle.voxel_general(pts[:, 0], pts[:, 1], pts[:, 2], [inten], leaf=0.7,
+                             attribute_first=True)
+    f = oracle.voxel_centroid(pts[:, 0], pts[:, 1], pts[:, 2], [inten], leaf=0.7)
+    assert np.array_equal(g.keys, f.keys) and np.array_equal(g.counts, f.counts)
+    o = pts.min(axis=0)
+    k = ((pts - o) * (F(1.0) / F(0.7))).astype(np.float32).astype(np.int64)
+    for row in range(0, len(g.x), 97):
+        m = np.nonzero(np.all(k == g.keys[row], axis=1))[0]
+        assert g.x[row] == np.float32(np.sum(pts[m, 0].astype(np.float64)) / len(m))
+        assert g.fields[3][row] == inten[m[0]]
+
+
 def test_plane_normals_upward_radius():
     # normal.rs:650-667 uses k=8 on a 5x5 unit grid; the radius-mode analogue
     # (r = 1.5 covers the 8-neighbourhood) must give the same upward normals.

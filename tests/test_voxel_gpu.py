@@ -212,3 +212,95 @@ def test_device_resident_inputs_match_host_inputs(cuda_ctx):
     for a, b in zip(host[0], devr[0]):
         assert np.array_equal(a, b)
     assert np.array_equal(host[1], devr[1]) and np.array_equal(host[2], devr[2])
+
+
+# ---- ApproximateFirst and the First attribute policy (general path) ---------
+
+def assert_general_parity(ctx, x, y, z, attrs, leaf, approximate, attribute_first, origin=None):
+    cols, keys, counts = ctx.voxel_centroid(x, y, z, list(attrs), leaf=leaf, origin=origin,
+                                            want_keys=True, approximate=approximate,
+                                            attribute_first=attribute_first)
+    ref = oracle.voxel_general(x, y, z, list(attrs), leaf=leaf, origin=origin,
+                               approximate=approximate, attribute_first=attribute_first)
+    assert np.array_equal(keys, ref.keys) and np.array_equal(counts, ref.counts)
+    for c, (g, r) in enumerate(zip(cols, ref.fields)):
+        assert np.array_equal(g, r), f"column {c}: {np.count_nonzero(g != r)} values differ"
+
+
+def test_approximate_keeps_first_point_in_voxel():
+    # voxel.rs:1329-1339
+    cloud = build_cloud(sr.StandardSchemas.point_xyzi(), [[0, 0, 0, 0.2], [0.1, 0, 0, 0.9]])
+    out = sr.VoxelGridDownsample(sr.VoxelGridDownsampleConfig.approximate(1.0)).filter_with_policy(
+        cloud, sr.GpuCuda)
+    assert len(out) == 1 and out.intensity()[0] == F(0.2)
+
+
+def test_approximate_first_matches_cpu_four_points():
+    # voxel.rs:1446-1471: x from the first point of each voxel, intensities exact
+    cloud = build_cloud(sr.StandardSchemas.point_xyzi(),
+                        [[0, 0, 0, 0.2], [0.1, 0, 0, 0.9], [1.0, 0, 0, 10], [1.1, 0, 0, 20]])
+    out = sr.VoxelGridDownsample(sr.VoxelGridDownsampleConfig.approximate(0.5)).filter_with_policy(
+        cloud, sr.GpuCuda)
+    x, _, _ = out.positions3()
+    assert x.tolist() == [0.0, 1.0]
+    assert out.intensity().tolist() == [F(0.2), F(10.0)]
+
+
+@pytest.mark.parametrize("approximate,attribute_first", [(True, True), (True, False), (False, True)])
+def test_general_modes_bit_exact(cuda_ctx, approximate, attribute_first):
+    # short voxels (thread path) and long voxels (warp path), with attributes
+    c = synthetic.georef_scan(300_000, seed=12)
+    extra = np.random.default_rng(3).random(c.n, dtype=np.float32)
+    for leaf in (0.1, 2.0):
+        assert_general_parity(cuda_ctx, c.x, c.y, c.z, [c.intensity, extra], leaf, approximate,
+                              attribute_first)
+    assert_general_parity(cuda_ctx, c.x, c.y, c.z, [c.intensity], 0.25, approximate,
+                          attribute_first, origin=(-3.0, -3.0, -1.0))
+
+
+def test_u8_rgb_approximate_first_exact():
+    rows = [[0.0, 0.0, 0.0, 10, 20, 30], [0.2, 0.0, 0.0, 200, 100, 0], [1.5, 0.0, 0.0, 7, 8, 9]]
+    cloud = build_cloud(sr.StandardSchemas.point_xyzrgb(), rows)
+    out = sr.VoxelGridDownsample(sr.VoxelGridDownsampleConfig.approximate(1.0)).filter_with_policy(
+        cloud, sr.GpuCuda)
+    assert out.field("r").tolist() == [10, 7] and out.field("b").tolist() == [30, 9]
+
+
+def test_modes_per_cloud_in_one_batch():
+    import torch
+    clouds = [synthetic.georef_scan(n, seed=30 + i) for i, n in enumerate([40_000, 9_000, 25_000])]
+    modes = [(True, True), (False, False), (False, True)]
+    cols = [torch.from_numpy(np.concatenate([getattr(c, k) for c in clouds])).cuda()
+            for k in ("x", "y", "z", "intensity")]
+    offsets = np.concatenate([[0], np.cumsum([c.n for c in clouds])]).astype(np.int64)
+    keep = _native._Keep()
+    pts = _native.make_cloud(cols[0], cols[1], cols[2], [cols[3]], keep)
+    ctx = _native.Context(0)
+    ctx.batch_voxel_normals_enqueue(pts, offsets, [0.2] * 3, [1.0] * 3, modes=modes)
+    voff = ctx.batch_voxel_offsets()
+    out = ctx.frame_fetch(int(offsets[-1]), n_attrs=1)
+    for b, (c, (a, f)) in enumerate(zip(clouds, modes)):
+        lo, hi = int(voff[b]), int(voff[b + 1])
+        if a or f:
+            ref = oracle.voxel_general(c.x, c.y, c.z, [c.intensity], leaf=0.2, approximate=a,
+                                       attribute_first=f)
+        else:
+            ref = oracle.voxel_centroid(c.x, c.y, c.z, [c.intensity], leaf=0.2)
+        assert np.array_equal(out["counts"][lo:hi], ref.counts)
+        for g, r in zip(out["columns"], ref.fields):
+            assert np.array_equal(g[lo:hi], r), f"cloud {b}"
+    ctx.close()
+
+
+def test_approximate_first_xyzinormal():
+    # voxel.rs:1474-1500: point_xyzinormal, approximate(0.5); CPU semantics take
+    # every field (intensity and normals too) from each voxel's first point
+    rows = [[0.0, 0.0, 0.0, 0.2, 0.0, 0.0, 1.0], [0.1, 0.0, 0.0, 0.9, 0.1, 0.0, 1.0],
+            [1.0, 0.0, 0.0, 10.0, 0.0, 1.0, 0.0], [1.1, 0.0, 0.0, 20.0, 0.0, 0.0, 1.0]]
+    cloud = build_cloud(sr.StandardSchemas.point_xyzinormal(), rows)
+    out = sr.VoxelGridDownsample(sr.VoxelGridDownsampleConfig.approximate(0.5)).filter_with_policy(
+        cloud, sr.GpuCuda)
+    assert out.field("x").tolist() == [0.0, 1.0]
+    assert out.field("intensity").tolist() == [F(0.2), F(10.0)]
+    assert out.field("normal_y").tolist() == [0.0, 1.0]
+    assert out.field("normal_z").tolist() == [1.0, 0.0]
