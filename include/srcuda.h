@@ -82,7 +82,7 @@ typedef struct srcu_cloud {
 /* VoxelGridDownsampleConfig (crates/spatialrust-filtering/src/voxel.rs:112-183).
  * Centroid + Average is the reference's fast path (voxel.rs:464-540:
  * (sum * (1/count)) as f32 for every field).  The other combinations follow
- * its general path (voxel.rs:1122-1160): Centroid + First averages the
+ * its general path (voxel.rs:1123-1165): Centroid + First averages the
  * positions as (sum / count) as f32 and takes the other fields from the
  * voxel's first point; ApproximateFirst takes every field from the first
  * point, whatever the attribute policy.  Zero-initialised = Centroid + Average. */

@@ -128,7 +128,7 @@ def voxel_centroid(x, y, z, attrs=(), leaf=1.0, origin=None, plain_xyz=False) ->
 
 def voxel_general(x, y, z, attrs=(), leaf=1.0, origin=None, approximate=False,
                   attribute_first=False) -> VoxelResult:
-    """Reference CPU general voxel path (voxel.rs:703-716, 1122-1171): the
+    """Reference CPU general voxel path (voxel.rs:703-716, 1123-1165): the
     modes other than Centroid + Average.  approximate: ApproximateFirst (every
     field from the voxel's first point); else Centroid with positions
     (sum / count) and attributes first (attribute_first) or (sum / count)."""

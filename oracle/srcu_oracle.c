@@ -324,9 +324,9 @@ nomem:
 
 /* General voxel path: build_voxel_cells_cpu (voxel.rs:703-716: floor keys,
  * point indices per cell in input order), cells sorted by key (voxel.rs:
- * 352-353), append_voxel_point (voxel.rs:1122-1160): with approximate != 0
+ * 354), append_voxel_point (voxel.rs:1123-1154): with approximate != 0
  * every field is the cell's first point; otherwise positions are
- * average_field (voxel.rs:1162-1171: f64 sum over the indices in order,
+ * average_field (voxel.rs:1156-1165: f64 sum over the indices in order,
  * divided by the count, cast to f32) and the other fields are the first
  * point's (attribute_first) or average_field (attribute average).  The
  * reference only reaches this path for modes other than Centroid + Average

@@ -297,8 +297,8 @@ __device__ __forceinline__ int32_t voxel_agg(const Batch &bt, uint64_t key, uint
 // use it (so the default mode keeps no extra registers live).
 //   AGG_FAST            (sum * (1.0 / count)) as f32, voxel.rs:531-536
 //   AGG_CENTROID_FIRST  positions (sum / count) as f32 (average_field,
-//                       voxel.rs:1162-1171), other fields from the first point
-//   AGG_FIRST           every field from the first point (voxel.rs:1135-1146)
+//                       voxel.rs:1156-1165), other fields from the first point
+//   AGG_FIRST           every field from the first point (voxel.rs:1144-1146)
 template <int NC, class First>
 __device__ __forceinline__ void write_centroid(const Columns<NC> &cols, const double (&s)[NC],
                                                First first, int32_t agg,

@@ -115,7 +115,7 @@ def test_approximate_first_four_points():
 
 
 def test_centroid_first_policy_divides_and_keeps_first_attribute():
-    # voxel.rs:1122-1171: Centroid + First: positions (f64 sum / count) as f32,
+    # voxel.rs:1123-1165: Centroid + First: positions (f64 sum / count) as f32,
     # attributes from the first point; the key set is the fast path's
     rng = np.random.default_rng(9)
     pts = (rng.random((3000, 3), dtype=np.float32) * F(7)).astype(np.float32)
