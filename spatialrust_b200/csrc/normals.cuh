@@ -400,7 +400,7 @@ __device__ __noinline__ void moments_fp64(const float4 *pts, const uint2 *rg, fl
 // differences): count, sum d, sum d d^T, accumulated in f32 for NM_FLUSH
 // candidates and then folded into FP64; C = S2/n - (S1/n)(S1/n)^T and its
 // eigensolve are FP64.
-__global__ void __launch_bounds__(NM_THREADS, 3) k_normals(Control *ctl, const float4 *pts,
+__global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const float4 *pts,
                                                            const uint32_t *pt_cell,
                                                            const uint2 *ranges,
                                                            const uint64_t *cell_key, Batch bt,
