@@ -628,14 +628,14 @@ def run_e2e(ctx, cloud, args, torch, dev, stream):
     outs = []
     for _ in LEAVES:
         vcols = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(4)]
-        counts = torch.empty(n, dtype=torch.int32).pin_memory()
         ncols = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(4)]
-        ncount = torch.empty(n, dtype=torch.int32).pin_memory()
         attr_out = keep.add((ctypes.c_void_p * 1)(vcols[3].data_ptr()))
+        # the reference's output schema: centroid columns and the four normal
+        # columns (no per-voxel or neighbour counts)
         vout = _native.SrcuVoxelOut(vcols[0].data_ptr(), vcols[1].data_ptr(), vcols[2].data_ptr(),
-                                    ctypes.cast(attr_out, ctypes.c_void_p), 0, counts.data_ptr(), 0)
-        nout = _native.SrcuNormalOut(*[c.data_ptr() for c in ncols], ncount.data_ptr(), 0)
-        outs.append((vcols, counts, ncols, ncount, vout, nout))
+                                    ctypes.cast(attr_out, ctypes.c_void_p), 0, 0, 0)
+        nout = _native.SrcuNormalOut(*[c.data_ptr() for c in ncols], 0, 0)
+        outs.append((vcols, ncols, vout, nout))
     params = [(_native._voxel_params(leaf, None),
                _native._normal_params(RADIUS, 3, VIEWPOINT, False, count_shell=False))
               for leaf in LEAVES]
@@ -646,8 +646,8 @@ def run_e2e(ctx, cloud, args, torch, dev, stream):
     def step():
         for k, (vp, np_) in enumerate(params):
             st = lib.srcu_voxel_normals(ctx.handle, ctypes.byref(hcloud), ctypes.byref(vp),
-                                        ctypes.byref(np_), ctypes.byref(outs[k][4]),
-                                        ctypes.byref(outs[k][5]), ctypes.byref(nv),
+                                        ctypes.byref(np_), ctypes.byref(outs[k][2]),
+                                        ctypes.byref(outs[k][3]), ctypes.byref(nv),
                                         ctypes.byref(stats))
             if st != 0:
                 ctx._check(st)
@@ -665,7 +665,7 @@ def run_e2e(ctx, cloud, args, torch, dev, stream):
     torch.cuda.synchronize()
     ms = start.elapsed_time(end) / steps
     h2d = len(LEAVES) * n * 16
-    d2h = sum(v * (16 + 4 + 16 + 4) for v in voxels)
+    d2h = sum(v * (16 + 16) for v in voxels)
     return dict(value=N_POINTS / (ms / 1e3) / 1e6, unit=UNIT, ms_per_step=ms,
                 h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
                 api="srcu_voxel_normals (include/srcuda.h), pinned host buffers, one call per leaf")

@@ -34,6 +34,12 @@ struct srcu_ctx {
   std::string err;
   Control *ctl = nullptr;       // device
   Control *ctl_host = nullptr;  // pinned mirror for read-back
+  // Side stream for read-backs that overlap later kernels of the same chain,
+  // the event that releases them, and a pinned copy of the control-block head
+  // (epoch, status, point and voxel counts) read once the voxel stage is done.
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_voxel = nullptr;
+  unsigned char *head_host = nullptr;
   int occ_onesweep_v = 1, occ_onesweep_c = 1, occ_normals = 1, occ_seg = 1, occ_cells = 1;
   // input staging (host inputs are copied here)
   DevBuf in[MAX_COLS];
@@ -527,10 +533,12 @@ srcu_status read_control(srcu_ctx *ctx) {
   return fail(ctx, SRCU_ERR_CUDA, "device status 0x%x", st);
 }
 
-srcu_status copy_out(srcu_ctx *ctx, void *dst, const void *src, size_t bytes, int on_device) {
+srcu_status copy_out(srcu_ctx *ctx, void *dst, const void *src, size_t bytes, int on_device,
+                     cudaStream_t stream = nullptr) {
   if (!dst || bytes == 0) return SRCU_OK;
   CU_TRY(cudaMemcpyAsync(dst, src, bytes,
-                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                         stream ? stream : ctx->stream));
   return SRCU_OK;
 }
 
@@ -554,14 +562,16 @@ srcu_status check_normal_params(srcu_ctx *ctx, const srcu_normal_params *np) {
   return SRCU_OK;
 }
 
-srcu_status fetch_voxels(srcu_ctx *ctx, uint32_t nc, const srcu_voxel_out *out, uint64_t v) {
+srcu_status fetch_voxels(srcu_ctx *ctx, uint32_t nc, const srcu_voxel_out *out, uint64_t v,
+                         cudaStream_t stream = nullptr, bool keys = true) {
   if (!out) return SRCU_OK;
   float *dst[MAX_COLS] = {out->x, out->y, out->z};
   for (uint32_t a = 3; a < nc; ++a) dst[a] = out->attrs ? out->attrs[a - 3] : nullptr;
   for (uint32_t c = 0; c < nc; ++c)
-    ST_TRY(copy_out(ctx, dst[c], ctx->vout[c].p, v * 4, out->on_device));
-  ST_TRY(copy_out(ctx, out->counts, ctx->vcounts.p, v * 4, out->on_device));
-  if (out->keys) ST_TRY(copy_out(ctx, out->keys, ctx->vkeys3.p, v * 24, out->on_device));
+    ST_TRY(copy_out(ctx, dst[c], ctx->vout[c].p, v * 4, out->on_device, stream));
+  ST_TRY(copy_out(ctx, out->counts, ctx->vcounts.p, v * 4, out->on_device, stream));
+  if (keys && out->keys)
+    ST_TRY(copy_out(ctx, out->keys, ctx->vkeys3.p, v * 24, out->on_device, stream));
   return SRCU_OK;
 }
 
@@ -627,6 +637,11 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
   ctx->used += sizeof(Control);
   if (cudaMemset(ctx->ctl, 0, sizeof(Control)) != cudaSuccess) return bail(SRCU_ERR_CUDA);
   if (cudaMallocHost(&ctx->ctl_host, sizeof(Control)) != cudaSuccess) return bail(SRCU_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_voxel, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost(reinterpret_cast<void **>(&ctx->head_host), offsetof(Control, n_cells)) !=
+          cudaSuccess)
+    return bail(SRCU_ERR_CUDA);
   // Kernels with more than 48 KB of dynamic shared memory opt in once.
   if (cudaFuncSetAttribute(k_sort<VoxelKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            sizeof(OnesweepSmem)) != cudaSuccess ||
@@ -675,6 +690,9 @@ void srcu_destroy(srcu_ctx *ctx) {
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->ctl) cudaFree(ctx->ctl);
   if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
+  if (ctx->head_host) cudaFreeHost(ctx->head_host);
+  if (ctx->ev_voxel) cudaEventDestroy(ctx->ev_voxel);
+  if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -778,16 +796,36 @@ srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
   const Batch bt = make_batch(ctx, 1);
   begin_chain(ctx, n, bt, 1, vparams, nparams);
   ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
+  // The centroids are final once the voxel stage is done: their read-back
+  // runs on the side stream while the normal kernels run.  The host learns V
+  // from a small copy of the control-block head taken at that point.
+  CU_TRY(cudaMemcpyAsync(ctx->head_host, ctx->ctl, offsetof(Control, n_cells),
+                         cudaMemcpyDeviceToHost, ctx->stream));
+  CU_TRY(cudaEventRecord(ctx->ev_voxel, ctx->stream));
   // Normals on the centroids (mvp.rs:220-222); the input bounds contain them.
   ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
                          ptr<float>(ctx->vout[2]), ptr<const float4>(ctx->vaos),
                          &ctx->ctl->n_voxels, n, bt, ptr<uint64_t>(ctx->vkeys)));
   if (vout && vout->keys) ST_TRY(unpack_keys(ctx, n));
-  ST_TRY(read_control(ctx));
+  bool early = false;
+  if (vout) {
+    CU_TRY(cudaEventSynchronize(ctx->ev_voxel));
+    const Control *head = reinterpret_cast<const Control *>(ctx->head_host);
+    if (head->status == 0) {  // otherwise read_control below reports the failure
+      CU_TRY(cudaStreamWaitEvent(ctx->side_stream, ctx->ev_voxel, 0));
+      ST_TRY(fetch_voxels(ctx, nc, vout, head->n_voxels, ctx->side_stream, false));
+      early = true;
+    }
+  }
+  const srcu_status st = read_control(ctx);
+  if (early && st != SRCU_OK) cudaStreamSynchronize(ctx->side_stream);  // no copy outlives the call
+  if (st != SRCU_OK) return st;
   const uint64_t v = ctx->ctl_host->n_voxels;
-  ST_TRY(fetch_voxels(ctx, nc, vout, v));
+  if (!early) ST_TRY(fetch_voxels(ctx, nc, vout, v));
+  else if (vout->keys) ST_TRY(copy_out(ctx, vout->keys, ctx->vkeys3.p, v * 24, vout->on_device));
   ST_TRY(fetch_normals(ctx, nout, v, stats));
   CU_TRY(cudaStreamSynchronize(ctx->stream));
+  CU_TRY(cudaStreamSynchronize(ctx->side_stream));
   if (out_voxels) *out_voxels = v;
   return SRCU_OK;
 }
