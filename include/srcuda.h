@@ -184,6 +184,22 @@ srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
                                const srcu_voxel_out *vout, const srcu_normal_out *nout,
                                uint64_t *out_voxels, srcu_normal_stats *stats);
 
+/* ---- Euclidean clustering on the same grid -------------------------------- */
+
+/* Connected-component roots of the graph "dx*dx + dy*dy + dz*dz <= tol*tol"
+ * (f32): roots[i] is the smallest point index of point i's component, the
+ * result of spatialrust_search::euclidean_cluster_roots
+ * (crates/spatialrust-search/src/uniform_grid.rs:90-139), which
+ * GpuEuclideanClusterExtractor::extract (crates/spatialrust-segmentation/src/
+ * cluster_gpu.rs:31-63) and the Gpu(Cuda) arm of
+ * EuclideanClusterExtractor::extract_with_policy (cluster.rs:156-235, rejected
+ * today at cluster.rs:233-235) turn into labels.  The whole union-find runs on
+ * the device (the reference runs it on the host).  roots: n entries, host or
+ * device memory as cloud->on_device.  cluster_tolerance must be > 0 and
+ * finite.  Synchronous. */
+srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                         float cluster_tolerance, uint32_t *roots);
+
 /* ---- many clouds in one chain ---------------------------------------------- */
 
 /* Enqueues voxel -> normals for `count` clouds in one chain: the clouds'
@@ -344,6 +360,7 @@ typedef enum srcu_kernel_id {
   SRCU_K_HASH,           /* cell hash table */
   SRCU_K_RANGES,         /* 3x3 neighbour column ranges */
   SRCU_K_NORMALS,        /* radius neighbours + covariance + eigensolve */
+  SRCU_K_CLUSTER,        /* Euclidean clustering: union-find over the radius grid */
   SRCU_K_COUNT
 } srcu_kernel_id;
 

@@ -50,6 +50,10 @@ def _load():
     lib.oracle_voxel_general.argtypes = [P, P, P, P, ctypes.c_int, ctypes.c_size_t, ctypes.c_float,
                                          ctypes.c_int, P, ctypes.c_int, ctypes.c_int, P, P, P, P]
     lib.oracle_voxel_general.restype = ctypes.c_int
+    lib.oracle_euclidean_roots.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float, P]
+    lib.oracle_euclidean_roots.restype = ctypes.c_int
+    lib.oracle_euclidean_roots_sparse.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float, P]
+    lib.oracle_euclidean_roots_sparse.restype = ctypes.c_int
     lib.oracle_radius_normals_ref.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float,
                                               ctypes.c_uint32, ctypes.c_int, P, ctypes.c_int, P, P,
                                               P, P, P, P, P]
@@ -153,6 +157,26 @@ def voxel_general(x, y, z, attrs=(), leaf=1.0, origin=None, approximate=False,
         raise OracleError(f"oracle_voxel_general failed: {rc}")
     v = nv.value
     return VoxelResult([o[:v].copy() for o in outs], keys[:v].copy(), counts[:v].copy())
+
+
+def euclidean_roots(x, y, z, tolerance, sparse=False) -> np.ndarray:
+    """Reference grid union-find (uniform_grid.rs:90-139, 262-289, 389-425):
+    the smallest point index of every point's connected component.  sparse:
+    the reference's sparse-cell path (euclidean_cluster.rs:9-58 ->
+    uniform_grid.rs:148-250), which has no dense cell cap."""
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    n = x.shape[0]
+    roots = np.empty(max(n, 1), np.uint32)
+    fn = lib.oracle_euclidean_roots_sparse if sparse else lib.oracle_euclidean_roots
+    rc = fn(_ptr(x), _ptr(y), _ptr(z), n, ctypes.c_float(tolerance), _ptr(roots))
+    if rc == -1:
+        raise OracleError("cluster_tolerance must be positive")
+    if rc == -3:
+        raise OracleError("grid would exceed the reference's dense cell cap")
+    if rc != 0:
+        raise OracleError(f"oracle_euclidean_roots failed: {rc}")
+    return roots[:n].copy()
 
 
 @dataclass

@@ -185,6 +185,18 @@ static int cell_map_get_or_insert(cell_map *m, const int64_t k[3], uint32_t next
   }
 }
 
+/* Id of key k, or UINT32_MAX when absent (read-only probe). */
+static uint32_t cell_map_find(const cell_map *m, const int64_t k[3]) {
+  size_t p = cell_hash(k) & (m->cap - 1);
+  for (;;) {
+    const uint32_t cur = m->ids[p];
+    if (cur == UINT32_MAX) return UINT32_MAX;
+    const int64_t *q = &m->keys[3 * p];
+    if (q[0] == k[0] && q[1] == k[1] && q[2] == k[2]) return cur;
+    p = (p + 1) & (m->cap - 1);
+  }
+}
+
 static const int64_t *g_sort_keys; /* qsort context (single-threaded use) */
 
 static int cmp_cell_ids(const void *a, const void *b) {
@@ -1077,6 +1089,198 @@ void oracle_brute_radius_counts(const float *x, const float *y, const float *z, 
     }
     counts[i] = c;
   }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Euclidean cluster roots (crates/spatialrust-search/src/uniform_grid.rs)   */
+/* ------------------------------------------------------------------------ */
+
+#define OR_ERR_GRID_TOO_LARGE (-3)
+#define UG_MAX_CELLS 64000000ull /* MAX_UNIFORM_GRID_CELLS, uniform_grid.rs:6 */
+
+/* find_root without compression (uniform_grid.rs:420-425) */
+static uint32_t uf_find_readonly(const uint32_t *parent, uint32_t i) {
+  while (parent[i] != i) i = parent[i];
+  return i;
+}
+
+/* union_min_root (uniform_grid.rs:410-418): the larger root joins the smaller */
+static void uf_union_min(uint32_t *parent, uint32_t a, uint32_t b) {
+  const uint32_t ra = uf_find_readonly(parent, a), rb = uf_find_readonly(parent, b);
+  if (ra == rb) return;
+  if (ra < rb) parent[rb] = ra;
+  else parent[ra] = rb;
+}
+
+/* euclidean_cluster_roots (uniform_grid.rs:90-139) on one thread:
+ * grid_bounds (:9-36: f32 min/max, dims = floor(span / cell) + 1, at most
+ * 64M dense cells), build_grid (:44-87: counting sort over dense cells,
+ * clamped floor cells), cluster_roots_sequential (:262-289: every point
+ * unioned with every point of the 27 surrounding cells that passes
+ * dx*dx + dy*dy + dz*dz <= tol*tol, differences neighbour minus point) and
+ * compress_roots (:389-395).  roots[i] is the smallest index of i's
+ * component.  Returns OR_ERR_INVALID for tol <= 0 or NaN, and
+ * OR_ERR_GRID_TOO_LARGE where the reference reports the grid cap. */
+int oracle_euclidean_roots(const float *x, const float *y, const float *z, size_t n, float tol,
+                           uint32_t *roots) {
+  if (!(tol > 0.0f)) return OR_ERR_INVALID;
+  if (n == 0) return OR_OK;
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (size_t i = 0; i < n; ++i) {
+    const float v[3] = {x[i], y[i], z[i]};
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = rs_minf(mn[a], v[a]);
+      mx[a] = rs_maxf(mx[a], v[a]);
+    }
+  }
+  const float inv = 1.0f / tol;
+  uint64_t dims[3];
+  for (int a = 0; a < 3; ++a) {
+    const int64_t span = sat_f32_to_i64(floorf((mx[a] - mn[a]) * inv)) + 1;
+    dims[a] = (uint64_t)(span < 1 ? 1 : (span > 0xFFFFFFFFll ? 0xFFFFFFFFll : span));
+  }
+  const uint64_t cells = dims[0] * dims[1] * dims[2];
+  if (dims[0] > UG_MAX_CELLS || dims[1] > UG_MAX_CELLS || dims[2] > UG_MAX_CELLS ||
+      cells > UG_MAX_CELLS)
+    return OR_ERR_GRID_TOO_LARGE;
+  uint32_t *cell = (uint32_t *)malloc(n * sizeof(uint32_t));
+  uint32_t *start = (uint32_t *)calloc(cells + 1, sizeof(uint32_t));
+  uint32_t *sorted = (uint32_t *)malloc(n * sizeof(uint32_t));
+  uint32_t *parent = (uint32_t *)malloc(n * sizeof(uint32_t));
+  int64_t (*ci)[3] = (int64_t(*)[3])malloc(n * sizeof(int64_t[3]));
+  if (!cell || !start || !sorted || !parent || !ci) {
+    free(cell); free(start); free(sorted); free(parent); free(ci);
+    return OR_ERR_NOMEM;
+  }
+  for (size_t i = 0; i < n; ++i) {
+    const float v[3] = {x[i], y[i], z[i]};
+    for (int a = 0; a < 3; ++a) {
+      int64_t c = sat_f32_to_i64(floorf((v[a] - mn[a]) * inv));
+      if (c < 0) c = 0;
+      if (c > (int64_t)dims[a] - 1) c = (int64_t)dims[a] - 1;
+      ci[i][a] = c;
+    }
+    cell[i] = (uint32_t)(((uint64_t)ci[i][2] * dims[1] + (uint64_t)ci[i][1]) * dims[0] +
+                         (uint64_t)ci[i][0]);
+    start[cell[i]]++;
+  }
+  uint32_t acc = 0;
+  for (uint64_t c = 0; c <= cells; ++c) {
+    const uint32_t k = start[c];
+    start[c] = acc;
+    acc += k;
+  }
+  {
+    uint32_t *cursor = (uint32_t *)malloc((cells + 1) * sizeof(uint32_t));
+    memcpy(cursor, start, (cells + 1) * sizeof(uint32_t));
+    for (size_t i = 0; i < n; ++i) sorted[cursor[cell[i]]++] = (uint32_t)i;
+    free(cursor);
+  }
+  for (size_t i = 0; i < n; ++i) parent[i] = (uint32_t)i;
+  const float r2 = tol * tol;
+  for (size_t i = 0; i < n; ++i) {
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int64_t cx = ci[i][0] + dx, cy = ci[i][1] + dy, cz = ci[i][2] + dz;
+          if (cx < 0 || cy < 0 || cz < 0 || cx >= (int64_t)dims[0] || cy >= (int64_t)dims[1] ||
+              cz >= (int64_t)dims[2])
+            continue;
+          const uint64_t c = ((uint64_t)cz * dims[1] + (uint64_t)cy) * dims[0] + (uint64_t)cx;
+          for (uint32_t s = start[c]; s < start[c + 1]; ++s) {
+            const uint32_t j = sorted[s];
+            const float ddx = x[j] - x[i], ddy = y[j] - y[i], ddz = z[j] - z[i];
+            if (ddx * ddx + ddy * ddy + ddz * ddz <= r2) uf_union_min(parent, (uint32_t)i, j);
+          }
+        }
+  }
+  for (size_t i = 0; i < n; ++i) roots[i] = uf_find_readonly(parent, (uint32_t)i);
+  free(cell); free(start); free(sorted); free(parent); free(ci);
+  return OR_OK;
+}
+
+/* The reference's sparse-cell path (euclidean_cluster_roots_gpu_with_receipt,
+ * crates/spatialrust-gpu/src/kernels/euclidean_cluster.rs:9-58, then
+ * euclidean_cluster_roots_from_segments, uniform_grid.rs:148-250): cells are
+ * voxel keys floor((p - min) * (1 / tol)) with the origin the f32 minimum
+ * starting from point 0, kept in a hash map (no dense cap); every point is
+ * unioned with the points of the 27 neighbouring keys (saturating) that pass
+ * the predicate.  Same roots as the dense grid wherever both run. */
+int oracle_euclidean_roots_sparse(const float *x, const float *y, const float *z, size_t n,
+                                  float tol, uint32_t *roots) {
+  if (!(tol > 0.0f)) return OR_ERR_INVALID;
+  if (n == 0) return OR_OK;
+  float o[3] = {x[0], y[0], z[0]};
+  for (size_t i = 1; i < n; ++i) {
+    o[0] = rs_minf(o[0], x[i]);
+    o[1] = rs_minf(o[1], y[i]);
+    o[2] = rs_minf(o[2], z[i]);
+  }
+  const float inv = 1.0f / tol;
+  cell_map map;
+  if (cell_map_init(&map, n < 16 ? 16 : n) != OR_OK) return OR_ERR_NOMEM;
+  int64_t (*key)[3] = (int64_t(*)[3])malloc(n * sizeof(int64_t[3]));
+  uint32_t *cell = (uint32_t *)malloc(n * sizeof(uint32_t));
+  uint32_t *count = (uint32_t *)calloc(n + 1, sizeof(uint32_t));
+  uint32_t *start = (uint32_t *)malloc((n + 1) * sizeof(uint32_t));
+  uint32_t *members = (uint32_t *)malloc(n * sizeof(uint32_t));
+  uint32_t *parent = (uint32_t *)malloc(n * sizeof(uint32_t));
+  int rc = OR_OK;
+  if (!key || !cell || !count || !start || !members || !parent) {
+    rc = OR_ERR_NOMEM;
+    goto done;
+  }
+  uint32_t ncells = 0;
+  for (size_t i = 0; i < n; ++i) {
+    voxel_key_floor(x[i], y[i], z[i], o, inv, key[i]);
+    uint32_t id;
+    int inserted;
+    if (cell_map_get_or_insert(&map, key[i], ncells, &id, &inserted) != OR_OK) {
+      rc = OR_ERR_NOMEM;
+      goto done;
+    }
+    if (inserted) ncells++;
+    cell[i] = id;
+    count[id]++;
+  }
+  {
+    uint32_t acc = 0;
+    for (uint32_t c = 0; c < ncells; ++c) {
+      start[c] = acc;
+      acc += count[c];
+      count[c] = 0;
+    }
+    start[ncells] = acc;
+    for (size_t i = 0; i < n; ++i) members[start[cell[i]] + count[cell[i]]++] = (uint32_t)i;
+  }
+  for (size_t i = 0; i < n; ++i) parent[i] = (uint32_t)i;
+  {
+    const float r2 = tol * tol;
+    for (size_t i = 0; i < n; ++i)
+      for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int64_t d[3] = {dx, dy, dz};
+            int64_t nk[3];
+            for (int a = 0; a < 3; ++a) {
+              const int64_t k = key[i][a];  /* saturating_add */
+              nk[a] = (d[a] > 0 && k == INT64_MAX) ? INT64_MAX
+                      : (d[a] < 0 && k == INT64_MIN) ? INT64_MIN : k + d[a];
+            }
+            const uint32_t id = cell_map_find(&map, nk);
+            if (id == UINT32_MAX) continue;
+            for (uint32_t s2 = start[id]; s2 < start[id + 1]; ++s2) {
+              const uint32_t j = members[s2];
+              const float ddx = x[j] - x[i], ddy = y[j] - y[i], ddz = z[j] - z[i];
+              if (ddx * ddx + ddy * ddy + ddz * ddz <= r2) uf_union_min(parent, (uint32_t)i, j);
+            }
+          }
+  }
+  for (size_t i = 0; i < n; ++i) roots[i] = uf_find_readonly(parent, (uint32_t)i);
+done:
+  free(key); free(cell); free(count); free(start); free(members); free(parent);
+  cell_map_free(&map);
+  return rc;
 }
 
 /* Exposes the f32 closed-form smallest eigenpair for unit tests. */

@@ -14,6 +14,8 @@ from .features import (GpuNormalEstimator, NormalEstimationConfig, NormalEstimat
                        NormalEstimator, build_output_cloud)
 from .filtering import (AttributeAggregation, VoxelAggregationMode, VoxelGridDownsample,
                         VoxelGridDownsampleConfig)
+from .segmentation import (EuclideanClusterConfig, EuclideanClusterExtractor,
+                           EuclideanClusterResult, GpuEuclideanClusterExtractor)
 
 __all__ = [
     "Auto", "AttributeAggregation", "BufferLengthMismatch", "CpuParallel", "CpuSingle",
@@ -22,5 +24,6 @@ __all__ = [
     "NormalEstimationConfig", "NormalEstimationResult", "NormalEstimator", "PointCloud",
     "PointCloudBuilder", "PointField", "PointSchema", "SpatialError", "StandardSchemas",
     "TransferDirection", "UnsupportedDType", "VoxelAggregationMode", "VoxelGridDownsample",
-    "VoxelGridDownsampleConfig", "build_output_cloud",
+    "VoxelGridDownsampleConfig", "build_output_cloud", "EuclideanClusterConfig",
+    "EuclideanClusterExtractor", "EuclideanClusterResult", "GpuEuclideanClusterExtractor",
 ]

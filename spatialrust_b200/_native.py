@@ -158,7 +158,7 @@ class SrcuServerStats(ctypes.Structure):
 
 KERNEL_IDS = ["begin", "bounds", "voxel_plan", "voxel_hist", "voxel_sort", "voxel_segments",
               "unpack_keys", "cell_plan", "cell_hist", "cell_sort", "cells", "hash", "ranges",
-              "normals"]
+              "normals", "cluster"]
 
 
 # Every symbol include/srcuda.h declares, with its ctypes signature.
@@ -206,6 +206,8 @@ SIGNATURES = {
                                      _P], ctypes.c_int),
     "srcu_profile_read": ([_P, ctypes.POINTER(SrcuKernelStat), ctypes.c_int, ctypes.c_int],
                           ctypes.c_int),
+    "srcu_euclidean_cluster_roots": ([_P, ctypes.POINTER(SrcuCloud), ctypes.c_float,
+                                      ctypes.c_void_p], ctypes.c_int),
     "srcu_server_create": ([ctypes.POINTER(SrcuServerConfig), ctypes.POINTER(ctypes.c_void_p)],
                            ctypes.c_int),
     "srcu_server_destroy": ([_P], None),
@@ -415,6 +417,23 @@ class Context:
         self._check(self._lib.srcu_radius_normals(self._h, ctypes.byref(cloud), ctypes.byref(np_),
                                                   ctypes.byref(nout), ctypes.byref(stats)))
         return (*[o[:n] for o in outs], counts[:n], _stats(stats))
+
+    def euclidean_cluster_roots(self, x, y, z, cluster_tolerance: float):
+        """Smallest point index of every point's component (numpy in and out,
+        or CUDA tensors in and a CUDA tensor out)."""
+        keep = _Keep()
+        cloud = make_cloud(x, y, z, (), keep)
+        n = int(cloud.n)
+        if cloud.on_device:
+            import torch
+            roots = torch.empty(max(n, 1), dtype=torch.int32, device=x.device)
+            addr = roots.data_ptr()
+        else:
+            roots = np.empty(max(n, 1), np.uint32)
+            addr = roots.ctypes.data
+        self._check(self._lib.srcu_euclidean_cluster_roots(self._h, ctypes.byref(cloud),
+                                                           ctypes.c_float(cluster_tolerance), addr))
+        return roots[:n]
 
     def voxel_normals(self, x, y, z, attrs=(), leaf: float = 1.0, origin=None, radius: float = 0.5,
                       min_neighbors: int = 3, viewpoint=None, include_self: bool = False,

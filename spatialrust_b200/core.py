@@ -70,6 +70,7 @@ class FieldSemantic(enum.Enum):
     ColorR = "r"
     ColorG = "g"
     ColorB = "b"
+    Label = "label"
     Custom = "custom"
 
 

@@ -65,6 +65,9 @@ __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ void st_relaxed_u32(uint32_t *p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 // Decoupled look-back words: [epoch:32][flag:2][count:30].  The epoch makes
 // words left over from earlier launches read as "not yet published", so the

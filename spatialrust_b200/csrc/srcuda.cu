@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/srcuda.h"
+#include "cluster.cuh"
 #include "normals.cuh"
 #include "voxel.cuh"
 
@@ -53,6 +54,7 @@ struct srcu_ctx {
   uint32_t table_log2 = 0;
   // normals outputs
   DevBuf nout[4], ncounts;
+  DevBuf parent;  // union-find parents (Euclidean clustering)
   uint32_t last_attrs = 0;  // attribute count of the last enqueued chain
   const float *frame_attr_ptrs[MAX_COLS] = {};
   // batch arrays (clouds of the last chain) and pinned staging for their parameters
@@ -151,7 +153,7 @@ const char *const kKernelNames[SRCU_K_COUNT] = {
     "k_begin",          "k_bounds",        "k_voxel_plan",  "(in k_sort<voxel>)",
     "k_sort<voxel>",    "k_voxel_segments", "k_unpack_voxel_keys", "k_cell_plan",
     "(in k_sort<cell>)", "k_sort<cell>",    "k_cells",       "k_column_insert",
-    "k_ranges",         "k_normals"};
+    "k_ranges",         "k_normals",       "k_cluster_union"};
 
 // Counts the launches of one kernel group and, when its bit is set in
 // prof_mask, brackets them with CUDA events on the context stream.
@@ -449,9 +451,10 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
 
 // Normals stage over (x, y, z) with the point count in *count_dev (device)
 // or ctl->n_points when count_dev is null; n_max bounds the grid sizes.
-srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const float *z,
-                            const float4 *aos, const unsigned long long *count_dev, uint64_t n_max,
-                            const Batch &bt, const uint64_t *voxel_keys) {
+// Radius grid: cell plans, cell sort, cell table, column hash, column ranges.
+srcu_status enqueue_grid(srcu_ctx *ctx, const float *x, const float *y, const float *z,
+                         const float4 *aos, const unsigned long long *count_dev, uint64_t n_max,
+                         const Batch &bt, const uint64_t *voxel_keys) {
   {
     Launch l(ctx, SRCU_K_CELL_PLAN);
     k_cell_plans<<<ceil_div(bt.clouds, 128), 128, 0, ctx->stream>>>(ctx->ctl, bt);
@@ -490,6 +493,14 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
                                               ptr<uint64_t>(ctx->table), ctx->table_log2,
                                               ptr<uint2>(ctx->ranges), bt);
   }
+  CU_TRY(cudaGetLastError());
+  return SRCU_OK;
+}
+
+srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const float *z,
+                            const float4 *aos, const unsigned long long *count_dev, uint64_t n_max,
+                            const Batch &bt, const uint64_t *voxel_keys) {
+  ST_TRY(enqueue_grid(ctx, x, y, z, aos, count_dev, n_max, bt, voxel_keys));
   const uint32_t grid_n = uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals);
   Launch l(ctx, SRCU_K_NORMALS);
   k_normals<<<grid_n, NM_THREADS, 0, ctx->stream>>>(
@@ -675,7 +686,7 @@ void srcu_destroy(srcu_ctx *ctx) {
   DevBuf *all[] = {&ctx->in_aos, &ctx->vaos, &ctx->keys[0], &ctx->keys[1], &ctx->vals[0], &ctx->vals[1], &ctx->lb_sort,
                    &ctx->lb_seg, &ctx->lb_cells, &ctx->vkeys, &ctx->vcounts, &ctx->vkeys3,
                    &ctx->pts, &ctx->pt_cell, &ctx->cell_key, &ctx->cell_start, &ctx->table, &ctx->ranges,
-                   &ctx->ncounts};
+                   &ctx->ncounts, &ctx->parent};
   for (DevBuf *b : all) release(ctx, *b);
   for (auto &b : ctx->in) release(ctx, b);
   for (auto &b : ctx->vout) release(ctx, b);
@@ -770,6 +781,59 @@ srcu_status srcu_radius_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
                          bt, nullptr));
   ST_TRY(read_control(ctx));
   ST_TRY(fetch_normals(ctx, out, n, stats));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  return SRCU_OK;
+}
+
+srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                         float cluster_tolerance, uint32_t *roots) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  ST_TRY(check_cloud(ctx, cloud));
+  // uniform_grid.rs:103-105 (an infinite tolerance has no grid here)
+  if (!(cluster_tolerance > 0.0f) || cluster_tolerance == INFINITY)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "cluster_tolerance must be positive and finite");
+  CU_TRY(cudaSetDevice(ctx->device));
+  const uint64_t n = cloud->n;
+  if (n == 0) return SRCU_OK;  // uniform_grid.rs:100-102
+  if (!roots) return fail(ctx, SRCU_ERR_MISSING_FIELD, "roots is NULL");
+  ST_TRY(reserve(ctx, n, 3, !cloud->on_device, false, true));
+  ST_TRY(reserve_batch(ctx, 1));
+  ST_TRY(ensure(ctx, ctx->parent, n * 4));
+  srcu_cloud xyz = *cloud;
+  xyz.n_attrs = 0;
+  const float *cols[MAX_COLS];
+  ST_TRY(stage_input(ctx, &xyz, cols));
+  const Batch bt = make_batch(ctx, 1);
+  srcu_normal_params np{};
+  np.radius = cluster_tolerance;  // the grid of a radius search with r = tolerance
+  np.min_neighbors = 1;
+  begin_chain(ctx, n, bt, 1, nullptr, &np);
+  const uint32_t grid_b = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4),
+                                                                    uint32_t(ctx->num_sms) * 8));
+  {
+    Launch l(ctx, SRCU_K_BOUNDS);
+    k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(cols[0], cols[1], cols[2], ctx->ctl, nullptr,
+                                                       nullptr, ptr<float4>(ctx->in_aos), bt);
+  }
+  ST_TRY(enqueue_grid(ctx, cols[0], cols[1], cols[2], ptr<const float4>(ctx->in_aos), nullptr, n,
+                      bt, nullptr));
+  const float r2 = cluster_tolerance * cluster_tolerance;  // radius_sq, uniform_grid.rs:109
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, CL_THREADS),
+                                                                  uint32_t(ctx->num_sms) * 8));
+  uint32_t *dst = cloud->on_device ? roots : ptr<uint32_t>(ctx->nout[0]);
+  {
+    Launch l(ctx, SRCU_K_CLUSTER);
+    k_cluster_init<<<grid, CL_THREADS, 0, ctx->stream>>>(ctx->ctl, ptr<uint32_t>(ctx->parent),
+                                                         nullptr);
+    k_cluster_union<<<grid, CL_THREADS, 0, ctx->stream>>>(
+        ctx->ctl, ptr<const float4>(ctx->pts), ptr<const uint32_t>(ctx->pt_cell),
+        ptr<const uint2>(ctx->ranges), nullptr, r2, ptr<uint32_t>(ctx->parent));
+    k_cluster_roots<<<grid, CL_THREADS, 0, ctx->stream>>>(ctx->ctl, ptr<uint32_t>(ctx->parent), dst,
+                                                          nullptr);
+  }
+  CU_TRY(cudaGetLastError());
+  ST_TRY(read_control(ctx));
+  if (!cloud->on_device) ST_TRY(copy_out(ctx, roots, dst, n * 4, 0));
   CU_TRY(cudaStreamSynchronize(ctx->stream));
   return SRCU_OK;
 }

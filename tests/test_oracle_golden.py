@@ -132,6 +132,61 @@ def test_centroid_first_policy_divides_and_keeps_first_attribute():
         assert g.fields[3][row] == inten[m[0]]
 
 
+def test_cluster_long_chain_is_one_component():
+    # uniform_grid.rs:564-576: 300 points spaced 1.0 on x, tolerance 1.5 -> all root 0
+    x = np.arange(300, dtype=F)
+    zero = np.zeros(300, F)
+    assert np.all(oracle.euclidean_roots(x, zero, zero, 1.5) == 0)
+
+
+def test_cluster_prebuilt_segments_example():
+    # uniform_grid.rs:578-597: x = 0, 0.5, 2.0, tolerance 1.0 -> roots 0, 0, 2
+    x = np.array([0.0, 0.5, 2.0], F)
+    zero = np.zeros(3, F)
+    assert oracle.euclidean_roots(x, zero, zero, 1.0).tolist() == [0, 0, 2]
+
+
+def test_cluster_three_separated_clusters():
+    # cluster.rs:370-383 / cluster_gpu.rs:90-101: three 3x3 grids 10 m apart,
+    # tolerance 1.5 -> three components of 9 points
+    pts = [(cx + dx, cy + dy, 0.0) for cx, cy in ((0, 0), (10, 0), (0, 10))
+           for dx in range(3) for dy in range(3)]
+    p = np.array(pts, F)
+    roots = oracle.euclidean_roots(p[:, 0], p[:, 1], p[:, 2], 1.5)
+    assert sorted(np.unique(roots, return_counts=True)[1].tolist()) == [9, 9, 9]
+    assert np.unique(roots).tolist() == [0, 9, 18]
+
+
+def test_cluster_roots_match_brute_force_components():
+    # the component structure of the f32 predicate, by brute-force flood fill
+    rng = np.random.default_rng(4)
+    p = (rng.random((400, 3)) * 6).astype(F)
+    tol = F(0.55)
+    roots = oracle.euclidean_roots(p[:, 0], p[:, 1], p[:, 2], tol)
+    d = p[None, :, :] - p[:, None, :]
+    adj = ((d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]) <= tol * tol
+    expect = np.full(400, -1)
+    for s in range(400):
+        if expect[s] >= 0:
+            continue
+        stack, expect[s] = [s], s
+        while stack:
+            i = stack.pop()
+            for j in np.nonzero(adj[i])[0]:
+                if expect[j] < 0:
+                    expect[j] = s
+                    stack.append(j)
+    assert roots.tolist() == expect.tolist()
+    sparse = oracle.euclidean_roots(p[:, 0], p[:, 1], p[:, 2], tol, sparse=True)
+    assert sparse.tolist() == expect.tolist()
+
+
+def test_cluster_rejects_non_positive_tolerance():
+    x = np.zeros(3, F)
+    with pytest.raises(oracle.OracleError):
+        oracle.euclidean_roots(x, x, x, 0.0)
+
+
 def test_plane_normals_upward_radius():
     # normal.rs:650-667 uses k=8 on a 5x5 unit grid; the radius-mode analogue
     # (r = 1.5 covers the 8-neighbourhood) must give the same upward normals.
