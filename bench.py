@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--batched-clouds", type=int, default=256)
     ap.add_argument("--no-shapes", action="store_true",
                     help="skip the 5M-point shapes radius-normals measurement")
+    ap.add_argument("--no-cluster", action="store_true",
+                    help="skip the Euclidean cluster-roots measurement")
     ap.add_argument("--no-serving", action="store_true",
                     help="skip the serving-loop (Poisson arrivals) measurement")
     ap.add_argument("--serving-rates", default="100,500,1000,2000",
@@ -382,6 +384,8 @@ def run_gpu(args):
         line["batched"] = run_batched(args, torch, dev, stream)
     if not args.no_shapes:
         line["shapes"] = run_shapes(args, torch, dev, stream)
+    if not args.no_cluster and rank == 0:
+        line["cluster"] = run_cluster(args, torch, dev, stream, cloud)
     if not args.no_serving:
         line["serving"] = run_serving(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -512,6 +516,52 @@ def run_shapes(args, torch, dev, stream):
                 neighbours=dict(mean=float(nb.mean()), p5=pct[0], p25=pct[1], p50=pct[2],
                                 p75=pct[3], p95=pct[4], max=int(nb.max())),
                 stats=_native._stats(stats))
+
+
+def run_cluster(args, torch, dev, stream, cloud):
+    """Euclidean cluster roots (srcu_euclidean_cluster_roots) on the 2M-point
+    georeferenced scan at tolerance 0.1 and 0.3 m, device-resident; its CPU
+    baseline is the reference's sparse-cell union-find (C restatement, one
+    thread) on the same points."""
+    import oracle
+    from spatialrust_b200 import _native
+    lib = _native.load()
+    n = cloud.n
+    cols = [torch.from_numpy(a).to(dev) for a in (cloud.x, cloud.y, cloud.z)]
+    roots = torch.empty(n, dtype=torch.int32, device=dev)
+    keep = _native._Keep()
+    dcloud = _native.make_cloud(cols[0], cols[1], cols[2], [], keep)
+    ctx = _native.Context(dev.index)
+    ctx.set_stream(stream.cuda_stream)
+    out = dict(workload="georef_scan_2M: Euclidean cluster roots", points=n, tolerances=[])
+    for tol in (0.1, 0.3):
+        def step():
+            ctx._check(lib.srcu_euclidean_cluster_roots(ctx.handle, ctypes.byref(dcloud),
+                                                        ctypes.c_float(tol), roots.data_ptr()))
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(5):
+            step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / 5
+        r = roots.cpu().numpy().view(np.uint32)
+        entry = dict(tolerance=tol, ms=ms, mpts_s=n / ms / 1e3,
+                     components=int(len(np.unique(r))))
+        if not args.no_cpu_baseline:
+            t0 = time.perf_counter()
+            oracle.euclidean_roots(cloud.x, cloud.y, cloud.z, tol, sparse=True)
+            cpu_s = time.perf_counter() - t0
+            entry["cpu_baseline"] = dict(
+                value=n / cpu_s / 1e6, unit="Mpoints/s", cores=1, kind="port",
+                sample=f"all {n} points once: the reference's sparse-cell union-find "
+                       "(euclidean_cluster.rs -> uniform_grid.rs:148-250), C restatement")
+        out["tolerances"].append(entry)
+    ctx.close()
+    return out
 
 
 def run_serving(args, device):
