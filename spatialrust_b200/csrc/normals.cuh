@@ -66,6 +66,39 @@ __global__ void k_cell_plans(Control *ctl, Batch bt) {
   if (total + ctl->cloud_bits > 64) atomicOr(&ctl->status, ST_KEY_OVERFLOW);
 }
 
+// Places every cloud's (cx, cy) columns in one dense table when all of them
+// fit its `capacity` slots: col_base per cloud by a block scan over clouds.
+// Otherwise the chain keeps the column hash.  One block.
+__global__ void k_column_base(Control *ctl, Batch bt, uint64_t capacity) {
+  if (ld_relaxed_u32(&ctl->status)) return;
+  __shared__ unsigned long long scratch[256];
+  unsigned long long running = 0;
+  for (uint32_t b0 = 0; b0 < bt.clouds; b0 += 256) {
+    const uint32_t b = b0 + threadIdx.x;
+    unsigned long long cols = 0;
+    if (b < bt.clouds) cols = (unsigned long long)bt.cplans[b].dims[0] * bt.cplans[b].dims[1];
+    scratch[threadIdx.x] = cols;
+    __syncthreads();
+    for (uint32_t off = 1; off < 256; off <<= 1) {  // inclusive Hillis-Steele scan
+      const unsigned long long v = threadIdx.x >= off ? scratch[threadIdx.x - off] : 0ull;
+      __syncthreads();
+      scratch[threadIdx.x] += v;
+      __syncthreads();
+    }
+    if (b < bt.clouds) bt.cplans[b].col_base = running + scratch[threadIdx.x] - cols;
+    running += scratch[255];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    ctl->col_total = running;
+    ctl->dense_cols = running <= capacity ? 1u : 0u;
+  }
+}
+
+__device__ __forceinline__ uint64_t dense_column(const CellPlan &pl, uint64_t cx, uint64_t cy) {
+  return pl.col_base + cx * pl.dims[1] + cy;
+}
+
 // Key source for the cell sort over `count_dev` points (V for the chained
 // voxel -> normals path, n otherwise).  The cloud of point i comes from its
 // packed voxel key (chained path) or from the batch offsets.
@@ -219,13 +252,24 @@ __global__ void k_column_insert(Control *ctl, const uint64_t *cell_key, uint64_t
   const uint32_t epoch = ctl->epoch + EP_CELLS;
   const uint32_t lb = ctl->ckey_bits;
   const uint32_t mask = (1u << log2cap) - 1u;
+  const bool dense = ctl->dense_cols != 0;
   for (uint64_t u = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; u < u_count;
        u += uint64_t(gridDim.x) * blockDim.x) {
     const uint64_t full = cell_key[u];
-    const uint64_t col = full & column_mask(bt, cloud_of_key(full, bt, lb));
+    const uint32_t b = cloud_of_key(full, bt, lb);
+    const uint64_t col = full & column_mask(bt, b);
     if (u > 0) {
       const uint64_t prev = cell_key[u - 1];
       if ((prev & column_mask(bt, cloud_of_key(prev, bt, lb))) == col) continue;
+    }
+    if (dense) {  // one slot per column: a plain store
+      const CellPlan &pl = bt.cplans[b < bt.clouds ? b : 0];
+      uint32_t cx, cy, cz;
+      cell_unpack(pl, full & (lb >= 64 ? ~0ull : ((1ull << lb) - 1)), cx, cy, cz);
+      const uint64_t idx = dense_column(pl, cx, cy);
+      if (idx <= mask) table[idx] = (uint64_t(epoch) << 32) | u;
+      else atomicOr(&ctl->status, ST_INTERNAL);
+      continue;
     }
     uint32_t h = cell_hash(col, log2cap);
     const uint64_t mine = (uint64_t(epoch) << 32) | u;
@@ -267,53 +311,82 @@ __device__ __forceinline__ int64_t column_lookup(const uint64_t *table, const ui
 // For every occupied cell and each of the 3x3 neighbouring columns, the range
 // of cell-sorted points in cells (cx+dx, cy+dy, cz-1 .. cz+1).  Those (at
 // most three) cells are consecutive in key order, so each column is one
-// contiguous range: 9 ranges cover the 27-cell neighbourhood.  The centre
-// column holds the cell itself (its z neighbours are its key-order
-// neighbours); another column is found through the column hash and searched
-// from its first cell by galloping over the sorted cell keys.
-__global__ void k_ranges(Control *ctl, const uint64_t *cell_key, const uint32_t *cell_start,
-                         const uint64_t *table, uint32_t log2cap, uint2 *ranges, Batch bt) {
+// contiguous range: 9 ranges cover the 27-cell neighbourhood.  One thread per
+// cell: the key is unpacked once; the centre column holds the cell itself
+// (its z neighbours are its key-order neighbours); the other eight columns
+// are probed in the column hash with all eight slot loads in flight at once,
+// then searched from their first cell by galloping over the sorted keys.
+__global__ void __launch_bounds__(256) k_ranges(Control *ctl, const uint64_t *cell_key,
+                                                const uint32_t *cell_start, const uint64_t *table,
+                                                uint32_t log2cap, uint2 *ranges, Batch bt) {
   if (ld_relaxed_u32(&ctl->status)) return;
   const uint64_t u_count = ctl->n_cells;
   const uint32_t epoch = ctl->epoch + EP_CELLS;
   const uint32_t lb = ctl->ckey_bits;
   const uint64_t local_mask = lb >= 64 ? ~0ull : ((1ull << lb) - 1);
-  const uint64_t total = u_count * 9;
-  const bool narrow = total <= 0xFFFFFFFFull;  // 32-bit index math (no 64-bit divide)
-  for (uint64_t w = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; w < total;
-       w += uint64_t(gridDim.x) * blockDim.x) {
-    uint64_t u;
-    uint32_t col;
-    if (narrow) {
-      const uint32_t u32 = uint32_t(w) / 9u;
-      u = u32;
-      col = uint32_t(w) - u32 * 9u;
-    } else {
-      u = w / 9;
-      col = uint32_t(w - u * 9);
-    }
+  const uint32_t tmask = (1u << log2cap) - 1u;
+  const bool dense = ctl->dense_cols != 0;
+  for (uint64_t u = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; u < u_count;
+       u += uint64_t(gridDim.x) * blockDim.x) {
     const uint64_t full = cell_key[u];
     const uint32_t b = cloud_of_key(full, bt, lb);
     const CellPlan &pl = bt.cplans[b < bt.clouds ? b : 0];
+    const uint32_t dims0 = pl.dims[0], dims1 = pl.dims[1], dims2 = pl.dims[2];
+    const uint32_t sx = pl.shift_x, sy = pl.shift_y;
     uint32_t cx, cy, cz;
     cell_unpack(pl, full & local_mask, cx, cy, cz);
-    const int64_t nx = int64_t(cx) + int64_t(col / 3) - 1;
-    const int64_t ny = int64_t(cy) + int64_t(col % 3) - 1;
-    uint2 rg = make_uint2(0, 0);
-    if (col == 4) {
+    const uint64_t cmask = ~((1ull << pl.bits[2]) - 1ull);
+    const uint64_t zlo = cz > 0 ? cz - 1 : 0;
+    const uint64_t zhi = cz + 1 < dims2 ? cz + 1 : cz;
+    uint2 *out = ranges + size_t(u) * 9;
+    // centre column
+    {
       uint64_t first = u, last = u;
       if (cz > 0 && u > 0 && cell_key[u - 1] == full - 1) first = u - 1;
-      if (cz + 1 < pl.dims[2] && u + 1 < u_count && cell_key[u + 1] == full + 1) last = u + 1;
-      rg = make_uint2(cell_start[first], cell_start[last + 1]);
-    } else if (nx >= 0 && ny >= 0 && nx < pl.dims[0] && ny < pl.dims[1]) {
-      const uint64_t cmask = column_mask(bt, b);
-      const uint64_t ckey =
-          with_cloud((uint64_t(nx) << pl.shift_x) | (uint64_t(ny) << pl.shift_y), b, lb);
-      const int64_t f = column_lookup(table, cell_key, ckey, cmask, log2cap, epoch);
+      if (cz + 1 < dims2 && u + 1 < u_count && cell_key[u + 1] == full + 1) last = u + 1;
+      out[4] = make_uint2(cell_start[first], cell_start[last + 1]);
+    }
+    // the other eight: column keys and first probes (a dense slot, or the
+    // first hash slot), all loads issued together
+    uint64_t ckey[8];
+    uint32_t slot[8];
+    uint64_t word[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int col = k < 4 ? k : k + 1;
+      const int64_t nx = int64_t(cx) + col / 3 - 1;
+      const int64_t ny = int64_t(cy) + col % 3 - 1;
+      const bool inside = nx >= 0 && ny >= 0 && nx < dims0 && ny < dims1;
+      ckey[k] = inside ? with_cloud((uint64_t(nx) << sx) | (uint64_t(ny) << sy), b, lb) : ~0ull;
+      uint64_t idx = cell_hash(ckey[k], log2cap);
+      if (dense) idx = inside ? dense_column(pl, uint64_t(nx), uint64_t(ny)) : 0;
+      slot[k] = uint32_t(idx);
+      word[k] = (inside && idx <= tmask) ? table[idx] : 0ull;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int col = k < 4 ? k : k + 1;
+      uint2 rg = make_uint2(0, 0);
+      int64_t f = -1;
+      if (dense) {
+        if (ckey[k] != ~0ull && uint32_t(word[k] >> 32) == epoch) f = uint32_t(word[k]);
+      } else if (ckey[k] != ~0ull) {
+        // resolve the probe chain from the slot already loaded
+        uint32_t h = slot[k];
+        uint64_t w = word[k];
+        for (uint32_t probe = 0; probe <= tmask; ++probe) {
+          if (uint32_t(w >> 32) != epoch) break;
+          const uint32_t c = uint32_t(w);
+          if ((cell_key[c] & cmask) == ckey[k]) {
+            f = c;
+            break;
+          }
+          h = (h + 1) & tmask;
+          w = table[h];
+        }
+      }
       if (f >= 0) {
-        const uint64_t lo_key = ckey | (cz > 0 ? cz - 1 : 0);
-        const uint64_t hi_key = ckey | (cz + 1 < pl.dims[2] ? cz + 1 : cz);
-        // first cell with key >= lo_key at or after the column head
+        const uint64_t lo_key = ckey[k] | zlo, hi_key = ckey[k] | zhi;
         uint64_t c = uint64_t(f);
         if (cell_key[c] < lo_key) {
           uint64_t step = 1;
@@ -321,7 +394,6 @@ __global__ void k_ranges(Control *ctl, const uint64_t *cell_key, const uint32_t 
             c += step;
             step <<= 1;
           }
-          // cell_key[c] < lo_key <= cell_key[hi] (or hi == u_count)
           uint64_t hi = c + step < u_count ? c + step : u_count;
           while (hi - c > 1) {
             const uint64_t mid = c + ((hi - c) >> 1);
@@ -336,8 +408,8 @@ __global__ void k_ranges(Control *ctl, const uint64_t *cell_key, const uint32_t 
           rg = make_uint2(cell_start[c], cell_start[last + 1]);
         }
       }
+      out[col] = rg;
     }
-    ranges[w] = rg;
   }
 }
 

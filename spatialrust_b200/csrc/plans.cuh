@@ -59,6 +59,7 @@ struct CellPlan {
   float shell_tol;   // 1e-6 * r2
   uint32_t valid;
   uint32_t pad;
+  uint64_t col_base; // first slot of this cloud's columns in the dense column table
 };
 
 // Per-cloud parameters on the device (srcu_voxel_params / srcu_normal_params).
@@ -152,6 +153,9 @@ struct Control {
   SortState csort;  // cell-key sort
   uint32_t hist_v[MAX_DIGITS * RADIX_BINS];  // voxel-key digit histograms
   uint32_t hist_c[MAX_DIGITS * RADIX_BINS];  // cell-key digit histograms
+  unsigned long long col_total;  // sum over clouds of dims_x * dims_y
+  uint32_t dense_cols;           // 1: the column table is dense (it fits the table buffer)
+  uint32_t pad2;
 };
 
 constexpr uint32_t EPOCHS_PER_RUN = 64;

@@ -458,6 +458,7 @@ srcu_status enqueue_grid(srcu_ctx *ctx, const float *x, const float *y, const fl
   {
     Launch l(ctx, SRCU_K_CELL_PLAN);
     k_cell_plans<<<ceil_div(bt.clouds, 128), 128, 0, ctx->stream>>>(ctx->ctl, bt);
+    k_column_base<<<1, 256, 0, ctx->stream>>>(ctx->ctl, bt, uint64_t(1) << ctx->table_log2);
   }
   CellKeySrc src;
   src.x = x;
@@ -484,8 +485,8 @@ srcu_status enqueue_grid(srcu_ctx *ctx, const float *x, const float *y, const fl
     k_column_insert<<<grid_g, 256, 0, ctx->stream>>>(ctx->ctl, ptr<uint64_t>(ctx->cell_key),
                                                      ptr<uint64_t>(ctx->table), ctx->table_log2, bt);
   }
-  const uint32_t grid_r = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n_max * 9, 256),
-                                                                    uint32_t(ctx->num_sms) * 16));
+  const uint32_t grid_r = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n_max, 256),
+                                                                    uint32_t(ctx->num_sms) * 8));
   {
     Launch l(ctx, SRCU_K_RANGES);
     k_ranges<<<grid_r, 256, 0, ctx->stream>>>(ctx->ctl, ptr<uint64_t>(ctx->cell_key),

@@ -111,3 +111,13 @@ def test_argument_errors(cuda_ctx):
         with pytest.raises(sr.InvalidArgument):
             cuda_ctx.euclidean_cluster_roots(x, x, x, bad)
     assert len(cuda_ctx.euclidean_cluster_roots(x[:0], x[:0], x[:0], 1.0)) == 0
+
+
+def test_column_hash_path_on_huge_extent(cuda_ctx):
+    # blobs 100 km apart: too many columns for the dense table (column hash)
+    rng = np.random.default_rng(13)
+    centres = rng.uniform(0, 100_000, (50, 3))
+    p = np.concatenate([c + rng.normal(0, 0.3, (200, 3)) for c in centres]).astype(F)
+    x, y, z = (np.ascontiguousarray(p[:, k]) for k in range(3))
+    assert np.array_equal(cuda_ctx.euclidean_cluster_roots(x, y, z, 0.25),
+                          oracle.euclidean_roots(x, y, z, 0.25, sparse=True))

@@ -246,3 +246,22 @@ def test_device_enqueue_matches_sync_path(cuda_ctx):
     assert np.array_equal(got["curvature"], sync["curvature"])
     assert np.array_equal(got["neighbor_counts"], sync["neighbor_counts"])
     assert got["stats"] == sync["stats"] == stats
+
+
+def test_column_hash_path_on_huge_extent(cuda_ctx):
+    # 100 km across at r = 0.5: the dense column table would need ~4e10
+    # slots, so the chain uses the column hash; counts must still be exact
+    rng = np.random.default_rng(12)
+    blobs = rng.uniform(0, 100_000, (40, 2))
+    pts = []
+    for cx, cy in blobs:
+        p = rng.normal(0, 0.4, (250, 3))
+        p[:, 0] += cx
+        p[:, 1] += cy
+        pts.append(p)
+    p = np.concatenate(pts).astype(np.float32)
+    x, y, z = (np.ascontiguousarray(p[:, k]) for k in range(3))
+    nx, ny, nz, curv, counts, stats = cuda_ctx.radius_normals(x, y, z, 0.5, 3)
+    ref = oracle.brute_radius_counts(x, y, z, 0.5)
+    assert np.array_equal(counts, ref)
+    assert stats["valid_count"] + stats["invalid_count"] == len(x)
