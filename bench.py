@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the many-clouds (batched vs per-cloud loop) measurement")
     ap.add_argument("--batched-clouds", type=int, default=256)
+    ap.add_argument("--batched-scale", type=float, default=1.0,
+                    help="scale of every cloud of the many-clouds measurement (profiling runs)")
+    ap.add_argument("--only-batched", action="store_true",
+                    help="run the many-clouds measurement alone and print its JSON (profiling runs)")
     ap.add_argument("--no-shapes", action="store_true",
                     help="skip the 5M-point shapes radius-normals measurement")
     ap.add_argument("--no-cluster", action="store_true",
@@ -406,7 +410,8 @@ def run_batched(args, torch, dev, stream):
     One batched chain (cloud id in the key high bits), as enqueued and as a
     replayed CUDA graph, against the plain loop of one chain per cloud."""
     from spatialrust_b200 import _native, synthetic
-    clouds, leaves, radii = synthetic.batched_uneven(args.batched_clouds, seed=3)
+    clouds, leaves, radii = synthetic.batched_uneven(args.batched_clouds, seed=3,
+                                                     scale=args.batched_scale)
     n = sum(c.n for c in clouds)
     cols = [torch.from_numpy(np.concatenate([getattr(c, k) for c in clouds])).to(dev)
             for k in ("x", "y", "z", "intensity")]
@@ -723,6 +728,14 @@ def run_e2e(ctx, cloud, args, torch, dev, stream):
 
 def main():
     args = parse()
+    if args.only_batched:
+        import torch
+        torch.cuda.set_device(0)
+        dev = torch.device("cuda", 0)
+        stream = torch.cuda.Stream(dev)
+        torch.cuda.set_stream(stream)
+        print(json.dumps(run_batched(args, torch, dev, stream)), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

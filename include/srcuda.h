@@ -71,6 +71,13 @@ typedef struct srcu_cloud {
   uint32_t n_attrs;
   int32_t on_device;
   uint64_t n;
+  /* f32 elements between consecutive points of every column: 0 or 1 for
+   * packed columns; larger for interleaved records such as the reference's
+   * AoSoA chunks (crates/spatialrust-core/src/tensor_aoso.rs:10-66: [x, y, z,
+   * intensity] stride 4, [x, y, z, nx, ny, nz] stride 6, ...), where x, y, z
+   * and attrs point at the first record's fields.  At most 64. */
+  uint32_t stride;
+  uint32_t reserved;
 } srcu_cloud;
 
 /* VoxelAggregationMode (voxel.rs:68-76) and AttributeAggregation (voxel.rs:78-86). */

@@ -75,7 +75,8 @@ c_float3 = ctypes.c_float * 3
 class SrcuCloud(ctypes.Structure):
     _fields_ = [("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("z", ctypes.c_void_p),
                 ("attrs", ctypes.c_void_p), ("n_attrs", ctypes.c_uint32),
-                ("on_device", ctypes.c_int32), ("n", ctypes.c_uint64)]
+                ("on_device", ctypes.c_int32), ("n", ctypes.c_uint64),
+                ("stride", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 SRCU_VOXEL_CENTROID = 0
@@ -292,7 +293,32 @@ class _Keep:
         return x
 
 
+def make_interleaved_cloud(records, position_offsets=(0, 1, 2), attr_offsets=(),
+                           keep: _Keep | None = None) -> SrcuCloud:
+    """A cloud over interleaved f32 records (n, stride): numpy (host) or a CUDA
+    tensor (device), e.g. the reference's AoSoA [x, y, z, intensity] chunks."""
+    keep = keep or _Keep()
+    on_dev = _is_device(records)
+    if not on_dev:
+        records = keep.add(np.ascontiguousarray(records, dtype=np.float32))
+    if records.ndim != 2:
+        raise InvalidArgument("interleaved records must be a 2-D (n, stride) array")
+    n, stride = int(records.shape[0]), int(records.shape[1])
+    offs = list(position_offsets) + list(attr_offsets)
+    if any(o < 0 or o >= stride for o in offs):
+        raise InvalidArgument("field offsets must lie inside one record")
+    base = _addr(records)
+    ptrs = [base + 4 * o for o in offs]
+    attr_arr = keep.add((ctypes.c_void_p * max(len(attr_offsets), 1))(*ptrs[3:]))
+    return SrcuCloud(ptrs[0], ptrs[1], ptrs[2], ctypes.cast(attr_arr, ctypes.c_void_p),
+                     len(attr_offsets), int(on_dev), n, stride, 0)
+
+
 def make_cloud(x, y, z, attrs: Sequence = (), keep: _Keep | None = None) -> SrcuCloud:
+    """SoA columns -> SrcuCloud; a SrcuCloud passed as x is returned as is
+    (e.g. one from make_interleaved_cloud)."""
+    if isinstance(x, SrcuCloud):
+        return x
     keep = keep or _Keep()
     on_dev = _is_device(x)
     cols = [x, y, z, *attrs]
@@ -388,7 +414,7 @@ class Context:
         keep = _Keep()
         cloud = make_cloud(x, y, z, attrs, keep)
         n = int(cloud.n)
-        ncol = 3 + len(attrs)
+        ncol = 3 + int(cloud.n_attrs)
         outs = [np.empty(max(n, 1), np.float32) for _ in range(ncol)]
         counts = np.empty(max(n, 1), np.uint32)
         keys = np.empty((max(n, 1), 3), np.int64) if want_keys else None
@@ -426,7 +452,7 @@ class Context:
         n = int(cloud.n)
         if cloud.on_device:
             import torch
-            roots = torch.empty(max(n, 1), dtype=torch.int32, device=x.device)
+            roots = torch.empty(max(n, 1), dtype=torch.int32, device=torch.device("cuda", self.device))
             addr = roots.data_ptr()
         else:
             roots = np.empty(max(n, 1), np.uint32)
@@ -442,7 +468,7 @@ class Context:
         keep = _Keep()
         cloud = make_cloud(x, y, z, attrs, keep)
         n = int(cloud.n)
-        ncol = 3 + len(attrs)
+        ncol = 3 + int(cloud.n_attrs)
         vcols = [np.empty(max(n, 1), np.float32) for _ in range(ncol)]
         counts = np.empty(max(n, 1), np.uint32)
         keys = np.empty((max(n, 1), 3), np.int64) if want_keys else None

@@ -114,6 +114,7 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
   if (cloud->n > NA_MAX_POINTS) return SRCU_ERR_INVALID_ARGUMENT;  // beyond the scratch size
   if (cloud->n_attrs > MAX_COLS - 3) return SRCU_ERR_INVALID_ARGUMENT;
   if (!cloud->on_device || !out->on_device) return SRCU_ERR_INVALID_ARGUMENT;
+  if (cloud->stride > 1) return SRCU_ERR_INVALID_ARGUMENT;  // packed columns only
   if (params->leaf_size <= 0.0f) return SRCU_ERR_INVALID_ARGUMENT;  // voxel.rs:260-264
   if ((params->mode != SRCU_VOXEL_CENTROID && params->mode != SRCU_VOXEL_APPROXIMATE_FIRST) ||
       (params->attribute_policy != SRCU_ATTRIBUTE_AVERAGE &&

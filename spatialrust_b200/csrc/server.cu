@@ -475,7 +475,7 @@ srcu_status srcu_server_submit(srcu_server *sv, uint64_t req_id, const srcu_clou
                                const srcu_voxel_params *vp, const srcu_normal_params *np) {
   const Clock::time_point t0 = Clock::now();
   if (!sv || !cloud || !vp || !np) return SRCU_ERR_INVALID_ARGUMENT;
-  if (cloud->on_device || cloud->n_attrs > 1) return SRCU_ERR_INVALID_ARGUMENT;
+  if (cloud->on_device || cloud->n_attrs > 1 || cloud->stride > 64) return SRCU_ERR_INVALID_ARGUMENT;
   if (cloud->n > sv->cfg.bulk_max_points) return SRCU_ERR_INVALID_ARGUMENT;
   if (cloud->n && (!cloud->x || !cloud->y || !cloud->z)) return SRCU_ERR_MISSING_FIELD;
   if (cloud->n_attrs == 1 && cloud->n && (!cloud->attrs || !cloud->attrs[0]))
@@ -517,9 +517,13 @@ srcu_status srcu_server_submit(srcu_server *sv, uint64_t req_id, const srcu_clou
     float *dst = reinterpret_cast<float *>(sv->arena.base + r->in_off);
     const float *src[NCOL_IN] = {cloud->x, cloud->y, cloud->z,
                                  r->has_attr ? cloud->attrs[0] : nullptr};
+    const size_t stride = cloud->stride > 1 ? cloud->stride : 1;
     for (int c = 0; c < NCOL_IN; ++c) {
-      if (src[c]) std::memcpy(dst + size_t(c) * r->n, src[c], r->n * sizeof(float));
-      else std::memset(dst + size_t(c) * r->n, 0, r->n * sizeof(float));
+      float *d = dst + size_t(c) * r->n;
+      if (!src[c]) std::memset(d, 0, r->n * sizeof(float));
+      else if (stride == 1) std::memcpy(d, src[c], r->n * sizeof(float));
+      else  // interleaved records: gather this field
+        for (uint64_t i = 0; i < r->n; ++i) d[i] = src[c][i * stride];
     }
   }
   {

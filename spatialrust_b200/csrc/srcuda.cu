@@ -55,6 +55,7 @@ struct srcu_ctx {
   // normals outputs
   DevBuf nout[4], ncounts;
   DevBuf parent;  // union-find parents (Euclidean clustering)
+  DevBuf stage_block;  // host interleaved records, copied once before deinterleaving
   uint32_t last_attrs = 0;  // attribute count of the last enqueued chain
   const float *frame_attr_ptrs[MAX_COLS] = {};
   // batch arrays (clouds of the last chain) and pinned staging for their parameters
@@ -204,8 +205,15 @@ srcu_status check_cloud(srcu_ctx *ctx, const srcu_cloud *cloud) {
   for (uint32_t a = 0; a < cloud->n_attrs; ++a)
     if (cloud->n > 0 && (!cloud->attrs || !cloud->attrs[a]))
       return fail(ctx, SRCU_ERR_MISSING_FIELD, "attribute column %u is NULL", a);
+  if (cloud->stride > 64)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "stride %u exceeds 64 f32 elements", cloud->stride);
   return SRCU_OK;
 }
+
+bool strided(const srcu_cloud *cloud) { return cloud->stride > 1; }
+
+// Host input, or interleaved records: the columns are staged in ctx->in[].
+bool needs_staging(const srcu_cloud *cloud) { return !cloud->on_device || strided(cloud); }
 
 // Buffers for a chain over n points with `cols` columns.
 srcu_status reserve(srcu_ctx *ctx, uint64_t n, uint32_t cols, bool host_input, bool voxel,
@@ -252,6 +260,46 @@ srcu_status stage_input(srcu_ctx *ctx, const srcu_cloud *cloud, const float **co
   const uint32_t nc = 3 + cloud->n_attrs;
   const float *src[MAX_COLS] = {cloud->x, cloud->y, cloud->z};
   for (uint32_t a = 0; a < cloud->n_attrs; ++a) src[3 + a] = cloud->attrs[a];
+  if (strided(cloud)) {
+    // Interleaved records: deinterleave into the staged columns on the device
+    // (from a copy of the record block when it lives in host memory).
+    Interleaved iv{};
+    iv.nc = nc;
+    iv.stride = cloud->stride;
+    if (cloud->on_device) {
+      for (uint32_t c = 0; c < nc; ++c) iv.src[c] = src[c];
+    } else if (cloud->n) {
+      uintptr_t base = reinterpret_cast<uintptr_t>(src[0]), top = base;
+      for (uint32_t c = 1; c < nc; ++c) {
+        base = std::min(base, reinterpret_cast<uintptr_t>(src[c]));
+        top = std::max(top, reinterpret_cast<uintptr_t>(src[c]));
+      }
+      for (uint32_t c = 0; c < nc; ++c) {
+        const uintptr_t off = reinterpret_cast<uintptr_t>(src[c]) - base;
+        if (off % 4 != 0 || off / 4 >= cloud->stride)
+          return fail(ctx, SRCU_ERR_INVALID_ARGUMENT,
+                      "interleaved host columns must be fields of one record array");
+      }
+      const size_t floats = size_t(cloud->n - 1) * cloud->stride + (top - base) / 4 + 1;
+      ST_TRY(ensure(ctx, ctx->stage_block, floats * 4));
+      CU_TRY(cudaMemcpyAsync(ctx->stage_block.p, reinterpret_cast<const void *>(base), floats * 4,
+                             cudaMemcpyHostToDevice, ctx->stream));
+      for (uint32_t c = 0; c < nc; ++c)
+        iv.src[c] = ptr<const float>(ctx->stage_block) +
+                    (reinterpret_cast<uintptr_t>(src[c]) - base) / 4;
+    }
+    for (uint32_t c = 0; c < nc; ++c) {
+      iv.dst[c] = ptr<float>(ctx->in[c]);
+      cols[c] = ptr<const float>(ctx->in[c]);
+    }
+    if (cloud->n) {
+      const uint32_t grid = std::max<uint32_t>(
+          1, std::min<uint32_t>(ceil_div(cloud->n, 256), uint32_t(ctx->num_sms) * 8));
+      k_deinterleave<<<grid, 256, 0, ctx->stream>>>(iv, cloud->n);
+      CU_TRY(cudaGetLastError());
+    }
+    return SRCU_OK;
+  }
   for (uint32_t c = 0; c < nc; ++c) {
     if (cloud->on_device) {
       cols[c] = src[c];
@@ -687,7 +735,7 @@ void srcu_destroy(srcu_ctx *ctx) {
   DevBuf *all[] = {&ctx->in_aos, &ctx->vaos, &ctx->keys[0], &ctx->keys[1], &ctx->vals[0], &ctx->vals[1], &ctx->lb_sort,
                    &ctx->lb_seg, &ctx->lb_cells, &ctx->vkeys, &ctx->vcounts, &ctx->vkeys3,
                    &ctx->pts, &ctx->pt_cell, &ctx->cell_key, &ctx->cell_start, &ctx->table, &ctx->ranges,
-                   &ctx->ncounts, &ctx->parent};
+                   &ctx->ncounts, &ctx->parent, &ctx->stage_block};
   for (DevBuf *b : all) release(ctx, *b);
   for (auto &b : ctx->in) release(ctx, b);
   for (auto &b : ctx->vout) release(ctx, b);
@@ -736,7 +784,7 @@ srcu_status srcu_voxel_centroid(srcu_ctx *ctx, const srcu_cloud *cloud,
   const uint64_t n = cloud->n;
   if (n == 0) return SRCU_OK;  // voxel.rs:257-259: empty input is returned unchanged
   const uint32_t nc = 3 + cloud->n_attrs;
-  ST_TRY(reserve(ctx, n, nc, !cloud->on_device, true, false));
+  ST_TRY(reserve(ctx, n, nc, needs_staging(cloud), true, false));
   ST_TRY(reserve_batch(ctx, 1));
   if (out && out->keys) ST_TRY(ensure(ctx, ctx->vkeys3, n * 24));
   const float *cols[MAX_COLS];
@@ -763,7 +811,7 @@ srcu_status srcu_radius_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
   CU_TRY(cudaSetDevice(ctx->device));
   const uint64_t n = cloud->n;
   if (n == 0) return SRCU_OK;  // normal.rs:106-108
-  ST_TRY(reserve(ctx, n, 3, !cloud->on_device, false, true));
+  ST_TRY(reserve(ctx, n, 3, needs_staging(cloud), false, true));
   ST_TRY(reserve_batch(ctx, 1));
   srcu_cloud xyz = *cloud;
   xyz.n_attrs = 0;
@@ -797,7 +845,7 @@ srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
   const uint64_t n = cloud->n;
   if (n == 0) return SRCU_OK;  // uniform_grid.rs:100-102
   if (!roots) return fail(ctx, SRCU_ERR_MISSING_FIELD, "roots is NULL");
-  ST_TRY(reserve(ctx, n, 3, !cloud->on_device, false, true));
+  ST_TRY(reserve(ctx, n, 3, needs_staging(cloud), false, true));
   ST_TRY(reserve_batch(ctx, 1));
   ST_TRY(ensure(ctx, ctx->parent, n * 4));
   srcu_cloud xyz = *cloud;
@@ -853,7 +901,7 @@ srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
   const uint64_t n = cloud->n;
   if (n == 0) return SRCU_OK;
   const uint32_t nc = 3 + cloud->n_attrs;
-  ST_TRY(reserve(ctx, n, nc, !cloud->on_device, true, true));
+  ST_TRY(reserve(ctx, n, nc, needs_staging(cloud), true, true));
   ST_TRY(reserve_batch(ctx, 1));
   if (vout && vout->keys) ST_TRY(ensure(ctx, ctx->vkeys3, n * 24));
   const float *cols[MAX_COLS];
@@ -906,7 +954,7 @@ srcu_status srcu_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
     return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "enqueue needs a device-resident cloud");
   const uint64_t n = cloud->n;
   const uint32_t nc = 3 + cloud->n_attrs;
-  ST_TRY(reserve(ctx, n, nc, false, true, true));
+  ST_TRY(reserve(ctx, n, nc, needs_staging(cloud), true, true));
   ST_TRY(reserve_batch(ctx, 1));
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, cloud, cols));
@@ -943,7 +991,7 @@ static srcu_status batch_enqueue(srcu_ctx *ctx, const srcu_cloud *points, const 
   }
   const uint64_t n = points->n;
   const uint32_t nc = 3 + points->n_attrs;
-  ST_TRY(reserve(ctx, n, nc, false, true, true));
+  ST_TRY(reserve(ctx, n, nc, needs_staging(points), true, true));
   ST_TRY(reserve_batch(ctx, count));
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, points, cols));

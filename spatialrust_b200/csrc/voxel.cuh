@@ -81,6 +81,19 @@ struct BoundsAcc {
 
 constexpr uint32_t BND_CHUNK = 16;  // points per lane of a warp span in the multi-cloud case
 
+// Interleaved input records (srcu_cloud.stride > 1) -> packed columns.
+struct Interleaved {
+  const float *src[MAX_COLS];
+  float *dst[MAX_COLS];
+  uint32_t nc, stride;
+};
+
+__global__ void k_deinterleave(Interleaved iv, uint64_t n) {
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * blockDim.x)
+    for (uint32_t c = 0; c < iv.nc; ++c) iv.dst[c][i] = iv.src[c][i * iv.stride];
+}
+
 // Per-cloud min/max over finite coordinates plus NaN / inf flags
 // (compute_bounds, voxel.rs:1067-1079, ignores NaN through f32::min/max).
 // The point count comes from *count_dev when non-null, else ctl->n_points.
