@@ -95,12 +95,14 @@ def cpu_crop(cloud, side=None):
             np.ascontiguousarray(cloud.z[m]), np.ascontiguousarray(cloud.intensity[m]))
 
 
-def cpu_step(crop):
+def cpu_step(crop, threads=0):
+    """One step of the reference CPU path; threads 0 = the reference's own
+    worker count for the sample (staging.rs:11-41)."""
     import oracle
     x, y, z, i = crop
     for leaf in LEAVES:
         v = oracle.voxel_centroid(x, y, z, [i], leaf=leaf)
-        oracle.radius_normals_ref(v.x, v.y, v.z, RADIUS, 3, VIEWPOINT, threads=0)
+        oracle.radius_normals_ref(v.x, v.y, v.z, RADIUS, 3, VIEWPOINT, threads=threads)
 
 
 def cpu_threads(n_centroids: int) -> int:
@@ -135,31 +137,49 @@ def cpu_baseline(cloud):
                         "the reference's CPU path (Rust is not buildable here)"))
 
 
+REFERENCE_BUDGET_S = 90.0  # timed CPU work of the reference arm
+
+
 def run_reference(args):
+    """The reference's CPU path (C restatement) on the box's host cores.  Each
+    step is a bounded sample of the workload: the full 2M-point step when K of
+    them fit in about REFERENCE_BUDGET_S, else the x, y < side tile of the same
+    cloud at full density, sized from one timed full step so that K steps take
+    about that long."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
     cloud = workload_cloud()
     import oracle
     oracle.build()
-    crop = cpu_crop(cloud, CROP_SIDE)
-    for _ in range(max(args.warmup, 1)):
-        cpu_step(crop)
+    full = cpu_crop(cloud, None)
+    t0 = time.perf_counter()
+    cpu_step(full)  # the first warm-up step, at full size, also sizes the sample
+    t_full = time.perf_counter() - t0
+    frac = min(1.0, REFERENCE_BUDGET_S / (max(args.steps, 1) * t_full))
+    side = None if frac >= 1.0 else 200.0 * float(np.sqrt(frac))
+    crop = cpu_crop(cloud, side)
+    # the sample runs with the worker count the reference uses on the whole workload
+    v = oracle.voxel_centroid(*full[:3], [full[3]], leaf=LEAVES[0])
+    threads = cpu_threads(len(v.x))
+    for _ in range(max(args.warmup - 1, 0)):
+        cpu_step(crop, threads)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        cpu_step(crop)
+        cpu_step(crop, threads)
     t = (time.perf_counter() - t0) / args.steps
-    v = oracle.voxel_centroid(*crop[:3], [crop[3]], leaf=LEAVES[0])
     value = len(crop[0]) / t / 1e6
     line = dict(
         impl="reference", metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus,
         steps=args.steps, warmup=args.warmup, ms_per_step=t * 1e3, higher_is_better=True,
         scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
         config=dict(workload=WORKLOAD, points=len(crop[0]), sample_of=N_POINTS),
-        cpu_baseline=dict(value=value, unit=UNIT, cores=cpu_threads(len(v.x)), kind="port",
-                          sample=(f"the full step on all {len(crop[0])} points each step; the "
-                                  "reference is Rust and cannot be built here, so its CPU path "
-                                  "runs as the C restatement in oracle/")),
+        cpu_baseline=dict(value=value, unit=UNIT, cores=threads, kind="port",
+                          sample=(f"each step: {len(crop[0])} of the {N_POINTS} points "
+                                  + ("(the whole cloud)" if side is None else
+                                     f"(the x, y < {side:.1f} m tile at full density)")
+                                  + "; the reference is Rust and cannot be built here, so its "
+                                  "CPU path runs as the C restatement in oracle/")),
         e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0),
     )
     print(json.dumps(line), flush=True)
@@ -578,8 +598,11 @@ def run_serving(args, device):
     scan mixture); each runs voxel 0.2 m -> radius normals 0.6 m.  Frames and
     chunks arrive as two independent Poisson streams (0.9 and 0.1 of the
     offered rate, i.e. one Poisson stream whose requests are chunks with
-    probability 0.1), each submitted by its own host thread; a third thread
-    polls results.  Latency = submit -> results in pinned host memory."""
+    probability 0.1).  Each stream's arrival clock runs in its own host thread,
+    which hands every arrival to a small pool of submitting threads (2 for
+    frames, 4 for chunks: a chunk's copy into the pinned arena takes ~10 ms);
+    another thread polls results.  Latency = submit -> results in pinned host
+    memory."""
     import threading
 
     from spatialrust_b200 import _native, synthetic
@@ -618,29 +641,40 @@ def run_serving(args, device):
         done = threading.Event()
         counts = {"frames": 0, "chunks": 0, "points": 0}
 
-        def stream_of(pool, share, key, seed):
+        from concurrent.futures import ThreadPoolExecutor
+        count_lock = threading.Lock()
+
+        def submit_counted(c, key):
+            submit(c)
+            with count_lock:
+                counts[key] += 1
+                counts["points"] += c.n
+
+        def stream_of(pool, share, key, seed, workers):
+            # Arrival times are kept by this thread; each arrival is handed to a
+            # worker, so one slow copy (a 4M-point chunk is 64 MB) does not
+            # delay the arrivals behind it.
             rng = np.random.default_rng(seed)
             t_next = time.perf_counter()
             end = t_next + args.serving_seconds
             k = 0
-            while True:
-                t_next += rng.exponential(1.0 / (rate * share))
-                if t_next >= end:
-                    break
+            with ThreadPoolExecutor(max_workers=workers) as ex:
                 while True:
-                    dt = t_next - time.perf_counter()
-                    if dt <= 0:
+                    t_next += rng.exponential(1.0 / (rate * share))
+                    if t_next >= end:
                         break
-                    time.sleep(dt if dt > 0.002 else 0)
-                c = pool[k % len(pool)]
-                k += 1
-                submit(c)
-                counts[key] += 1
-                counts["points"] += c.n
+                    while True:
+                        dt = t_next - time.perf_counter()
+                        if dt <= 0:
+                            break
+                        time.sleep(dt if dt > 0.002 else 0)
+                    c = pool[k % len(pool)]
+                    k += 1
+                    ex.submit(submit_counted, c, key)
 
         t0 = time.perf_counter()
-        ths = [threading.Thread(target=stream_of, args=(frames, 0.9, "frames", int(rate))),
-               threading.Thread(target=stream_of, args=(chunks, 0.1, "chunks", int(rate) + 7))]
+        ths = [threading.Thread(target=stream_of, args=(frames, 0.9, "frames", int(rate), 2)),
+               threading.Thread(target=stream_of, args=(chunks, 0.1, "chunks", int(rate) + 7, 4))]
         for t in ths:
             t.start()
         poller_count = [0]
