@@ -428,6 +428,20 @@ __device__ __forceinline__ Eig3 eig_from_moments(const double (&S)[9], uint32_t 
   return smallest_eigenpair(cxx, cyy, czz, cxy, cxz, cyz);
 }
 
+// The same covariance (assembled in FP64), solved in FP32: the closed form
+// carries ~6e-8 of the trace in absolute error, so wherever the gap l1 - l0
+// is at least NM_REFINE_GAP of the trace the eigenvector is within ~1e-6 rad.
+// Smaller gaps go to the FP64 path.
+__device__ __forceinline__ Eig3 eig_from_moments_f32(const double (&S)[9], uint32_t n) {
+  const double inv = 1.0 / double(n);
+  const double mx = S[0] * inv, my = S[1] * inv, mz = S[2] * inv;
+  const double cxx = S[3] * inv - mx * mx, cyy = S[4] * inv - my * my;
+  const double czz = S[5] * inv - mz * mz, cxy = S[6] * inv - mx * my;
+  const double cxz = S[7] * inv - mx * mz, cyz = S[8] * inv - my * mz;
+  return smallest_eigenpair_t<float>(float(cxx), float(cyy), float(czz), float(cxy), float(cxz),
+                                     float(cyz));
+}
+
 // The same neighbour set (the f32 predicate), with every moment term formed
 // and summed in FP64 -- used for near-degenerate covariances only.
 __device__ __noinline__ void moments_fp64(const float4 *pts, const uint2 *rg, float4 qp, float r2,
@@ -576,11 +590,12 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
     const bool valid = prm.include_self ? (n_eff >= 3) : (cnt >= prm.min_neighbors && cnt > 0);
     float ox, oy, oz, oc;
     if (valid) {
-      Eig3 e = eig_from_moments(S, n_eff);
-      // The f32 moments carry ~1e-7 r^2 of rounding; when the gap to the
-      // second eigenvalue is under NM_REFINE_GAP of the trace that rounding
-      // can tilt the normal by more than 1e-5 rad, so this point's moments
-      // are recomputed with FP64 products (same neighbour set) and re-solved.
+      Eig3 e = eig_from_moments_f32(S, n_eff);
+      // The f32 moments carry ~1e-7 r^2 of rounding and the FP32 solve ~6e-8
+      // of the trace; when the gap to the second eigenvalue is under
+      // NM_REFINE_GAP of the trace that rounding can tilt the normal by more
+      // than 1e-5 rad, so this point's moments are recomputed with FP64
+      // products (same neighbour set) and solved in FP64.
       const double trace = e.l0 + e.l1 + e.l2;
       if (!(e.l1 - e.l0 >= NM_REFINE_GAP * trace)) {
         moments_fp64(pts, rg, qp, r2, S);
