@@ -486,6 +486,10 @@ __device__ __noinline__ void moments_fp64(const float4 *pts, const uint2 *rg, fl
 // differences): count, sum d, sum d d^T, accumulated in f32 for NM_FLUSH
 // candidates and then folded into FP64; C = S2/n - (S1/n)(S1/n)^T and its
 // eigensolve are FP64.
+// CountShell: the chain reports shell points (some cloud asked for it); the
+// check costs a few instructions per candidate, so chains that do not want
+// it run the variant without it.
+template <bool CountShell>
 __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const float4 *pts,
                                                            const uint32_t *pt_cell,
                                                            const uint2 *ranges,
@@ -544,7 +548,8 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
         F[7] = fmaf(dx, dz, F[7]);
         F[8] = fmaf(dy, dz, F[8]);
       }
-      if (prm.count_shell && d2 != 0.f && fabsf(__fsub_rn(d2, r2)) <= shell_tol) shell = 1;
+      if (CountShell && prm.count_shell && d2 != 0.f && fabsf(__fsub_rn(d2, r2)) <= shell_tol)
+        shell = 1;
     };
     auto flush = [&]() {
 #pragma unroll

@@ -63,6 +63,7 @@ struct srcu_ctx {
   uint32_t batch_cap = 0;
   uint32_t last_clouds = 1;
   int32_t agg_all = AGG_FAST;  // the chain's voxel aggregation when every cloud shares it, else -1
+  bool count_shell = true;     // some cloud of the chain reports shell points
   unsigned char *h_stage[2] = {nullptr, nullptr};
   size_t h_stage_bytes[2] = {0, 0};
   cudaEvent_t h_stage_ev[2] = {nullptr, nullptr};
@@ -491,8 +492,9 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
     case 12: launch_segments_nc<12>(ctx, in, grid, bt); break;
     default: return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "unsupported column count %u", nc);
   }
-  k_voxel_offsets<<<ceil_div(bt.clouds + 1, 128), 128, 0, ctx->stream>>>(
-      ctx->ctl, ptr<uint64_t>(ctx->vkeys), bt);
+  if (bt.clouds > 1)  // one cloud's range is [0, V), read from the control block
+    k_voxel_offsets<<<ceil_div(bt.clouds + 1, 128), 128, 0, ctx->stream>>>(
+        ctx->ctl, ptr<uint64_t>(ctx->vkeys), bt);
   CU_TRY(cudaGetLastError());
   return SRCU_OK;
 }
@@ -552,7 +554,8 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
   ST_TRY(enqueue_grid(ctx, x, y, z, aos, count_dev, n_max, bt, voxel_keys));
   const uint32_t grid_n = uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals);
   Launch l(ctx, SRCU_K_NORMALS);
-  k_normals<<<grid_n, NM_THREADS, 0, ctx->stream>>>(
+  auto kernel = ctx->count_shell ? k_normals<true> : k_normals<false>;
+  kernel<<<grid_n, NM_THREADS, 0, ctx->stream>>>(
       ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint2>(ctx->ranges),
       ptr<uint64_t>(ctx->cell_key), bt, count_dev, ptr<float>(ctx->nout[0]),
       ptr<float>(ctx->nout[1]), ptr<float>(ctx->nout[2]), ptr<float>(ctx->nout[3]),
@@ -569,7 +572,10 @@ void begin_chain(srcu_ctx *ctx, uint64_t n, const Batch &bt, int single,
   k_begin<<<1, 256, 0, ctx->stream>>>(ctx->ctl, n, bt, cloud_bits_for(bt.clouds), single,
                                       to_dev(vp), to_dev(np));
   ctx->last_clouds = bt.clouds;
-  if (single) ctx->agg_all = to_dev(vp).agg;
+  if (single) {
+    ctx->agg_all = to_dev(vp).agg;
+    ctx->count_shell = np && np->count_shell;
+  }
 }
 
 srcu_status read_control(srcu_ctx *ctx) {
@@ -713,7 +719,7 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
                                                 OS_THREADS, sizeof(OnesweepSmem));
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_c, k_sort<CellKeySrc>,
                                                 OS_THREADS, sizeof(OnesweepSmem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals, k_normals, NM_THREADS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals, k_normals<true>, NM_THREADS, 0);
   if (configure_segment_kernels() != cudaSuccess) return bail(SRCU_ERR_CUDA);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_seg, k_voxel_segments<4>, SEG_THREADS,
                                                 segment_smem_bytes(4));
@@ -1001,6 +1007,8 @@ static srcu_status batch_enqueue(srcu_ctx *ctx, const srcu_cloud *points, const 
   ctx->agg_all = to_dev(&vparams[0]).agg;
   for (uint32_t b = 1; b < count; ++b)
     if (to_dev(&vparams[b]).agg != ctx->agg_all) ctx->agg_all = -1;
+  ctx->count_shell = false;
+  for (uint32_t b = 0; b < count; ++b) ctx->count_shell |= nparams[b].count_shell != 0;
   if (n > 0) {
     ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
     ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
@@ -1087,9 +1095,14 @@ srcu_status srcu_batch_voxel_offsets(srcu_ctx *ctx, uint64_t *voxel_offsets) {
   if (!ctx || !voxel_offsets) return SRCU_ERR_INVALID_ARGUMENT;
   const uint32_t count = ctx->last_clouds;
   std::vector<uint32_t> tmp(count + 1);
-  CU_TRY(cudaMemcpyAsync(tmp.data(), ctx->b_voff.p, (count + 1) * 4, cudaMemcpyDeviceToHost,
-                         ctx->stream));
+  if (count > 1)
+    CU_TRY(cudaMemcpyAsync(tmp.data(), ctx->b_voff.p, (count + 1) * 4, cudaMemcpyDeviceToHost,
+                           ctx->stream));
   ST_TRY(read_control(ctx));
+  if (count <= 1) {
+    tmp[0] = 0;
+    tmp[count] = uint32_t(ctx->ctl_host->n_voxels);
+  }
   for (uint32_t b = 0; b <= count; ++b) voxel_offsets[b] = tmp[b];
   return SRCU_OK;
 }
