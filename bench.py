@@ -42,6 +42,10 @@ WORKLOAD = "georef_scan_2M_xyzi: voxel leaf 0.1 + leaf 0.5, each -> radius norma
 METRIC = "M points/s voxel+normals (2M georeferenced point_xyzi, leaf 0.1 & 0.5, r 0.5)"
 UNIT = "Mpoints/s"
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) per launch of the dominant kernel group on this
+# workload, mean over the leaf-0.1 and leaf-0.5 chains, from one ncu capture
+# (profiles/k_normals_georef2M_leaf0.1.md); ncu cannot run inside the bench.
+MEASURED_TRAFFIC = {"normals": (97.0e6 + 42.4e6) / 2}
 
 
 def parse():
@@ -386,7 +390,13 @@ def run_gpu(args):
     avg_launch_ms = dom_ms / max(dom_regions, 1)
     achieved = dom_bytes / (avg_launch_ms / 1e3) / 1e9 if dom_regions else 0.0
     roofline = dict(bound="hbm", kernel=dominant, achieved=achieved, peak=hbm, unit="GB/s",
-                    frac=achieved / hbm, traffic=None,
+                    frac=achieved / hbm, traffic=MEASURED_TRAFFIC.get(dominant),
+                    traffic_source=("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                                    "profiles/k_normals_georef2M_leaf0.1.md")
+                    if dominant in MEASURED_TRAFFIC else None,
+                    note=("the normals kernel is bound by FP32 issue and L1 latency on its "
+                          "candidate walk (ncu: 64% issue active, 3% of DRAM peak), not by HBM")
+                    if dominant == "normals" else None,
                     peak_source="MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
                     else "fallback 6650 GB/s",
                     algorithmic_bytes_per_launch=dom_bytes, avg_launch_ms=avg_launch_ms,
