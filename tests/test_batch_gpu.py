@@ -133,3 +133,35 @@ def test_chain_graph_replays_match_enqueue():
     assert np.array_equal(got1["nx"], ref1["nx"], equal_nan=True)
     g1.close()
     ctx.close()
+
+
+def test_thousand_tiny_clouds_equal_alone():
+    # the serving loop's shape: up to 1024 small requests in one chain, some
+    # empty or single points; every cloud must match its own chain
+    import torch
+    rng = np.random.default_rng(91)
+    sizes = rng.integers(0, 600, 1000)
+    sizes[::97] = 0
+    sizes[5::101] = 1
+    clouds = [synthetic.georef_scan(int(n), seed=500 + i, offset=rng.uniform(0, 1e5, 3))
+              if n else synthetic.uniform_cube(0, seed=1) for i, n in enumerate(sizes)]
+    leaves = rng.choice([0.1, 0.2, 0.5], len(clouds)).tolist()
+    radii = [4 * l for l in leaves]
+    ctx = _native.Context(0)
+    voff, out = run_batch(ctx, torch, clouds, leaves, radii)
+    assert voff[-1] == len(out["counts"])
+    alone = _native.Context(0)
+    for b in rng.choice(len(clouds), 60, replace=False):
+        c = clouds[b]
+        mine = slice_out(out, int(voff[b]), int(voff[b + 1]))
+        if c.n == 0:
+            assert voff[b] == voff[b + 1]
+            continue
+        ref = alone.voxel_normals(c.x, c.y, c.z, [c.intensity], leaf=leaves[b], radius=radii[b])
+        assert np.array_equal(mine["counts"], ref["counts"]), f"cloud {b}"
+        for g, r in zip(mine["columns"], ref["columns"]):
+            assert np.array_equal(g, r), f"cloud {b}"
+        for k in ("nx", "ny", "nz", "curvature", "neighbor_counts"):
+            assert np.array_equal(mine[k], ref[k], equal_nan=True), f"cloud {b}: {k}"
+    alone.close()
+    ctx.close()
