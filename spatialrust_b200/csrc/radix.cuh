@@ -1,8 +1,9 @@
 // radix.cuh -- onesweep LSD radix sort of keys with their point indices, as
 // one persistent cooperative kernel per sort.
 //
-// Phase 1 histograms every 8-bit digit of every key (shared-memory atomics,
-// which B200 executes at full rate even when lanes collide).  After a grid
+// Phase 1 computes every key once (kept for the first pass) and histograms
+// its 8-bit digits (shared-memory atomics, which B200 executes at full rate
+// even when lanes collide).  After a grid
 // barrier, each digit pass that is not trivial (some key differs in that
 // digit) ranks 4096-key tiles with a warp-level multi-split, resolves the
 // tile's global digit offsets by decoupled look-back over earlier tiles, and
@@ -148,9 +149,14 @@ __global__ void __launch_bounds__(OS_THREADS, 2) k_sort(Src src, Control *ctl, u
     (&sm.u.hist[0][0][0])[i] = 0;
   __syncthreads();
   {
+    // The keys are computed once, here, and kept in the ping-pong buffer that
+    // the first digit pass reads (keys[1]); the grid barrier below publishes
+    // them like any pass's output.
     uint32_t(*h)[RADIX_BINS] = sm.u.hist[warp & (HIST_COPIES - 1)];
+    uint64_t *kcache = buf.keys[1];
     for (uint32_t i = blockIdx.x * OS_THREADS + t; i < n; i += gridDim.x * OS_THREADS) {
       const uint64_t k = src.key(i);
+      kcache[i] = k;
       for (uint32_t d = 0; d < nd; ++d) atomicAdd(&h[d][uint32_t(k >> (RADIX_BITS * d)) & 0xffu], 1u);
     }
   }
@@ -161,6 +167,7 @@ __global__ void __launch_bounds__(OS_THREADS, 2) k_sort(Src src, Control *ctl, u
     for (int cp = 0; cp < HIST_COPIES; ++cp) c += (&sm.u.hist[cp][0][0])[i];
     if (c) atomicAdd(&hist[i], c);
   }
+  __threadfence();  // the cached keys, before the barrier releases the first pass
   grid_barrier(st, &ctl->status);
 
   // ---- which digits need a pass ----------------------------------------
@@ -222,8 +229,8 @@ __global__ void __launch_bounds__(OS_THREADS, 2) k_sort(Src src, Control *ctl, u
         k[i] = 0;
         v[i] = 0;
         if (idx < n) {
-          if (from_src) {
-            const uint64_t key = src.key(idx);
+          if (from_src) {  // the key stored by the histogram phase
+            const uint64_t key = kin[idx];
             k[i] = packed ? ((key << idx_bits) | idx) : key;
             v[i] = idx;
           } else {
