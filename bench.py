@@ -5,7 +5,8 @@ Workload (one step): the 2,000,000-point georeferenced scan-like point_xyzi
 cloud (60% ground, 30% box faces, 10% clutter; offset (450000, 3900000, 50) m,
 fed as f32(world - origin)), voxel-downsampled at leaf 0.1 m and at leaf 0.5 m,
 each followed by radius normals (r = 0.5 m, viewpoint origin + (0, 0, 100)) on
-the centroids -- the MvpPipeline chain.  value = input points per second
+the centroids -- the MvpPipeline chain.  The two leaf chains are independent and
+run on two streams, one context each (--serial-leaves: one stream).  value = input points per second
 through the whole step (2M points / step time), inputs resident in HBM, L2
 flushed (256 MB write) between timed steps.  e2e = the same through the C ABI
 with pinned host buffers (H2D of the inputs and D2H of all results inside the
@@ -55,6 +56,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serial-leaves", action="store_true",
+                    help="run the two leaf chains of a step on one stream, one after the other")
     ap.add_argument("--profile-all", action="store_true",
                     help="print the per-kernel-group timing table to stderr")
     ap.add_argument("--no-batched", action="store_true",
@@ -308,16 +311,32 @@ def run_gpu(args):
     torch.cuda.set_stream(stream)
     # one context per leaf so both chains' results stay resident
     ctxs = [_native.Context(local) for _ in LEAVES]
-    for c in ctxs:
-        c.set_stream(stream.cuda_stream)
+    # The two leaf chains are independent: each context gets its own stream,
+    # forked from and joined back to the timing stream every step, so their
+    # latency-bound phases overlap (--serial-leaves runs both on one stream).
+    leaf_streams = [stream] * len(LEAVES) if args.serial_leaves else \
+        [torch.cuda.Stream(dev) for _ in LEAVES]
+    for c, s in zip(ctxs, leaf_streams):
+        c.set_stream(s.cuda_stream)
     cols = [torch.from_numpy(a).to(dev) for a in (cloud.x, cloud.y, cloud.z, cloud.intensity)]
     keep = _native._Keep()
     dcloud = _native.make_cloud(cols[0], cols[1], cols[2], [cols[3]], keep)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
+    fork = torch.cuda.Event()
+    joins = [torch.cuda.Event() for _ in LEAVES]
+
     def step():
+        if not args.serial_leaves:
+            fork.record(stream)
+            for s in leaf_streams:
+                s.wait_event(fork)
         for c, leaf in zip(ctxs, LEAVES):
             c.voxel_normals_enqueue(dcloud, leaf, None, RADIUS, 3, VIEWPOINT, count_shell=False)
+        if not args.serial_leaves:
+            for s, e in zip(leaf_streams, joins):
+                e.record(s)
+                stream.wait_event(e)
 
     # warm-up (also sizes every buffer)
     for _ in range(max(args.warmup, 3)):
@@ -330,16 +349,23 @@ def run_gpu(args):
         nstats.append(c.frame_check()[1])
         infos.append(c.chain_info())
 
-    # untimed profile pass: which kernel group dominates
+    # untimed profile pass: which kernel group dominates, with the two chains
+    # run one after the other so every group's time is its own
     for c in ctxs:
         c.profile_read(reset=True)
         c.profile_enable(_native.KERNEL_IDS)
+        c.set_stream(stream.cuda_stream)
     for _ in range(3):
         flush.zero_()
-        step()
+        for c, leaf in zip(ctxs, LEAVES):
+            c.voxel_normals_enqueue(dcloud, leaf, None, RADIUS, 3, VIEWPOINT, count_shell=False)
     torch.cuda.synchronize()
     prof = [c.profile_read(reset=True) for c in ctxs]
+    for c, s in zip(ctxs, leaf_streams):
+        c.set_stream(s.cuda_stream)
     group_ms = {g: sum(p[g]["total_ms"] for p in prof) for g in _native.KERNEL_IDS}
+    iso_group = {g: (sum(p[g]["total_ms"] for p in prof),
+                     sum(p[g]["timed_regions"] for p in prof)) for g in _native.KERNEL_IDS}
     dominant = max(group_ms, key=group_ms.get)
     if args.profile_all and rank == 0:
         tot = sum(group_ms.values())
@@ -389,6 +415,9 @@ def run_gpu(args):
     hbm = peaks.get("hbm_gbs", 6650.0)
     avg_launch_ms = dom_ms / max(dom_regions, 1)
     achieved = dom_bytes / (avg_launch_ms / 1e3) / 1e9 if dom_regions else 0.0
+    iso_ms, iso_regions = iso_group[dominant]
+    iso_launch_ms = iso_ms / max(iso_regions, 1)
+    iso_achieved = dom_bytes / (iso_launch_ms / 1e3) / 1e9 if iso_regions else 0.0
     roofline = dict(bound="hbm", kernel=dominant, achieved=achieved, peak=hbm, unit="GB/s",
                     frac=achieved / hbm, traffic=MEASURED_TRAFFIC.get(dominant),
                     traffic_source=("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
@@ -400,6 +429,11 @@ def run_gpu(args):
                     peak_source="MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
                     else "fallback 6650 GB/s",
                     algorithmic_bytes_per_launch=dom_bytes, avg_launch_ms=avg_launch_ms,
+                    timing=("CUDA events around each launch of the group in the timed region, "
+                            "where the two leaf chains share the GPU" if not args.serial_leaves
+                            else "CUDA events around each launch of the group in the timed region"),
+                    isolated_avg_launch_ms=iso_launch_ms, isolated_achieved=iso_achieved,
+                    isolated_frac=iso_achieved / hbm,
                     step_share=group_ms[dominant] / max(sum(group_ms.values()), 1e-9))
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
@@ -411,7 +445,9 @@ def run_gpu(args):
                     normals=[{k: st[k] for k in ("valid_count", "invalid_count", "fp64_eigensolves")}
                              for st in nstats],
                     l2="flushed by a 256 MB write before every timed step (outside the events)",
-                    parallelism=f"replicas x{world}"),
+                    parallelism=f"replicas x{world}",
+                    leaf_chains=("one stream, one after the other" if args.serial_leaves else
+                                 "two streams (one context each), forked and joined every step")),
         e2e=e2e, roofline=roofline, clocks=clock, gpu_launches=int(launches),
     )
     if not args.no_batched:
@@ -718,6 +754,7 @@ def run_e2e(ctx, cloud, args, torch, dev, stream):
     """Synchronous srcu_voxel_normals calls with pinned host inputs and outputs."""
     from spatialrust_b200 import _native
     lib = _native.load()
+    ctx.set_stream(stream.cuda_stream)  # the timing stream
     n = cloud.n
     pin = [torch.from_numpy(a).pin_memory() for a in (cloud.x, cloud.y, cloud.z, cloud.intensity)]
     keep = _native._Keep()
