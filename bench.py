@@ -406,7 +406,7 @@ def run_gpu(args):
     value = job_mpts(world, N_POINTS, ms_per_step)
 
     # end to end through the C ABI with pinned host buffers
-    e2e = run_e2e(ctxs[0], cloud, args, torch, dev, stream)
+    e2e = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream)
 
     peaks = {}
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -750,11 +750,21 @@ def run_serving(args, device):
     return out
 
 
-def run_e2e(ctx, cloud, args, torch, dev, stream):
-    """Synchronous srcu_voxel_normals calls with pinned host inputs and outputs."""
+def run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream):
+    """Synchronous srcu_voxel_normals calls with pinned host inputs and outputs,
+    one call per leaf.  Unless --serial-leaves, the two calls of a step are
+    made from two host threads on their own contexts and streams, so one
+    call's transfers overlap the other's kernels.  Device time: every leaf
+    stream waits on the start event, and the timing stream joins them all
+    before the end event."""
+    import threading
+
     from spatialrust_b200 import _native
     lib = _native.load()
-    ctx.set_stream(stream.cuda_stream)  # the timing stream
+    serial = args.serial_leaves
+    streams = [stream] * len(LEAVES) if serial else leaf_streams
+    for c, s in zip(ctxs, streams):
+        c.set_stream(s.cuda_stream)
     n = cloud.n
     pin = [torch.from_numpy(a).pin_memory() for a in (cloud.x, cloud.y, cloud.z, cloud.intensity)]
     keep = _native._Keep()
@@ -775,19 +785,34 @@ def run_e2e(ctx, cloud, args, torch, dev, stream):
     params = [(_native._voxel_params(leaf, None),
                _native._normal_params(RADIUS, 3, VIEWPOINT, False, count_shell=False))
               for leaf in LEAVES]
-    nv = ctypes.c_uint64(0)
-    stats = _native.SrcuNormalStats()
+    nvs = [ctypes.c_uint64(0) for _ in LEAVES]
+    stats = [_native.SrcuNormalStats() for _ in LEAVES]
     voxels = [0] * len(LEAVES)
+    errors = []
+
+    def call(k):
+        vp, np_ = params[k]
+        st = lib.srcu_voxel_normals(ctxs[k].handle, ctypes.byref(hcloud), ctypes.byref(vp),
+                                    ctypes.byref(np_), ctypes.byref(outs[k][2]),
+                                    ctypes.byref(outs[k][3]), ctypes.byref(nvs[k]),
+                                    ctypes.byref(stats[k]))
+        if st != 0:
+            errors.append((k, st))
+        voxels[k] = int(nvs[k].value)
 
     def step():
-        for k, (vp, np_) in enumerate(params):
-            st = lib.srcu_voxel_normals(ctx.handle, ctypes.byref(hcloud), ctypes.byref(vp),
-                                        ctypes.byref(np_), ctypes.byref(outs[k][2]),
-                                        ctypes.byref(outs[k][3]), ctypes.byref(nv),
-                                        ctypes.byref(stats))
-            if st != 0:
-                ctx._check(st)
-            voxels[k] = int(nv.value)
+        if serial:
+            for k in range(len(LEAVES)):
+                call(k)
+        else:
+            ths = [threading.Thread(target=call, args=(k,)) for k in range(len(LEAVES))]
+            for t in ths:
+                t.start()
+            for t in ths:
+                t.join()
+        if errors:
+            k, st = errors[0]
+            ctxs[k]._check(st)
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -795,8 +820,16 @@ def run_e2e(ctx, cloud, args, torch, dev, stream):
     steps = max(args.steps // 2, 3)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
+    for s in set(streams):
+        if s is not stream:
+            s.wait_event(start)
     for _ in range(steps):
         step()
+    for s in set(streams):
+        if s is not stream:
+            done = torch.cuda.Event()
+            done.record(s)
+            stream.wait_event(done)
     end.record(stream)
     torch.cuda.synchronize()
     ms = start.elapsed_time(end) / steps
@@ -804,7 +837,8 @@ def run_e2e(ctx, cloud, args, torch, dev, stream):
     d2h = sum(v * (16 + 16) for v in voxels)
     return dict(value=N_POINTS / (ms / 1e3) / 1e6, unit=UNIT, ms_per_step=ms,
                 h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
-                api="srcu_voxel_normals (include/srcuda.h), pinned host buffers, one call per leaf")
+                api=("srcu_voxel_normals (include/srcuda.h), pinned host buffers, one call per "
+                     "leaf" + ("" if serial else ", the two calls from two host threads")))
 
 
 def main():
