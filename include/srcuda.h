@@ -207,6 +207,22 @@ srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
 srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
                                          float cluster_tolerance, uint32_t *roots);
 
+/* ---- GICP plane covariances on the same grid ------------------------------ */
+
+/* Replaces spatialrust_gpu::estimate_plane_covariances_grid_gpu
+ * (crates/spatialrust-gpu/src/kernels/covariances_grid.rs:216-364), which
+ * GicpRegistration::point_covariances calls when covariance_radius is set
+ * (crates/spatialrust-registration/src/gicp.rs:89-101, 237-256).  For every
+ * point: the covariance of the points within radius of it (itself included,
+ * f32 predicate), its eigenvalues replaced by (epsilon, 1, 1) -- the
+ * plane-to-plane model -- as 6 floats [c00, c11, c22, c01, c02, c12]
+ * (GpuCovariance) at cov[6 i .. 6 i + 5]; fewer than 3 points in the
+ * neighbourhood give (epsilon, epsilon, epsilon, 0, 0, 0).  cov: 6 n floats,
+ * host or device memory as cloud->on_device.  radius must be > 0 and finite.
+ * stats (nullable) counts the valid and the fallback points.  Synchronous. */
+srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float radius,
+                                   float epsilon, float *cov, srcu_normal_stats *stats);
+
 /* ---- many clouds in one chain ---------------------------------------------- */
 
 /* Enqueues voxel -> normals for `count` clouds in one chain: the clouds'

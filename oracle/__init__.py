@@ -62,6 +62,9 @@ def _load():
                                                ctypes.c_uint32, ctypes.c_int, P, ctypes.c_double,
                                                ctypes.c_int, P, P, P, P, P, P, P]
     lib.oracle_radius_normals_fp64.restype = ctypes.c_int
+    lib.oracle_plane_covariances.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float,
+                                             ctypes.c_double, ctypes.c_int, P, P, P]
+    lib.oracle_plane_covariances.restype = ctypes.c_int
     lib.oracle_brute_radius_counts.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float, P]
     lib.oracle_brute_radius_counts.restype = None
     lib.oracle_compute_bounds.argtypes = [P, P, P, ctypes.c_size_t, P, P]
@@ -234,6 +237,32 @@ def radius_normals_fp64(x, y, z, radius, min_neighbors=3, viewpoint=None, shell_
     nx, ny, nz, curv, gap = [o[:n] for o in outs]
     valid = int(np.count_nonzero(~np.isnan(nx)))
     return NormalResult(nx, ny, nz, curv, counts[:n], valid, n - valid, gap, shell[:n].astype(bool))
+
+
+@dataclass
+class PlaneCovResult:
+    cov: np.ndarray     # (n, 6) float64: c00, c11, c22, c01, c02, c12
+    gap: np.ndarray     # (l1 - l0) / l2 of the neighbourhood covariance (0 when invalid)
+    counts: np.ndarray  # points within radius, the query included
+
+
+def plane_covariances(x, y, z, radius, epsilon, threads=0) -> PlaneCovResult:
+    """GICP plane-regularised covariances on radius neighbourhoods
+    (covariances_grid.rs:87-206), FP64 covariance and Jacobi."""
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    n = x.shape[0]
+    cov = np.empty((max(n, 1), 6), np.float64)
+    gap = np.zeros(max(n, 1), np.float64)
+    counts = np.zeros(max(n, 1), np.uint32)
+    rc = lib.oracle_plane_covariances(_ptr(x), _ptr(y), _ptr(z), n, ctypes.c_float(radius),
+                                      ctypes.c_double(epsilon), threads, _ptr(cov), _ptr(gap),
+                                      _ptr(counts))
+    if rc == -1:
+        raise OracleError("grid radius must be positive")
+    if rc != 0:
+        raise OracleError(f"oracle_plane_covariances failed: {rc}")
+    return PlaneCovResult(cov[:n], gap[:n], counts[:n])
 
 
 def brute_radius_counts(x, y, z, radius) -> np.ndarray:

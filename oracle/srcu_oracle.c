@@ -1283,6 +1283,131 @@ done:
   return rc;
 }
 
+/* ------------------------------------------------------------------------ */
+/* GICP plane covariances on the radius grid                                */
+/* (crates/spatialrust-gpu/src/kernels/covariances_grid.rs:87-206)          */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  const kd_tree *tree;
+  const float *x, *y, *z;
+  size_t start, end;
+  float radius;
+  double eps;
+  double *cov, *gap;
+  uint32_t *counts;
+} cov_job;
+
+/*
+ * Per point: every point within radius (the f32 predicate, the query itself
+ * included, covariances_grid.rs:100-121); fewer than 3 -> (eps, eps, eps, 0,
+ * 0, 0) (:127-131); else the FP64 two-pass covariance, its eigenvectors by
+ * FP64 cyclic-max Jacobi run to convergence, and sum_col lambda v v^T with
+ * lambda = eps for the smallest eigenvalue and 1 for the others
+ * (:165-202, the same rebuild as gicp.rs:276-291).  Output order
+ * [c00, c11, c22, c01, c02, c12].  gap = (l1 - l0) / max(l2, tiny) flags
+ * neighbourhoods whose plane is ill-defined.
+ */
+static void *cov_worker(void *arg) {
+  cov_job *j = (cov_job *)arg;
+  u32_vec found = {0};
+  const float r2 = j->radius * j->radius;
+  for (size_t i = j->start; i < j->end; ++i) {
+    found.len = 0;
+    if (j->tree->root != KD_INVALID)
+      kd_radius(j->tree, j->tree->root, j->x[i], j->y[i], j->z[i], r2, &found);
+    double *o = j->cov + 6 * i;
+    j->counts[i] = (uint32_t)found.len;
+    j->gap[i] = 0.0;
+    if (found.len < 3) {
+      o[0] = o[1] = o[2] = j->eps;
+      o[3] = o[4] = o[5] = 0.0;
+      continue;
+    }
+    double mx = 0, my = 0, mz = 0;
+    for (size_t k = 0; k < found.len; ++k) {
+      uint32_t p = found.idx[k];
+      mx += j->x[p];
+      my += j->y[p];
+      mz += j->z[p];
+    }
+    mx /= (double)found.len;
+    my /= (double)found.len;
+    mz /= (double)found.len;
+    double c[3][3] = {{0}};
+    for (size_t k = 0; k < found.len; ++k) {
+      uint32_t p = found.idx[k];
+      double dx = j->x[p] - mx, dy = j->y[p] - my, dz = j->z[p] - mz;
+      c[0][0] += dx * dx;
+      c[1][1] += dy * dy;
+      c[2][2] += dz * dz;
+      c[0][1] += dx * dy;
+      c[0][2] += dx * dz;
+      c[1][2] += dy * dz;
+    }
+    c[1][0] = c[0][1];
+    c[2][0] = c[0][2];
+    c[2][1] = c[1][2];
+    double vals[3], vecs[3][3];
+    rs_symmetric_eigen3(c, vals, vecs, 200, 1e-300);
+    double reg[6] = {0, 0, 0, 0, 0, 0};
+    for (int col = 0; col < 3; ++col) {
+      const double lam = col == 0 ? j->eps : 1.0;
+      const double ax = vecs[0][col], ay = vecs[1][col], az = vecs[2][col];
+      reg[0] += lam * ax * ax;
+      reg[1] += lam * ay * ay;
+      reg[2] += lam * az * az;
+      reg[3] += lam * ax * ay;
+      reg[4] += lam * ax * az;
+      reg[5] += lam * ay * az;
+    }
+    memcpy(o, reg, sizeof(reg));
+    double top = fabs(vals[2]) > 1e-300 ? fabs(vals[2]) : 1e-300;
+    j->gap[i] = (vals[1] - vals[0]) / top;
+  }
+  free(found.idx);
+  return NULL;
+}
+
+int oracle_plane_covariances(const float *x, const float *y, const float *z, size_t n,
+                             float radius, double eps, int threads, double *cov, double *gap,
+                             uint32_t *counts) {
+  if (n == 0) return OR_OK;
+  if (!(radius > 0.0f)) return OR_ERR_INVALID; /* covariances_grid.rs:231-233 */
+  kd_tree tree;
+  if (kd_build(&tree, x, y, z, n) != OR_OK) return OR_ERR_NOMEM;
+  size_t avail = threads > 0 ? (size_t)threads : (size_t)sysconf(_SC_NPROCESSORS_ONLN);
+  size_t workers = n < 4096 ? 1 : (avail < n / 1024 ? avail : (n / 1024 ? n / 1024 : 1));
+  size_t chunk = (n + workers - 1) / workers;
+  size_t njobs = (n + chunk - 1) / chunk;
+  cov_job *jobs = (cov_job *)calloc(njobs, sizeof(cov_job));
+  pthread_t *tids = (pthread_t *)calloc(njobs, sizeof(pthread_t));
+  for (size_t w = 0; w < njobs; ++w) {
+    cov_job *j = &jobs[w];
+    j->tree = &tree;
+    j->x = x;
+    j->y = y;
+    j->z = z;
+    j->start = w * chunk;
+    j->end = j->start + chunk < n ? j->start + chunk : n;
+    j->radius = radius;
+    j->eps = eps;
+    j->cov = cov;
+    j->gap = gap;
+    j->counts = counts;
+  }
+  if (njobs == 1) {
+    cov_worker(&jobs[0]);
+  } else {
+    for (size_t w = 0; w < njobs; ++w) pthread_create(&tids[w], NULL, cov_worker, &jobs[w]);
+    for (size_t w = 0; w < njobs; ++w) pthread_join(tids[w], NULL);
+  }
+  free(jobs);
+  free(tids);
+  kd_free(&tree);
+  return OR_OK;
+}
+
 /* Exposes the f32 closed-form smallest eigenpair for unit tests. */
 void oracle_smallest_eigenpair_f32(const float c[6], float normal[3], float *curv) {
   rs_smallest_eigenpair(c[0], c[1], c[2], c[3], c[4], c[5], normal, curv);

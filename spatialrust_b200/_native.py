@@ -209,6 +209,8 @@ SIGNATURES = {
                           ctypes.c_int),
     "srcu_euclidean_cluster_roots": ([_P, ctypes.POINTER(SrcuCloud), ctypes.c_float,
                                       ctypes.c_void_p], ctypes.c_int),
+    "srcu_plane_covariances": ([_P, ctypes.POINTER(SrcuCloud), ctypes.c_float, ctypes.c_float,
+                                ctypes.c_void_p, ctypes.POINTER(SrcuNormalStats)], ctypes.c_int),
     "srcu_server_create": ([ctypes.POINTER(SrcuServerConfig), ctypes.POINTER(ctypes.c_void_p)],
                            ctypes.c_int),
     "srcu_server_destroy": ([_P], None),
@@ -460,6 +462,26 @@ class Context:
         self._check(self._lib.srcu_euclidean_cluster_roots(self._h, ctypes.byref(cloud),
                                                            ctypes.c_float(cluster_tolerance), addr))
         return roots[:n]
+
+    def plane_covariances(self, x, y, z, radius: float, epsilon: float, with_stats: bool = False):
+        """(n, 6) plane-regularised covariances [c00, c11, c22, c01, c02, c12]
+        (numpy in and out, or CUDA tensors in and a CUDA tensor out)."""
+        keep = _Keep()
+        cloud = make_cloud(x, y, z, (), keep)
+        n = int(cloud.n)
+        if cloud.on_device:
+            import torch
+            cov = torch.empty((max(n, 1), 6), dtype=torch.float32,
+                              device=torch.device("cuda", self.device))
+            addr = cov.data_ptr()
+        else:
+            cov = np.empty((max(n, 1), 6), np.float32)
+            addr = cov.ctypes.data
+        stats = SrcuNormalStats()
+        self._check(self._lib.srcu_plane_covariances(self._h, ctypes.byref(cloud),
+                                                     ctypes.c_float(radius), ctypes.c_float(epsilon),
+                                                     addr, ctypes.byref(stats)))
+        return (cov[:n], _stats(stats)) if with_stats else cov[:n]
 
     def voxel_normals(self, x, y, z, attrs=(), leaf: float = 1.0, origin=None, radius: float = 0.5,
                       min_neighbors: int = 3, viewpoint=None, include_self: bool = False,

@@ -489,14 +489,23 @@ __device__ __noinline__ void moments_fp64(const float4 *pts, const uint2 *rg, fl
 // CountShell: the chain reports shell points (some cloud asked for it); the
 // check costs a few instructions per candidate, so chains that do not want
 // it run the variant without it.
-template <bool CountShell>
+// PlaneCov: instead of normal and curvature, write the GICP plane-regularised
+// covariance of each point (crates/spatialrust-gpu/src/kernels/
+// covariances_grid.rs:87-206): the neighbourhood covariance with its
+// eigenvalues replaced by (eps, 1, 1).  With the orthonormal eigenbasis
+// (n, a, b) that is eps n n^T + a a^T + b b^T = I + (eps - 1) n n^T, so only
+// the smallest eigenvector is needed.  Six floats per point in cov
+// ([c00, c11, c22, c01, c02, c12], the GpuCovariance layout); fewer than 3
+// points in the (self-inclusive) neighbourhood give (eps, eps, eps, 0, 0, 0).
+template <bool CountShell, bool PlaneCov = false>
 __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const float4 *pts,
                                                            const uint32_t *pt_cell,
                                                            const uint2 *ranges,
                                                            const uint64_t *cell_key, Batch bt,
                                                            const unsigned long long *count_dev,
                                                            float *nx, float *ny, float *nz,
-                                                           float *curv, uint32_t *counts) {
+                                                           float *curv, uint32_t *counts,
+                                                           float *cov, float cov_eps) {
   if (ld_relaxed_u32(&ctl->status)) return;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t n = uint32_t(count_dev ? *count_dev : ctl->n_points);
@@ -608,7 +617,7 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
         ++n_fp64;
       }
       double v0 = e.v[0], v1 = e.v[1], v2 = e.v[2];
-      if (prm.has_viewpoint) {
+      if (!PlaneCov && prm.has_viewpoint) {
         // orient_normal_towards_viewpoint, normal.rs:408-421
         const double wx = double(prm.vp[0]) - double(qp.x);
         const double wy = double(prm.vp[1]) - double(qp.y);
@@ -638,6 +647,28 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
     const uint32_t qidx = __float_as_uint(qp.w);
     if (qidx >= n) {  // cannot happen: records carry indices < n
       atomicOr(&ctl->status, ST_INTERNAL);
+      continue;
+    }
+    if constexpr (PlaneCov) {
+      float *o = cov + size_t(qidx) * 6;
+      if (valid) {
+        // (ox, oy, oz) is the unit normal; I + (eps - 1) n n^T
+        const float s = cov_eps - 1.0f;
+        o[0] = fmaf(s * ox, ox, 1.0f);
+        o[1] = fmaf(s * oy, oy, 1.0f);
+        o[2] = fmaf(s * oz, oz, 1.0f);
+        o[3] = s * ox * oy;
+        o[4] = s * ox * oz;
+        o[5] = s * oy * oz;
+      } else {
+        o[0] = cov_eps;
+        o[1] = cov_eps;
+        o[2] = cov_eps;
+        o[3] = 0.0f;
+        o[4] = 0.0f;
+        o[5] = 0.0f;
+      }
+      if (counts) counts[qidx] = n_eff;
       continue;
     }
     nx[qidx] = ox;

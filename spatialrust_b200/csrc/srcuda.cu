@@ -55,6 +55,7 @@ struct srcu_ctx {
   // normals outputs
   DevBuf nout[4], ncounts;
   DevBuf parent;  // union-find parents (Euclidean clustering)
+  DevBuf cov6;    // plane-regularised covariances, 6 floats per point
   DevBuf stage_block;  // host interleaved records, copied once before deinterleaving
   uint32_t last_attrs = 0;  // attribute count of the last enqueued chain
   const float *frame_attr_ptrs[MAX_COLS] = {};
@@ -559,7 +560,7 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
       ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint2>(ctx->ranges),
       ptr<uint64_t>(ctx->cell_key), bt, count_dev, ptr<float>(ctx->nout[0]),
       ptr<float>(ctx->nout[1]), ptr<float>(ctx->nout[2]), ptr<float>(ctx->nout[3]),
-      ptr<uint32_t>(ctx->ncounts));
+      ptr<uint32_t>(ctx->ncounts), nullptr, 0.0f);
   CU_TRY(cudaGetLastError());
   return SRCU_OK;
 }
@@ -741,7 +742,7 @@ void srcu_destroy(srcu_ctx *ctx) {
   DevBuf *all[] = {&ctx->in_aos, &ctx->vaos, &ctx->keys[0], &ctx->keys[1], &ctx->vals[0], &ctx->vals[1], &ctx->lb_sort,
                    &ctx->lb_seg, &ctx->lb_cells, &ctx->vkeys, &ctx->vcounts, &ctx->vkeys3,
                    &ctx->pts, &ctx->pt_cell, &ctx->cell_key, &ctx->cell_start, &ctx->table, &ctx->ranges,
-                   &ctx->ncounts, &ctx->parent, &ctx->stage_block};
+                   &ctx->ncounts, &ctx->parent, &ctx->cov6, &ctx->stage_block};
   for (DevBuf *b : all) release(ctx, *b);
   for (auto &b : ctx->in) release(ctx, b);
   for (auto &b : ctx->vout) release(ctx, b);
@@ -844,12 +845,12 @@ srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
                                          float cluster_tolerance, uint32_t *roots) {
   if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
   ST_TRY(check_cloud(ctx, cloud));
+  const uint64_t n = cloud->n;
+  if (n == 0) return SRCU_OK;  // uniform_grid.rs:100-102, before the tolerance check
   // uniform_grid.rs:103-105 (an infinite tolerance has no grid here)
   if (!(cluster_tolerance > 0.0f) || cluster_tolerance == INFINITY)
     return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "cluster_tolerance must be positive and finite");
   CU_TRY(cudaSetDevice(ctx->device));
-  const uint64_t n = cloud->n;
-  if (n == 0) return SRCU_OK;  // uniform_grid.rs:100-102
   if (!roots) return fail(ctx, SRCU_ERR_MISSING_FIELD, "roots is NULL");
   ST_TRY(reserve(ctx, n, 3, needs_staging(cloud), false, true));
   ST_TRY(reserve_batch(ctx, 1));
@@ -889,6 +890,62 @@ srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
   CU_TRY(cudaGetLastError());
   ST_TRY(read_control(ctx));
   if (!cloud->on_device) ST_TRY(copy_out(ctx, roots, dst, n * 4, 0));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  return SRCU_OK;
+}
+
+srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float radius,
+                                   float epsilon, float *cov, srcu_normal_stats *stats) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  if (stats) memset(stats, 0, sizeof(*stats));
+  ST_TRY(check_cloud(ctx, cloud));
+  const uint64_t n = cloud->n;
+  if (n == 0) return SRCU_OK;  // covariances_grid.rs:228-230, before the radius check
+  // covariances_grid.rs:231-233 (an infinite radius has no grid here)
+  if (!(radius > 0.0f) || radius == INFINITY)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "grid radius must be positive and finite");
+  CU_TRY(cudaSetDevice(ctx->device));
+  if (!cov) return fail(ctx, SRCU_ERR_MISSING_FIELD, "cov is NULL");
+  ST_TRY(reserve(ctx, n, 3, needs_staging(cloud), false, true));
+  ST_TRY(reserve_batch(ctx, 1));
+  float *dst = cov;
+  if (!cloud->on_device) {
+    ST_TRY(ensure(ctx, ctx->cov6, n * 24));
+    dst = ptr<float>(ctx->cov6);
+  }
+  srcu_cloud xyz = *cloud;
+  xyz.n_attrs = 0;
+  const float *cols[MAX_COLS];
+  ST_TRY(stage_input(ctx, &xyz, cols));
+  const Batch bt = make_batch(ctx, 1);
+  // The shader's neighbourhood includes the query (covariances_grid.rs:100-121)
+  // and needs 3 points (:127-131): the include_self rule of the normals.
+  srcu_normal_params np{};
+  np.radius = radius;
+  np.min_neighbors = 3;
+  np.include_self = 1;
+  begin_chain(ctx, n, bt, 1, nullptr, &np);
+  const uint32_t grid_b = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4),
+                                                                    uint32_t(ctx->num_sms) * 8));
+  {
+    Launch l(ctx, SRCU_K_BOUNDS);
+    k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(cols[0], cols[1], cols[2], ctx->ctl, nullptr,
+                                                       nullptr, ptr<float4>(ctx->in_aos), bt);
+  }
+  ST_TRY(enqueue_grid(ctx, cols[0], cols[1], cols[2], ptr<const float4>(ctx->in_aos), nullptr, n,
+                      bt, nullptr));
+  {
+    const uint32_t grid_n = uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals);
+    Launch l(ctx, SRCU_K_NORMALS);
+    k_normals<false, true><<<grid_n, NM_THREADS, 0, ctx->stream>>>(
+        ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint2>(ctx->ranges),
+        ptr<uint64_t>(ctx->cell_key), bt, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+        dst, epsilon);
+  }
+  CU_TRY(cudaGetLastError());
+  ST_TRY(read_control(ctx));
+  if (!cloud->on_device) ST_TRY(copy_out(ctx, cov, dst, n * 24, 0));
+  ST_TRY(fetch_normals(ctx, nullptr, n, stats));
   CU_TRY(cudaStreamSynchronize(ctx->stream));
   return SRCU_OK;
 }

@@ -187,6 +187,47 @@ def test_cluster_rejects_non_positive_tolerance():
         oracle.euclidean_roots(x, x, x, 0.0)
 
 
+def test_plane_covariance_planar_patch_is_disk():
+    # crates/spatialrust-gpu/src/kernels/covariances_grid.rs:371-395: 12x12
+    # grid step 0.1 at z = 0, radius 0.25, eps 1e-3 -> c22 ~ eps, c00, c11 > 0.5
+    xs, ys = np.meshgrid(np.arange(12) * 0.1, np.arange(12) * 0.1, indexing="ij")
+    x, y = xs.ravel().astype(F), ys.ravel().astype(F)
+    r = oracle.plane_covariances(x, y, np.zeros_like(x), 0.25, 1e-3)
+    assert r.cov.shape == (144, 6)
+    assert np.all(np.abs(r.cov[:, 2] - 1e-3) < 1e-2)
+    assert np.all(r.cov[:, 0] > 0.5) and np.all(r.cov[:, 1] > 0.5)
+
+
+def test_plane_covariance_tilted_plane_and_fallback():
+    # eigenvalues (eps, 1, 1) about the plane normal: I + (eps - 1) n n^T;
+    # an isolated point (1 point in its neighbourhood, < 3) -> (eps, eps, eps, 0, 0, 0)
+    eps = 0.01
+    u, v = np.meshgrid(np.arange(15) * 0.1, np.arange(15) * 0.1, indexing="ij")
+    u, v = u.ravel(), v.ravel()
+    x, y, z = u, v, 0.5 * u - 0.25 * v
+    x = np.append(x, 50.0).astype(F)
+    y = np.append(y, 50.0).astype(F)
+    z = np.append(z, 50.0).astype(F)
+    r = oracle.plane_covariances(x, y, z, 0.25, eps)
+    n = np.array([0.5, -0.25, -1.0])
+    n /= np.linalg.norm(n)
+    want = np.eye(3) + (eps - 1.0) * np.outer(n, n)
+    six = np.array([want[0, 0], want[1, 1], want[2, 2], want[0, 1], want[0, 2], want[1, 2]])
+    assert np.max(np.abs(r.cov[:-1] - six[None, :])) < 1e-5
+    assert np.array_equal(r.cov[-1], [eps, eps, eps, 0.0, 0.0, 0.0])
+    assert r.counts[-1] == 1
+
+
+def test_plane_covariance_counts_include_the_query():
+    rng = np.random.default_rng(5)
+    p = rng.uniform(0, 2, (800, 3)).astype(F)
+    r = oracle.plane_covariances(p[:, 0], p[:, 1], p[:, 2], 0.3, 1e-3)
+    brute = oracle.brute_radius_counts(p[:, 0], p[:, 1], p[:, 2], 0.3)
+    assert np.array_equal(r.counts, brute + 1)
+    with pytest.raises(oracle.OracleError):
+        oracle.plane_covariances(p[:, 0], p[:, 1], p[:, 2], 0.0, 1e-3)
+
+
 def test_plane_normals_upward_radius():
     # normal.rs:650-667 uses k=8 on a 5x5 unit grid; the radius-mode analogue
     # (r = 1.5 covers the 8-neighbourhood) must give the same upward normals.
