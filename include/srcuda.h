@@ -223,6 +223,61 @@ srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
 srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float radius,
                                    float epsilon, float *cov, srcu_normal_stats *stats);
 
+/* ---- bounded streaming voxel centroids ------------------------------------ */
+
+/* Replaces StreamingVoxelSource (crates/spatialrust-pipeline/src/streaming.rs:
+ * 334-700): global voxel centroids of a chunked stream.  The voxel of a point
+ * is floor(f64(v) / f64(leaf)) per axis (no origin, :986-994); points with a
+ * non-finite coordinate are skipped (:464-466); every column is averaged in
+ * FP64 over the whole stream; voxels come out in ascending (ix, iy, iz) order.
+ * Chunks are reduced on the device run by run; only the reduced runs stay
+ * resident (device memory under the context's HBM budget plays the part of
+ * the reference's disk spool).  push and finish use the context's sort
+ * buffers and stream; like the context, a stream belongs to one thread. */
+typedef struct srcu_stream_voxel srcu_stream_voxel;
+
+typedef struct srcu_stream_voxel_params {
+  float leaf_size;          /* > 0 and finite (StreamingVoxelConfig::new, streaming.rs:345-363) */
+  uint32_t n_attrs;         /* attribute columns in every chunk */
+  uint32_t attr_f64_mask;   /* bit a: attrs[a] of every chunk points at f64 data, not f32 */
+  uint32_t device_run_points; /* points sorted per device run; 0: max(run_points, 2^20) */
+  uint64_t run_points;      /* > 0: finite points per run of the reference's run limit */
+  uint64_t max_runs;        /* > 0: more runs than this fail, as flush_run does (:742-746) */
+  uint64_t spool_limit_bytes; /* 0: none; else the reference's spool extent rule: runs * 8 +
+                                 finite points * (32 + 8 * (3 + n_attrs)) bytes at most */
+} srcu_stream_voxel_params;
+
+typedef struct srcu_stream_voxel_info {
+  uint64_t points;          /* points pushed */
+  uint64_t finite_points;   /* points kept */
+  uint64_t runs;            /* the reference's run count: ceil(finite / run_points) */
+  uint64_t spool_bytes;     /* the reference's spool bytes for those runs */
+  uint64_t device_runs;     /* runs reduced on the device */
+  uint64_t partial_records; /* reduced records held before the final merge */
+  uint64_t voxels;          /* output voxels */
+} srcu_stream_voxel_info;
+
+typedef struct srcu_stream_voxel_out {
+  float *x;
+  float *y;
+  float *z;
+  double *const *attrs; /* n_attrs columns of FP64 means (nullable entries skip a column) */
+  int64_t *keys;        /* nullable: 3 int64 per voxel */
+  uint64_t *counts;     /* nullable: points per voxel */
+  int32_t on_device;
+} srcu_stream_voxel_out;
+
+srcu_status srcu_stream_voxel_create(srcu_ctx *ctx, const srcu_stream_voxel_params *params,
+                                     srcu_stream_voxel **out);
+/* Appends one chunk (packed columns, host or device; stride must be 0 or 1). */
+srcu_status srcu_stream_voxel_push(srcu_stream_voxel *sv, const srcu_cloud *chunk);
+/* Reduces the last run and merges every run; info is nullable. */
+srcu_status srcu_stream_voxel_finish(srcu_stream_voxel *sv, srcu_stream_voxel_info *info);
+/* Copies voxels [first, first + count) of the finished stream. */
+srcu_status srcu_stream_voxel_fetch(srcu_stream_voxel *sv, uint64_t first, uint64_t count,
+                                    const srcu_stream_voxel_out *out);
+void srcu_stream_voxel_destroy(srcu_stream_voxel *sv);
+
 /* ---- many clouds in one chain ---------------------------------------------- */
 
 /* Enqueues voxel -> normals for `count` clouds in one chain: the clouds'

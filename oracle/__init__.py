@@ -65,6 +65,9 @@ def _load():
     lib.oracle_plane_covariances.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float,
                                              ctypes.c_double, ctypes.c_int, P, P, P]
     lib.oracle_plane_covariances.restype = ctypes.c_int
+    lib.oracle_stream_voxel.argtypes = [P, P, P, P, ctypes.c_int, ctypes.c_size_t, ctypes.c_float,
+                                        P, P, P, P]
+    lib.oracle_stream_voxel.restype = ctypes.c_longlong
     lib.oracle_brute_radius_counts.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float, P]
     lib.oracle_brute_radius_counts.restype = None
     lib.oracle_compute_bounds.argtypes = [P, P, P, ctypes.c_size_t, P, P]
@@ -263,6 +266,37 @@ def plane_covariances(x, y, z, radius, epsilon, threads=0) -> PlaneCovResult:
     if rc != 0:
         raise OracleError(f"oracle_plane_covariances failed: {rc}")
     return PlaneCovResult(cov[:n], gap[:n], counts[:n])
+
+
+@dataclass
+class StreamVoxelResult:
+    keys: np.ndarray    # (V, 3) int64
+    counts: np.ndarray  # (V,) uint64
+    pos: np.ndarray     # (V, 3) float32
+    attrs: np.ndarray   # (V, n_attrs) float64 means
+
+
+def stream_voxel(x, y, z, attrs=(), leaf=1.0) -> StreamVoxelResult:
+    """StreamingVoxelSource's global voxel centroids (streaming.rs:334-700)
+    over the whole stream; attributes are FP64 columns."""
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    n = x.shape[0]
+    cols = [np.ascontiguousarray(a, np.float64) for a in attrs]
+    arr = (ctypes.c_void_p * max(len(cols), 1))(*[c.ctypes.data for c in cols])
+    m = max(n, 1)
+    keys = np.empty((m, 3), np.int64)
+    counts = np.empty(m, np.uint64)
+    pos = np.empty((m, 3), np.float32)
+    out_attrs = np.empty((m, max(len(cols), 1)), np.float64)
+    v = lib.oracle_stream_voxel(_ptr(x), _ptr(y), _ptr(z), ctypes.cast(arr, ctypes.c_void_p),
+                                len(cols), n, ctypes.c_float(leaf), _ptr(keys), _ptr(counts),
+                                _ptr(pos), _ptr(out_attrs))
+    if v == -4:
+        raise OracleError("voxel coordinate exceeds signed 64-bit range")
+    if v < 0:
+        raise OracleError(f"oracle_stream_voxel failed: {v}")
+    return StreamVoxelResult(keys[:v], counts[:v], pos[:v], out_attrs[:v, :len(cols)])
 
 
 def brute_radius_counts(x, y, z, radius) -> np.ndarray:

@@ -1408,6 +1408,95 @@ int oracle_plane_covariances(const float *x, const float *y, const float *z, siz
   return OR_OK;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Bounded streaming voxel (crates/spatialrust-pipeline/src/streaming.rs)    */
+/* ------------------------------------------------------------------------ */
+
+#define OR_ERR_KEY_RANGE (-4)
+
+typedef struct {
+  int64_t k[3];
+  uint64_t src; /* stream offset: ties keep stream order (:805-838) */
+} sv_item;
+
+static int cmp_sv_item(const void *a, const void *b) {
+  const sv_item *x = (const sv_item *)a, *y = (const sv_item *)b;
+  for (int i = 0; i < 3; ++i) {
+    if (x->k[i] < y->k[i]) return -1;
+    if (x->k[i] > y->k[i]) return 1;
+  }
+  return x->src < y->src ? -1 : (x->src > y->src ? 1 : 0);
+}
+
+/* voxel_coordinate (:986-994): floor(value / leaf) in f64; out of the i64
+ * range is an error; 2^63 saturates like `as i64`. */
+static int sv_coordinate(double value, double leaf, int64_t *out) {
+  double c = floor(value / leaf);
+  if (c < -9223372036854775808.0 || c > 9223372036854775808.0) return 0;
+  *out = c >= 9223372036854775808.0 ? INT64_MAX : (int64_t)c;
+  return 1;
+}
+
+/*
+ * StreamingVoxelSource over the whole stream at once (the result does not
+ * depend on the chunk or run sizes, :1099-1130): points with a non-finite
+ * coordinate are skipped (:464-466), keys by voxel_coordinate, every field
+ * summed per voxel in stream order with CompensatedSum (:240-262, 852-858),
+ * value sum / count (:631-633), voxels in ascending key order.  Fields are
+ * x, y, z (f32) and n_attrs FP64 attribute columns.  Outputs (capacity n):
+ * keys (3 per voxel), counts, positions as f32, attribute means in FP64.
+ * Returns the voxel count, or OR_ERR_KEY_RANGE.
+ */
+long long oracle_stream_voxel(const float *x, const float *y, const float *z,
+                              const double *const *attrs, int n_attrs, size_t n, float leaf_f32,
+                              int64_t *out_keys, uint64_t *out_counts, float *out_pos,
+                              double *out_attrs) {
+  const double leaf = (double)leaf_f32;
+  sv_item *items = (sv_item *)malloc((n ? n : 1) * sizeof(sv_item));
+  if (!items) return OR_ERR_NOMEM;
+  size_t m = 0;
+  for (size_t i = 0; i < n; ++i) {
+    const double p[3] = {(double)x[i], (double)y[i], (double)z[i]};
+    if (!isfinite(p[0]) || !isfinite(p[1]) || !isfinite(p[2])) continue;
+    for (int a = 0; a < 3; ++a)
+      if (!sv_coordinate(p[a], leaf, &items[m].k[a])) {
+        free(items);
+        return OR_ERR_KEY_RANGE;
+      }
+    items[m].src = i;
+    m++;
+  }
+  qsort(items, m, sizeof(sv_item), cmp_sv_item);
+  const int nf = 3 + n_attrs;
+  long long v = 0;
+  size_t s = 0;
+  while (s < m) {
+    size_t e = s + 1;
+    while (e < m && memcmp(items[e].k, items[s].k, sizeof(items[s].k)) == 0) e++;
+    for (int f = 0; f < nf; ++f) {
+      double sum = 0.0, corr = 0.0; /* CompensatedSum */
+      for (size_t t = s; t < e; ++t) {
+        const size_t i = items[t].src;
+        const double val = f == 0 ? (double)x[i] : f == 1 ? (double)y[i] : f == 2 ? (double)z[i]
+                                                                               : attrs[f - 3][i];
+        const double corrected = val - corr;
+        const double next = sum + corrected;
+        corr = (next - sum) - corrected;
+        sum = next;
+      }
+      const double mean = sum / (double)(e - s);
+      if (f < 3) out_pos[3 * v + f] = (float)mean;
+      else out_attrs[(size_t)n_attrs * v + (f - 3)] = mean;
+    }
+    memcpy(&out_keys[3 * v], items[s].k, sizeof(items[s].k));
+    out_counts[v] = e - s;
+    v++;
+    s = e;
+  }
+  free(items);
+  return v;
+}
+
 /* Exposes the f32 closed-form smallest eigenpair for unit tests. */
 void oracle_smallest_eigenpair_f32(const float c[6], float normal[3], float *curv) {
   rs_smallest_eigenpair(c[0], c[1], c[2], c[3], c[4], c[5], normal, curv);

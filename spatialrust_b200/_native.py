@@ -157,6 +157,25 @@ class SrcuServerStats(ctypes.Structure):
                  "all_p99_ms", "elapsed_s")]
 
 
+class SrcuStreamVoxelParams(ctypes.Structure):
+    _fields_ = [("leaf_size", ctypes.c_float), ("n_attrs", ctypes.c_uint32),
+                ("attr_f64_mask", ctypes.c_uint32), ("device_run_points", ctypes.c_uint32),
+                ("run_points", ctypes.c_uint64), ("max_runs", ctypes.c_uint64),
+                ("spool_limit_bytes", ctypes.c_uint64)]
+
+
+class SrcuStreamVoxelInfo(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in
+                ("points", "finite_points", "runs", "spool_bytes", "device_runs",
+                 "partial_records", "voxels")]
+
+
+class SrcuStreamVoxelOut(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("z", ctypes.c_void_p),
+                ("attrs", ctypes.c_void_p), ("keys", ctypes.c_void_p), ("counts", ctypes.c_void_p),
+                ("on_device", ctypes.c_int32)]
+
+
 KERNEL_IDS = ["begin", "bounds", "voxel_plan", "voxel_hist", "voxel_sort", "voxel_segments",
               "unpack_keys", "cell_plan", "cell_hist", "cell_sort", "cells", "hash", "ranges",
               "normals", "cluster"]
@@ -211,6 +230,13 @@ SIGNATURES = {
                                       ctypes.c_void_p], ctypes.c_int),
     "srcu_plane_covariances": ([_P, ctypes.POINTER(SrcuCloud), ctypes.c_float, ctypes.c_float,
                                 ctypes.c_void_p, ctypes.POINTER(SrcuNormalStats)], ctypes.c_int),
+    "srcu_stream_voxel_create": ([_P, ctypes.POINTER(SrcuStreamVoxelParams),
+                                  ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "srcu_stream_voxel_push": ([_P, ctypes.POINTER(SrcuCloud)], ctypes.c_int),
+    "srcu_stream_voxel_finish": ([_P, ctypes.POINTER(SrcuStreamVoxelInfo)], ctypes.c_int),
+    "srcu_stream_voxel_fetch": ([_P, ctypes.c_uint64, ctypes.c_uint64,
+                                 ctypes.POINTER(SrcuStreamVoxelOut)], ctypes.c_int),
+    "srcu_stream_voxel_destroy": ([_P], None),
     "srcu_server_create": ([ctypes.POINTER(SrcuServerConfig), ctypes.POINTER(ctypes.c_void_p)],
                            ctypes.c_int),
     "srcu_server_destroy": ([_P], None),
@@ -594,6 +620,89 @@ class Context:
         return dict(columns=[c[:v] for c in vcols], counts=counts[:v], nx=nouts[0][:v],
                     ny=nouts[1][:v], nz=nouts[2][:v], curvature=nouts[3][:v],
                     neighbor_counts=ncounts[:v], stats=_stats(stats))
+
+
+class StreamVoxel:
+    """srcu_stream_voxel: global voxel centroids of a chunked stream, reduced
+    run by run on the device (StreamingVoxelSource, streaming.rs:334-700).
+
+    attr_f64: one flag per attribute column; True columns are pushed and
+    averaged as FP64 (e.g. gps_time), the others as f32."""
+
+    def __init__(self, ctx: "Context", leaf: float, attr_f64=(), run_points: int = 1 << 20,
+                 max_runs: int = 1 << 40, spool_limit_bytes: int = 0, device_run_points: int = 0):
+        self._ctx = ctx
+        self._lib = ctx._lib
+        self.attr_f64 = tuple(bool(f) for f in attr_f64)
+        mask = sum(1 << i for i, f in enumerate(self.attr_f64) if f)
+        prm = SrcuStreamVoxelParams(ctypes.c_float(leaf), len(self.attr_f64), mask,
+                                    int(device_run_points), int(run_points), int(max_runs),
+                                    int(spool_limit_bytes))
+        h = ctypes.c_void_p()
+        ctx._check(self._lib.srcu_stream_voxel_create(ctx._h, ctypes.byref(prm), ctypes.byref(h)))
+        self._h = h
+        self.info = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.srcu_stream_voxel_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def push(self, x, y, z, attrs=()):
+        if len(attrs) != len(self.attr_f64):
+            raise InvalidArgument(f"expected {len(self.attr_f64)} attribute columns, got {len(attrs)}")
+        keep = _Keep()
+        on_dev = _is_device(x)
+        if on_dev:
+            import torch
+            cols = [x, y, z, *attrs]
+            want = [torch.float32] * 3 + [torch.float64 if f else torch.float32 for f in self.attr_f64]
+            for c, w in zip(cols, want):
+                if not _is_device(c) or c.dtype != w or not c.is_contiguous():
+                    raise InvalidArgument("device columns must be contiguous CUDA tensors of the "
+                                          "stream's column types")
+        else:
+            cols = [keep.add(np.ascontiguousarray(c, np.float32)) for c in (x, y, z)]
+            cols += [keep.add(np.ascontiguousarray(a, np.float64 if f else np.float32))
+                     for a, f in zip(attrs, self.attr_f64)]
+        n = int(cols[0].shape[0])
+        for c in cols:
+            if int(c.shape[0]) != n:
+                raise BufferLengthMismatch(f"expected {n}, found {int(c.shape[0])}")
+        arr = keep.add((ctypes.c_void_p * max(len(attrs), 1))(*[_addr(c) for c in cols[3:]]))
+        cloud = SrcuCloud(_addr(cols[0]), _addr(cols[1]), _addr(cols[2]),
+                          ctypes.cast(arr, ctypes.c_void_p), len(attrs), int(on_dev), n)
+        self._ctx._check(self._lib.srcu_stream_voxel_push(self._h, ctypes.byref(cloud)))
+
+    def finish(self) -> dict:
+        info = SrcuStreamVoxelInfo()
+        self._ctx._check(self._lib.srcu_stream_voxel_finish(self._h, ctypes.byref(info)))
+        self.info = {k: int(getattr(info, k)) for k, _ in SrcuStreamVoxelInfo._fields_}
+        return self.info
+
+    def fetch(self, first: int = 0, count: int | None = None):
+        """(x, y, z, attrs (count, n_attrs) FP64 means, keys (count, 3), counts)."""
+        total = self.info["voxels"] if self.info else 0
+        count = total - first if count is None else count
+        m = max(count, 1)
+        pos = [np.empty(m, np.float32) for _ in range(3)]
+        attrs = [np.empty(m, np.float64) for _ in self.attr_f64]
+        keys = np.empty((m, 3), np.int64)
+        counts = np.empty(m, np.uint64)
+        keep = _Keep()
+        arr = keep.add((ctypes.c_void_p * max(len(attrs), 1))(*[a.ctypes.data for a in attrs]))
+        out = SrcuStreamVoxelOut(pos[0].ctypes.data, pos[1].ctypes.data, pos[2].ctypes.data,
+                                 ctypes.cast(arr, ctypes.c_void_p), keys.ctypes.data,
+                                 counts.ctypes.data, 0)
+        self._ctx._check(self._lib.srcu_stream_voxel_fetch(self._h, first, count, ctypes.byref(out)))
+        a = np.stack([c[:count] for c in attrs], axis=1) if attrs else np.zeros((count, 0))
+        return pos[0][:count], pos[1][:count], pos[2][:count], a, keys[:count], counts[:count]
 
 
 class ChainGraph:

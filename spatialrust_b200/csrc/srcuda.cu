@@ -1260,3 +1260,5 @@ int srcu_profile_read(srcu_ctx *ctx, srcu_kernel_stat *out, int max_entries, int
 
 // The allocation-free variant of the voxel chain shares this translation unit's kernels.
 #include "noalloc.cu"
+// So does the bounded streaming voxel.
+#include "stream.cu"

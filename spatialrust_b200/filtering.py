@@ -80,8 +80,13 @@ def _widen(col: np.ndarray) -> np.ndarray:
 
 
 def _round_half_away(v: np.ndarray) -> np.ndarray:
-    d = v.astype(np.float64)
-    return np.trunc(d + np.copysign(0.5, d))
+    """f64::round: half away from zero.  The fraction d - trunc(d) is exact, so
+    this does not round 0.49999999999999994 up as trunc(d + 0.5) would."""
+    d = np.asarray(v, np.float64)
+    t = np.trunc(d)
+    with np.errstate(invalid="ignore"):
+        up = np.abs(d - t) >= 0.5
+    return t + np.where(up, np.sign(d), 0.0)
 
 
 def narrow(values: np.ndarray, dtype: DType) -> np.ndarray:

@@ -59,6 +59,10 @@ def test_struct_layouts_match_c(tmp_path):
         'printf("%zu %zu %zu %zu %zu\\n", offsetof(srcu_cloud, n),'
         " offsetof(srcu_normal_params, include_self), offsetof(srcu_frame_view, n_attrs),"
         " offsetof(srcu_request_result, points), offsetof(srcu_server_stats, frame_p50_ms));\n"
+        'printf("%zu %zu %zu %zu %zu\\n", sizeof(srcu_stream_voxel_params),'
+        " sizeof(srcu_stream_voxel_info), sizeof(srcu_stream_voxel_out),"
+        " offsetof(srcu_stream_voxel_params, run_points),"
+        " offsetof(srcu_stream_voxel_out, on_device));\n"
         "return 0;}\n")
     exe = tmp_path / "sizes"
     subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)])
@@ -72,6 +76,12 @@ def test_struct_layouts_match_c(tmp_path):
     assert offs == [_native.SrcuCloud.n.offset, _native.SrcuNormalParams.include_self.offset,
                     _native.SrcuFrameView.n_attrs.offset, _native.SrcuRequestResult.points.offset,
                     _native.SrcuServerStats.frame_p50_ms.offset]
+    stream = [int(v) for v in lines[2].split()]
+    assert stream == [ctypes.sizeof(_native.SrcuStreamVoxelParams),
+                      ctypes.sizeof(_native.SrcuStreamVoxelInfo),
+                      ctypes.sizeof(_native.SrcuStreamVoxelOut),
+                      _native.SrcuStreamVoxelParams.run_points.offset,
+                      _native.SrcuStreamVoxelOut.on_device.offset]
 
 
 def test_header_compiles_as_c_and_cxx(tmp_path):

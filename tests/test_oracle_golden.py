@@ -321,3 +321,37 @@ def test_parallel_worker_count():
     assert oracle.parallel_worker_count(4096, 8) == 1
     assert oracle.parallel_worker_count(100_000, 8) == 6
     assert oracle.parallel_worker_count(2_000_000, 8) == 8
+
+
+# ---- bounded streaming voxel (crates/spatialrust-pipeline/src/streaming.rs) --
+
+def test_stream_voxel_identical_output_golden():
+    # streaming.rs:1098-1130: leaf 1.0 -> [[0.15,0,0],[1.2,0,0],[2.8,0,0]]
+    r = oracle.stream_voxel([1.3, 0.1, 1.1, 0.2, 2.8], [0] * 5, [0] * 5, leaf=1.0)
+    assert r.pos.tolist() == np.array([[0.15, 0, 0], [1.2, 0, 0], [2.8, 0, 0]], F).tolist()
+    assert r.keys.tolist() == [[0, 0, 0], [1, 0, 0], [2, 0, 0]]
+    assert r.counts.tolist() == [2, 2, 1]
+
+
+def test_stream_voxel_averages_attributes_golden():
+    # streaming.rs:1132-1149: intensities 10, 20 | 50 -> [15, 50]
+    r = oracle.stream_voxel([0.1, 0.2, 1.1], [0] * 3, [0] * 3,
+                            attrs=[np.array([10.0, 20.0, 50.0])], leaf=1.0)
+    assert r.attrs[:, 0].tolist() == [15.0, 50.0]
+
+
+def test_stream_voxel_skips_non_finite_and_floors_negatives():
+    r = oracle.stream_voxel([0.0, -0.5, np.nan, 2.0, -1.0], [0, 0, 0, np.inf, 0], [0] * 5, leaf=1.0)
+    assert r.keys.tolist() == [[-1, 0, 0], [0, 0, 0]]
+    assert r.counts.tolist() == [2, 1]
+    with pytest.raises(oracle.OracleError):
+        oracle.stream_voxel([1e30], [0], [0], leaf=1e-12)
+
+
+def test_stream_voxel_compensated_sum_beats_plain_sum():
+    # CompensatedSum (streaming.rs:240-262): 1 + 1e-16 * 1000 keeps the small terms
+    x = np.full(1001, 0.5, F)
+    a = np.full(1001, 1e-16)
+    a[0] = 1.0
+    r = oracle.stream_voxel(x, np.zeros_like(x), np.zeros_like(x), attrs=[a], leaf=1.0)
+    assert r.attrs[0, 0] == (1.0 + 1e-13) / 1001
