@@ -278,6 +278,43 @@ srcu_status srcu_stream_voxel_fetch(srcu_stream_voxel *sv, uint64_t first, uint6
                                     const srcu_stream_voxel_out *out);
 void srcu_stream_voxel_destroy(srcu_stream_voxel *sv);
 
+/* ---- LAS point records ---------------------------------------------------- */
+
+/* One LAS file's point data layout (public header fields, ASPRS LAS 1.4 R15
+ * table 3) and an optional FP64 origin. */
+typedef struct srcu_las_format {
+  uint32_t point_format;   /* point data record format 0-10 (header byte 104, compression bits clear) */
+  uint32_t record_length;  /* point data record length (header bytes 105-106), extra bytes included */
+  double scale[3];         /* x, y, z scale factors (header bytes 131-154) */
+  double offset[3];        /* x, y, z offsets (header bytes 155-178) */
+  int32_t has_origin;      /* 1: subtract origin from scale * X + offset in FP64 before the f32 */
+  int32_t reserved;
+  double origin[3];
+} srcu_las_format;
+
+/* Decoded columns (n entries each; every pointer but x, y, z is nullable). */
+typedef struct srcu_las_out {
+  float *x;
+  float *y;
+  float *z;
+  float *intensity;        /* F32, as schema_for_las_header's point_xyzi */
+  uint8_t *classification; /* class number: low 5 bits for formats 0-5, the byte for 6-10 */
+  double *gps_time;        /* formats 1, 3-10 */
+  uint16_t *red;           /* formats 2, 3, 5, 7, 8, 10 */
+  uint16_t *green;
+  uint16_t *blue;
+  int32_t on_device;
+} srcu_las_out;
+
+/* Decodes n uncompressed LAS point records (records: n * record_length
+ * bytes, host or device memory as records_on_device) into columns, the
+ * fields read_las keeps (crates/spatialrust-io/src/las/reader.rs:242-279):
+ * each coordinate is scale * X + offset in FP64 (minus origin when
+ * has_origin), stored as f32.  Synchronous. */
+srcu_status srcu_las_decode(srcu_ctx *ctx, const void *records, uint64_t n,
+                            int32_t records_on_device, const srcu_las_format *fmt,
+                            const srcu_las_out *out);
+
 /* ---- many clouds in one chain ---------------------------------------------- */
 
 /* Enqueues voxel -> normals for `count` clouds in one chain: the clouds'
@@ -439,6 +476,7 @@ typedef enum srcu_kernel_id {
   SRCU_K_RANGES,         /* 3x3 neighbour column ranges */
   SRCU_K_NORMALS,        /* radius neighbours + covariance + eigensolve */
   SRCU_K_CLUSTER,        /* Euclidean clustering: union-find over the radius grid */
+  SRCU_K_LAS_DECODE,     /* LAS point records -> columns */
   SRCU_K_COUNT
 } srcu_kernel_id;
 

@@ -68,6 +68,9 @@ def _load():
     lib.oracle_stream_voxel.argtypes = [P, P, P, P, ctypes.c_int, ctypes.c_size_t, ctypes.c_float,
                                         P, P, P, P]
     lib.oracle_stream_voxel.restype = ctypes.c_longlong
+    lib.oracle_las_decode.argtypes = [P, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, P, P,
+                                      ctypes.c_int, P, P, P, P, P, P, P, P]
+    lib.oracle_las_decode.restype = ctypes.c_int
     lib.oracle_brute_radius_counts.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float, P]
     lib.oracle_brute_radius_counts.restype = None
     lib.oracle_compute_bounds.argtypes = [P, P, P, ctypes.c_size_t, P, P]
@@ -297,6 +300,33 @@ def stream_voxel(x, y, z, attrs=(), leaf=1.0) -> StreamVoxelResult:
     if v < 0:
         raise OracleError(f"oracle_stream_voxel failed: {v}")
     return StreamVoxelResult(keys[:v], counts[:v], pos[:v], out_attrs[:v, :len(cols)])
+
+
+def las_decode(records, point_format, record_length, scale, offset, origin=None) -> dict:
+    """The point-record fields read_las keeps (reader.rs:242-279), decoded on
+    the CPU: x, y, z (f32 of scale * X + offset [- origin] in f64), intensity,
+    classification, gps_time, red, green, blue."""
+    lib = _load()
+    rec = np.ascontiguousarray(np.frombuffer(bytes(records), np.uint8) if not isinstance(
+        records, np.ndarray) else records, np.uint8)
+    n = rec.nbytes // record_length
+    m = max(n, 1)
+    out = {k: np.zeros(m, np.float32) for k in ("x", "y", "z", "intensity")}
+    out["classification"] = np.zeros(m, np.uint8)
+    out["gps_time"] = np.zeros(m, np.float64)
+    rgb = np.zeros(3 * m, np.uint16)
+    sc = np.asarray(scale, np.float64)
+    of = np.asarray(offset, np.float64)
+    org = np.asarray(origin if origin is not None else (0, 0, 0), np.float64)
+    rc = lib.oracle_las_decode(_ptr(rec), n, point_format, record_length, _ptr(sc), _ptr(of),
+                               int(origin is not None), _ptr(org), _ptr(out["x"]), _ptr(out["y"]),
+                               _ptr(out["z"]), _ptr(out["intensity"]), _ptr(out["classification"]),
+                               _ptr(out["gps_time"]), _ptr(rgb))
+    if rc != 0:
+        raise OracleError(f"oracle_las_decode failed: {rc}")
+    out = {k: v[:n] for k, v in out.items()}
+    out["red"], out["green"], out["blue"] = rgb[:n], rgb[n:2 * n], rgb[2 * n:3 * n]
+    return out
 
 
 def brute_radius_counts(x, y, z, radius) -> np.ndarray:

@@ -1497,6 +1497,55 @@ long long oracle_stream_voxel(const float *x, const float *y, const float *z,
   return v;
 }
 
+/* ------------------------------------------------------------------------ */
+/* LAS point records (crates/spatialrust-io/src/las/reader.rs:242-279)       */
+/* ------------------------------------------------------------------------ */
+
+static uint32_t le_u32(const uint8_t *p) {
+  return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+static uint16_t le_u16(const uint8_t *p) { return (uint16_t)(p[0] | (p[1] << 8)); }
+
+/*
+ * The fields read_las keeps, from uncompressed point records of formats 0-10
+ * (ASPRS LAS 1.4 R15 tables 7-17; the reference delegates the byte layout to
+ * the `las` crate 0.9): x = (f32)(scale * X + offset [- origin]) with the
+ * f64 products and sums rounded step by step, intensity as f32,
+ * classification (low 5 bits of byte 15 for formats 0-5, byte 16 for 6-10),
+ * gps_time (f64 at byte 20, or 22 for formats 6-10), red/green/blue (u16 at
+ * byte 20 for format 2, 28 for 3 and 5, 30 for 7, 8 and 10).  rgb holds 3
+ * columns of n.  Returns 0, or OR_ERR_INVALID for an unknown format.
+ */
+int oracle_las_decode(const uint8_t *rec, size_t n, int format, int record_length,
+                      const double *scale, const double *offset, int has_origin,
+                      const double *origin, float *x, float *y, float *z, float *intensity,
+                      uint8_t *cls, double *gps, uint16_t *rgb) {
+  static const int gps_off[11] = {-1, 20, -1, 20, 20, 20, 22, 22, 22, 22, 22};
+  static const int rgb_off[11] = {-1, -1, 20, 28, -1, 28, -1, 30, 30, -1, 30};
+  if (format < 0 || format > 10) return OR_ERR_INVALID;
+  float *pos[3] = {x, y, z};
+  for (size_t i = 0; i < n; ++i) {
+    const uint8_t *r = rec + i * (size_t)record_length;
+    for (int a = 0; a < 3; ++a) {
+      const int32_t raw = (int32_t)le_u32(r + 4 * a);
+      double v = scale[a] * (double)raw;
+      v = v + offset[a];
+      if (has_origin) v = v - origin[a];
+      pos[a][i] = (float)v;
+    }
+    intensity[i] = (float)le_u16(r + 12);
+    cls[i] = format >= 6 ? r[16] : (uint8_t)(r[15] & 0x1f);
+    if (gps_off[format] >= 0) {
+      uint64_t bits = (uint64_t)le_u32(r + gps_off[format]) |
+                      ((uint64_t)le_u32(r + gps_off[format] + 4) << 32);
+      memcpy(&gps[i], &bits, 8);
+    }
+    if (rgb_off[format] >= 0)
+      for (int c = 0; c < 3; ++c) rgb[c * n + i] = le_u16(r + rgb_off[format] + 2 * c);
+  }
+  return OR_OK;
+}
+
 /* Exposes the f32 closed-form smallest eigenpair for unit tests. */
 void oracle_smallest_eigenpair_f32(const float c[6], float normal[3], float *curv) {
   rs_smallest_eigenpair(c[0], c[1], c[2], c[3], c[4], c[5], normal, curv);

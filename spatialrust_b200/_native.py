@@ -176,9 +176,22 @@ class SrcuStreamVoxelOut(ctypes.Structure):
                 ("on_device", ctypes.c_int32)]
 
 
+class SrcuLasFormat(ctypes.Structure):
+    _fields_ = [("point_format", ctypes.c_uint32), ("record_length", ctypes.c_uint32),
+                ("scale", ctypes.c_double * 3), ("offset", ctypes.c_double * 3),
+                ("has_origin", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("origin", ctypes.c_double * 3)]
+
+
+class SrcuLasOut(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in
+                ("x", "y", "z", "intensity", "classification", "gps_time", "red", "green", "blue")] + [
+                ("on_device", ctypes.c_int32)]
+
+
 KERNEL_IDS = ["begin", "bounds", "voxel_plan", "voxel_hist", "voxel_sort", "voxel_segments",
               "unpack_keys", "cell_plan", "cell_hist", "cell_sort", "cells", "hash", "ranges",
-              "normals", "cluster"]
+              "normals", "cluster", "las_decode"]
 
 
 # Every symbol include/srcuda.h declares, with its ctypes signature.
@@ -237,6 +250,8 @@ SIGNATURES = {
     "srcu_stream_voxel_fetch": ([_P, ctypes.c_uint64, ctypes.c_uint64,
                                  ctypes.POINTER(SrcuStreamVoxelOut)], ctypes.c_int),
     "srcu_stream_voxel_destroy": ([_P], None),
+    "srcu_las_decode": ([_P, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32,
+                         ctypes.POINTER(SrcuLasFormat), ctypes.POINTER(SrcuLasOut)], ctypes.c_int),
     "srcu_server_create": ([ctypes.POINTER(SrcuServerConfig), ctypes.POINTER(ctypes.c_void_p)],
                            ctypes.c_int),
     "srcu_server_destroy": ([_P], None),

@@ -71,6 +71,7 @@ class FieldSemantic(enum.Enum):
     ColorG = "g"
     ColorB = "b"
     Label = "label"
+    TimeOffset = "time_offset"
     Custom = "custom"
 
 

@@ -156,7 +156,7 @@ const char *const kKernelNames[SRCU_K_COUNT] = {
     "k_begin",          "k_bounds",        "k_voxel_plan",  "(in k_sort<voxel>)",
     "k_sort<voxel>",    "k_voxel_segments", "k_unpack_voxel_keys", "k_cell_plan",
     "(in k_sort<cell>)", "k_sort<cell>",    "k_cells",       "k_column_insert",
-    "k_ranges",         "k_normals",       "k_cluster_union"};
+    "k_ranges",         "k_normals",       "k_cluster_union", "k_las_decode"};
 
 // Counts the launches of one kernel group and, when its bit is set in
 // prof_mask, brackets them with CUDA events on the context stream.
@@ -1260,5 +1260,6 @@ int srcu_profile_read(srcu_ctx *ctx, srcu_kernel_stat *out, int max_entries, int
 
 // The allocation-free variant of the voxel chain shares this translation unit's kernels.
 #include "noalloc.cu"
-// So does the bounded streaming voxel.
+// So do the bounded streaming voxel and the LAS record decoder.
 #include "stream.cu"
+#include "las.cu"
