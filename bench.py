@@ -71,6 +71,10 @@ def parse():
                     help="skip the 5M-point shapes radius-normals measurement")
     ap.add_argument("--no-cluster", action="store_true",
                     help="skip the Euclidean cluster-roots measurement")
+    ap.add_argument("--no-plane-cov", action="store_true",
+                    help="skip the GICP plane-covariance leg")
+    ap.add_argument("--no-las-stream", action="store_true",
+                    help="skip the LAS ingest -> streaming voxel leg")
     ap.add_argument("--no-serving", action="store_true",
                     help="skip the serving-loop (Poisson arrivals) measurement")
     ap.add_argument("--serving-rates", default="100,500,1000,2000",
@@ -456,6 +460,10 @@ def run_gpu(args):
         line["shapes"] = run_shapes(args, torch, dev, stream)
     if not args.no_cluster and rank == 0:
         line["cluster"] = run_cluster(args, torch, dev, stream, cloud)
+    if not args.no_plane_cov and rank == 0:
+        line["plane_cov"] = run_plane_cov(args, torch, dev, stream, cloud)
+    if not args.no_las_stream and rank == 0:
+        line["las_stream"] = run_las_stream(args, torch, dev, stream, cloud)
     if not args.no_serving:
         line["serving"] = run_serving(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -631,6 +639,231 @@ def run_cluster(args, torch, dev, stream, cloud):
                 sample=f"all {n} points once: the reference's sparse-cell union-find "
                        "(euclidean_cluster.rs -> uniform_grid.rs:148-250), C restatement")
         out["tolerances"].append(entry)
+    ctx.close()
+    return out
+
+
+def hbm_peak():
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(pp)) if os.path.exists(pp) else {}
+    return peaks.get("hbm_gbs", 6650.0), ("MEASURED_PEAKS.json hbm_gbs (measured)"
+                                          if "hbm_gbs" in peaks else "fallback 6650 GB/s")
+
+
+PLANE_RADIUS = 0.3
+PLANE_EPS = 1e-3
+
+
+def run_plane_cov(args, torch, dev, stream, cloud):
+    """GICP plane covariances (srcu_plane_covariances) of every point of the
+    2M-point scan, radius 0.3 m, eps 1e-3, device-resident in and out; CPU
+    baseline: the FP64 oracle (KD-tree radius neighbourhoods, all host
+    threads) on the same points."""
+    import oracle
+    from spatialrust_b200 import _native
+    lib = _native.load()
+    n = cloud.n
+    cols = [torch.from_numpy(a).to(dev) for a in (cloud.x, cloud.y, cloud.z)]
+    cov = torch.empty((n, 6), dtype=torch.float32, device=dev)
+    keep = _native._Keep()
+    dcloud = _native.make_cloud(cols[0], cols[1], cols[2], [], keep)
+    ctx = _native.Context(dev.index)
+    ctx.set_stream(stream.cuda_stream)
+    stats = _native.SrcuNormalStats()
+
+    def step():
+        ctx._check(lib.srcu_plane_covariances(ctx.handle, ctypes.byref(dcloud),
+                                              ctypes.c_float(PLANE_RADIUS),
+                                              ctypes.c_float(PLANE_EPS), cov.data_ptr(),
+                                              ctypes.byref(stats)))
+    for _ in range(3):
+        step()
+    ctx.profile_enable(["normals"])
+    ctx.profile_read(reset=True)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    a.record(stream)
+    for _ in range(reps):
+        step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    prof = ctx.profile_read(reset=True)["normals"]
+    kernel_ms = prof["total_ms"] / max(prof["timed_regions"], 1)
+    out = dict(workload=f"georef_scan_2M: GICP plane covariances r {PLANE_RADIUS} eps {PLANE_EPS}",
+               points=n, ms=ms, mpts_s=n / ms / 1e3, kernel_ms=kernel_ms,
+               valid=int(stats.valid_count), fallback=int(stats.invalid_count),
+               fp64_eigensolves=int(stats.fp64_eigensolves),
+               timing="CUDA events around 5 synchronous calls (grid build + covariance kernel)")
+    if not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        oracle.plane_covariances(cloud.x, cloud.y, cloud.z, PLANE_RADIUS, PLANE_EPS)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = dict(
+            value=n / cpu_s / 1e6, unit="Mpoints/s", cores=os.cpu_count() or 1, kind="port",
+            sample=f"all {n} points once: KD-tree radius neighbourhoods, FP64 covariance and "
+                   "Jacobi, C restatement of covariances_grid.rs:87-206")
+    ctx.close()
+    return out
+
+
+LAS_TILES = 8          # the 2M scan tiled 8 times, 250 m apart in x: 16M points
+LAS_CHUNK = 1 << 20    # records per decode call / points per streaming push
+STREAM_LEAF = 0.1
+
+
+def run_las_stream(args, torch, dev, stream, cloud):
+    """LAS ingest -> bounded streaming voxel.  16M LAS 1.4 point-format-1
+    records (28 B: mm-scaled i32 XYZ, intensity, classification, GPS time) of
+    the scan tiled 8x, decoded on the device with the FP64 origin subtracted
+    (srcu_las_decode), then pushed in 1M-point chunks through the streaming
+    voxel at leaf 0.1 with intensity (f32) and GPS time (f64) averaged
+    (srcu_stream_voxel_*).  decode: device-resident records -> columns, kernel
+    time by CUDA events; stream: device-resident columns -> voxels; e2e:
+    pinned host LAS bytes -> H2D + decode per chunk -> push -> finish -> all
+    voxels fetched to the host."""
+    import oracle
+    from spatialrust_b200 import _native, las
+    n1 = cloud.n
+    n = n1 * LAS_TILES
+    origin = tuple(float(v) for v in cloud.origin)
+    wx = np.concatenate([cloud.x.astype(np.float64) + origin[0] + 250.0 * t
+                         for t in range(LAS_TILES)])
+    wy = np.tile(cloud.y.astype(np.float64) + origin[1], LAS_TILES)
+    wz = np.tile(cloud.z.astype(np.float64) + origin[2], LAS_TILES)
+    buf = las.encode_las(wx, wy, wz, point_format=1, scale=(0.001,) * 3,
+                         offset=tuple(np.floor(origin)),
+                         intensity=np.tile((cloud.intensity * 65535).astype(np.int64), LAS_TILES),
+                         classification=np.arange(n) % 8,
+                         gps_time=1.4e9 + np.arange(n) * 1e-5)
+    del wx, wy, wz
+    h = las.parse_header(buf)
+    rl = h.record_length
+    pinned = torch.empty(n * rl, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = np.frombuffer(buf, np.uint8, n * rl, h.offset_to_point_data)
+    rec_dev = pinned.to(dev)
+    ctx = _native.Context(dev.index)
+    ctx.set_stream(stream.cuda_stream)
+    lib = ctx._lib
+    f32 = dict(dtype=torch.float32, device=dev)
+    cols = dict(x=torch.empty(n, **f32), y=torch.empty(n, **f32), z=torch.empty(n, **f32),
+                intensity=torch.empty(n, **f32),
+                classification=torch.empty(n, dtype=torch.uint8, device=dev),
+                gps_time=torch.empty(n, dtype=torch.float64, device=dev))
+    fmt = _native.SrcuLasFormat(1, rl, (ctypes.c_double * 3)(*h.scale),
+                                (ctypes.c_double * 3)(*h.offset), 1, 0,
+                                (ctypes.c_double * 3)(*origin))
+
+    def las_out(lo, hi):
+        ptrs = [cols[k][lo:hi].data_ptr() for k in
+                ("x", "y", "z", "intensity", "classification", "gps_time")]
+        return _native.SrcuLasOut(*ptrs, 0, 0, 0, 1)
+
+    full_out = las_out(0, n)
+
+    def decode_all():
+        ctx._check(lib.srcu_las_decode(ctx.handle, ctypes.c_void_p(rec_dev.data_ptr()), n, 1,
+                                       ctypes.byref(fmt), ctypes.byref(full_out)))
+    for _ in range(3):
+        decode_all()
+    ctx.profile_enable(["las_decode"])
+    ctx.profile_read(reset=True)
+    for _ in range(10):
+        decode_all()
+    prof = ctx.profile_read(reset=True)["las_decode"]
+    ctx.profile_enable([])
+    dec_ms = prof["total_ms"] / max(prof["timed_regions"], 1)
+    bytes_per_rec = rl + 4 * 4 + 1 + 8
+    hbm, peak_src = hbm_peak()
+    achieved = n * bytes_per_rec / (dec_ms / 1e3) / 1e9
+
+    def stream_all():
+        sv = _native.StreamVoxel(ctx, STREAM_LEAF, [False, True])
+        for lo in range(0, n, LAS_CHUNK):
+            hi = min(n, lo + LAS_CHUNK)
+            sv.push(cols["x"][lo:hi], cols["y"][lo:hi], cols["z"][lo:hi],
+                    [cols["intensity"][lo:hi], cols["gps_time"][lo:hi]])
+        info = sv.finish()
+        return sv, info
+
+    sv, info = stream_all()
+    sv.close()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    t0 = time.perf_counter()
+    a.record(stream)
+    for _ in range(reps):
+        sv, info = stream_all()
+        sv.close()
+    b.record(stream)
+    torch.cuda.synchronize()
+    stream_ms = a.elapsed_time(b) / reps
+    stream_wall_ms = (time.perf_counter() - t0) * 1e3 / reps
+
+    vmax = n  # voxel capacity of the pinned result buffers
+    res_host = dict(x=torch.empty(vmax, dtype=torch.float32, pin_memory=True),
+                    y=torch.empty(vmax, dtype=torch.float32, pin_memory=True),
+                    z=torch.empty(vmax, dtype=torch.float32, pin_memory=True),
+                    intensity=torch.empty(vmax, dtype=torch.float64, pin_memory=True),
+                    gps_time=torch.empty(vmax, dtype=torch.float64, pin_memory=True))
+    attr_ptrs = (ctypes.c_void_p * 2)(res_host["intensity"].data_ptr(),
+                                      res_host["gps_time"].data_ptr())
+    fetch_out = _native.SrcuStreamVoxelOut(res_host["x"].data_ptr(), res_host["y"].data_ptr(),
+                                           res_host["z"].data_ptr(),
+                                           ctypes.cast(attr_ptrs, ctypes.c_void_p), None, None, 0)
+
+    def e2e_once():
+        sv = _native.StreamVoxel(ctx, STREAM_LEAF, [False, True])
+        for lo in range(0, n, LAS_CHUNK):
+            hi = min(n, lo + LAS_CHUNK)
+            o = las_out(lo, hi)
+            ctx._check(lib.srcu_las_decode(ctx.handle, ctypes.c_void_p(pinned.data_ptr() + lo * rl),
+                                           hi - lo, 0, ctypes.byref(fmt), ctypes.byref(o)))
+            sv.push(cols["x"][lo:hi], cols["y"][lo:hi], cols["z"][lo:hi],
+                    [cols["intensity"][lo:hi], cols["gps_time"][lo:hi]])
+        inf = sv.finish()
+        ctx._check(lib.srcu_stream_voxel_fetch(sv._h, 0, inf["voxels"], ctypes.byref(fetch_out)))
+        sv.close()
+        return inf, None
+    e2e_once()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a.record(stream)
+    inf, res = e2e_once()
+    b.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b)
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    out = dict(
+        workload=(f"LAS 1.4 format 1 ({rl} B records, mm scale), {n} points (georef scan x"
+                  f"{LAS_TILES}) -> FP64-origin decode -> streaming voxel leaf {STREAM_LEAF} "
+                  "(intensity f32 + GPS time f64 averaged)"),
+        points=n, voxels=int(info["voxels"]), device_runs=int(info["device_runs"]),
+        partial_records=int(info["partial_records"]),
+        decode=dict(kernel_ms=dec_ms, grecords_s=n / dec_ms / 1e6,
+                    roofline=dict(bound="hbm", achieved=achieved, peak=hbm, unit="GB/s",
+                                  frac=achieved / hbm, peak_source=peak_src,
+                                  algorithmic_bytes_per_record=bytes_per_rec)),
+        stream=dict(ms=stream_ms, wall_ms=stream_wall_ms, mpts_s=n / stream_ms / 1e3,
+                    timing="CUDA events around 3 device-resident streams (16 pushes + finish)"),
+        e2e=dict(ms=e2e_ms, wall_ms=wall_ms, mpts_s=n / e2e_ms / 1e3,
+                 h2d_bytes=n * rl, d2h_bytes=int(inf["voxels"]) * (12 + 8 * 2),
+                 api="srcu_las_decode (pinned host records) + srcu_stream_voxel_push/finish/fetch "
+                     "(positions and both attribute means into pinned host buffers)"),
+    )
+    if not args.no_cpu_baseline:
+        rec1 = pinned.numpy()[: n1 * rl]
+        t0 = time.perf_counter()
+        d = oracle.las_decode(rec1, 1, rl, h.scale, h.offset, origin)
+        oracle.stream_voxel(d["x"], d["y"], d["z"], [d["intensity"], d["gps_time"]], leaf=STREAM_LEAF)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = dict(
+            value=n1 / cpu_s / 1e6, unit="Mpoints/s", cores=1, kind="port",
+            sample=f"the first {n1} records once: LAS decode + global streaming voxel "
+                   "(streaming.rs:414-676 semantics, C restatement, one thread, no disk spool)")
+    del rec_dev, pinned
     ctx.close()
     return out
 

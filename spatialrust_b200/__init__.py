@@ -1,6 +1,8 @@
 """spatialrust_b200: SpatialRust's uniform-grid hot path (VoxelGrid centroid
 downsample + radius-mode normal estimation) as hand-written CUDA for B200
-(sm_100a), behind the reference's own API shape.
+(sm_100a), behind the reference's own API shape -- with the consumers on the
+same grid (Euclidean cluster roots, GICP plane covariances), the bounded
+streaming voxel and LAS record decoding on either side of it.
 
 The compute path is libsrcuda.so (C ABI: include/srcuda.h).  This Python
 layer mirrors the reference's Rust API so that code written against
@@ -16,6 +18,10 @@ from .filtering import (AttributeAggregation, VoxelAggregationMode, VoxelGridDow
                         VoxelGridDownsampleConfig)
 from .segmentation import (EuclideanClusterConfig, EuclideanClusterExtractor,
                            EuclideanClusterResult, GpuEuclideanClusterExtractor)
+from .streaming import (MemoryChunkSource, SpoolOptions, StreamingVoxelConfig,
+                        StreamingVoxelSource)
+from .las import LasChunkSource, LasReader, read_las
+from . import gpu
 
 __all__ = [
     "Auto", "AttributeAggregation", "BufferLengthMismatch", "CpuParallel", "CpuSingle",
@@ -26,4 +32,6 @@ __all__ = [
     "TransferDirection", "UnsupportedDType", "VoxelAggregationMode", "VoxelGridDownsample",
     "VoxelGridDownsampleConfig", "build_output_cloud", "EuclideanClusterConfig",
     "EuclideanClusterExtractor", "EuclideanClusterResult", "GpuEuclideanClusterExtractor",
+    "MemoryChunkSource", "SpoolOptions", "StreamingVoxelConfig", "StreamingVoxelSource",
+    "LasChunkSource", "LasReader", "read_las", "gpu",
 ]

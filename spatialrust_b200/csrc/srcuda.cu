@@ -57,6 +57,8 @@ struct srcu_ctx {
   DevBuf parent;  // union-find parents (Euclidean clustering)
   DevBuf cov6;    // plane-regularised covariances, 6 floats per point
   DevBuf stage_block;  // host interleaved records, copied once before deinterleaving
+  // the buffers of the last destroyed streaming voxel, kept for the next one
+  srcu_stream_voxel *parked_stream = nullptr;
   uint32_t last_attrs = 0;  // attribute count of the last enqueued chain
   const float *frame_attr_ptrs[MAX_COLS] = {};
   // batch arrays (clouds of the last chain) and pinned staging for their parameters
@@ -77,6 +79,9 @@ struct srcu_ctx {
   std::vector<cudaEvent_t> ev_pool;     // 2 per pending region
   std::vector<int> ev_pending;          // kernel id per pending region
 };
+
+// Frees a streaming voxel and its buffers (stream.cu).
+void stream_voxel_free(srcu_stream_voxel *sv);
 
 namespace {
 
@@ -739,6 +744,8 @@ void srcu_destroy(srcu_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  stream_voxel_free(ctx->parked_stream);
+  ctx->parked_stream = nullptr;
   DevBuf *all[] = {&ctx->in_aos, &ctx->vaos, &ctx->keys[0], &ctx->keys[1], &ctx->vals[0], &ctx->vals[1], &ctx->lb_sort,
                    &ctx->lb_seg, &ctx->lb_cells, &ctx->vkeys, &ctx->vcounts, &ctx->vkeys3,
                    &ctx->pts, &ctx->pt_cell, &ctx->cell_key, &ctx->cell_start, &ctx->table, &ctx->ranges,

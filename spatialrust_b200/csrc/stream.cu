@@ -57,7 +57,7 @@ srcu_status grow_keep(srcu_ctx *ctx, DevBuf &b, size_t bytes, size_t keep) {
 srcu_status sv_reserve_records(srcu_stream_voxel *sv, uint64_t need) {
   if (need <= sv->rec_cap) return SRCU_OK;
   srcu_ctx *ctx = sv->ctx;
-  const uint64_t cap = std::max<uint64_t>(need, sv->rec_cap + sv->rec_cap / 2);
+  const uint64_t cap = std::max<uint64_t>({need, 2 * sv->rec_cap, 4 * sv->dev_run});
   const size_t keep = size_t(sv->records) * 8;
   for (int a = 0; a < 3; ++a) ST_TRY(grow_keep(ctx, sv->rk[a], cap * 8, keep));
   ST_TRY(grow_keep(ctx, sv->rcnt, cap * 8, keep));
@@ -271,11 +271,18 @@ srcu_status srcu_stream_voxel_create(srcu_ctx *ctx, const srcu_stream_voxel_para
     return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "at most %d attribute columns are supported",
                 MAX_COLS - 3);
   CU_TRY(cudaSetDevice(ctx->device));
-  srcu_stream_voxel *sv = new srcu_stream_voxel();
+  // Reuse the buffers of the context's last stream: a new stream then
+  // allocates nothing until it outgrows them.
+  srcu_stream_voxel *sv = ctx->parked_stream;
+  ctx->parked_stream = nullptr;
+  if (!sv) sv = new srcu_stream_voxel();
   sv->ctx = ctx;
   sv->prm = *params;
   sv->nc = 3 + params->n_attrs;
   sv->leaf = double(params->leaf_size);
+  sv->fill = sv->points = sv->device_runs = sv->records = sv->voxels = 0;
+  sv->rec_cap = 0;  // re-derived from the kept buffers' sizes as records arrive
+  sv->finished = false;
   // By default a device run holds at least 2^20 points whatever run_points
   // is: the run size only partitions the sums, the voxels do not depend on it.
   sv->dev_run = params->device_run_points
@@ -283,7 +290,7 @@ srcu_status srcu_stream_voxel_create(srcu_ctx *ctx, const srcu_stream_voxel_para
                     : std::max<uint64_t>(params->run_points, uint64_t(1) << 20);
   sv->dev_run = std::min<uint64_t>(sv->dev_run, uint64_t(1) << 26);
   auto bail = [&](srcu_status st) {
-    srcu_stream_voxel_destroy(sv);
+    stream_voxel_free(sv);
     return st;
   };
   if (cudaFuncSetAttribute(k_sort<StreamPointSrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -303,7 +310,8 @@ srcu_status srcu_stream_voxel_create(srcu_ctx *ctx, const srcu_stream_voxel_para
   if (s == SRCU_OK) s = ensure(ctx, sv->plan, sizeof(StreamPlan));
   if (s == SRCU_OK) s = ensure(ctx, sv->state, sizeof(StreamState));
   if (s != SRCU_OK) return bail(s);
-  if (cudaMallocHost(reinterpret_cast<void **>(&sv->state_host), sizeof(StreamState)) != cudaSuccess)
+  if (!sv->state_host &&
+      cudaMallocHost(reinterpret_cast<void **>(&sv->state_host), sizeof(StreamState)) != cudaSuccess)
     return bail(fail(ctx, SRCU_ERR_CUDA, "cannot allocate pinned stream state"));
   StreamState init{};
   for (int a = 0; a < 3; ++a) {
@@ -400,11 +408,21 @@ srcu_status srcu_stream_voxel_fetch(srcu_stream_voxel *sv, uint64_t first, uint6
 
 void srcu_stream_voxel_destroy(srcu_stream_voxel *sv) {
   if (!sv) return;
-  cudaSetDevice(sv->ctx->device);
-  cudaStreamSynchronize(sv->ctx->stream);
+  srcu_ctx *ctx = sv->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (!ctx->parked_stream) {  // kept for the context's next stream
+    ctx->parked_stream = sv;
+    return;
+  }
+  stream_voxel_free(sv);
+}
+
+}  // extern "C"
+
+void stream_voxel_free(srcu_stream_voxel *sv) {
+  if (!sv) return;
   sv_release(sv);
   if (sv->state_host) cudaFreeHost(sv->state_host);
   delete sv;
 }
-
-}  // extern "C"
