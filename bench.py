@@ -433,6 +433,8 @@ def run_gpu(args):
                     peak_source="MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
                     else "fallback 6650 GB/s",
                     algorithmic_bytes_per_launch=dom_bytes, avg_launch_ms=avg_launch_ms,
+                    isolated_split_ms={g: round(ms / 3, 4) for g, ms in
+                                       sorted(group_ms.items(), key=lambda kv: -kv[1]) if ms > 0},
                     timing=("CUDA events around each launch of the group in the timed region, "
                             "where the two leaf chains share the GPU" if not args.serial_leaves
                             else "CUDA events around each launch of the group in the timed region"),
