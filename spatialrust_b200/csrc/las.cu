@@ -49,7 +49,8 @@ srcu_status srcu_las_decode(srcu_ctx *ctx, const void *records, uint64_t n, int3
   LasDecodeDev d{};
   d.n = n;
   d.record_len = rl;
-  d.per_tile = std::min<uint32_t>(LAS_THREADS, LAS_SMEM_MAX / rl);
+  d.per_tile = std::min<uint32_t>(LAS_TILE_RECORDS, LAS_BUF_MAX / rl);
+  d.buf_bytes = (d.per_tile * rl + 32 + 15) & ~15u;
   const bool extended = fmt->point_format >= 6;
   d.class_off = extended ? 16 : 15;
   d.class_mask = extended ? 0xffu : 0x1fu;
@@ -82,13 +83,25 @@ srcu_status srcu_las_decode(srcu_ctx *ctx, const void *records, uint64_t n, int3
   o.gps = static_cast<double *>(dev[5]);
   for (int c = 0; c < 3; ++c) o.rgb[c] = static_cast<uint16_t *>(dev[6 + c]);
   const uint64_t tiles = (n + d.per_tile - 1) / d.per_tile;
-  const uint32_t grid = uint32_t(std::min<uint64_t>(tiles, uint64_t(ctx->num_sms) * 8));
-  const size_t smem = size_t(d.per_tile) * rl + 32;
+  const size_t smem = 2 * size_t(d.buf_bytes);  // two tile buffers
+  CU_TRY(cudaFuncSetAttribute(k_las_decode, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(2 * (LAS_BUF_MAX + 48))));
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_las_decode, LAS_THREADS, smem);
+  const uint32_t grid = uint32_t(std::min<uint64_t>(
+      tiles, uint64_t(ctx->num_sms) * uint64_t(std::max(per_sm, 1))));
+  uint32_t *status = &ctx->ctl->status;
+  CU_TRY(cudaMemsetAsync(status, 0, sizeof(uint32_t), ctx->stream));
   {
     Launch l(ctx, SRCU_K_LAS_DECODE);
-    k_las_decode<<<grid, LAS_THREADS, smem, ctx->stream>>>(src, d, o);
+    k_las_decode<<<grid, LAS_THREADS, smem, ctx->stream>>>(src, d, o, status);
   }
   CU_TRY(cudaGetLastError());
+  CU_TRY(cudaMemcpyAsync(&ctx->ctl_host->status, status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                         ctx->stream));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  if (ctx->ctl_host->status & ST_TIMEOUT)
+    return fail(ctx, SRCU_ERR_TIMEOUT, "a bounded wait for a LAS record copy gave up");
   if (!out->on_device)
     for (int c = 0; c < 9; ++c)
       if (dst[c]) ST_TRY(copy_out(ctx, dst[c], dev[c], n * elem[c], 0));
