@@ -240,7 +240,7 @@ typedef struct srcu_stream_voxel_params {
   float leaf_size;          /* > 0 and finite (StreamingVoxelConfig::new, streaming.rs:345-363) */
   uint32_t n_attrs;         /* attribute columns in every chunk */
   uint32_t attr_f64_mask;   /* bit a: attrs[a] of every chunk points at f64 data, not f32 */
-  uint32_t device_run_points; /* points sorted per device run; 0: max(run_points, 2^20) */
+  uint32_t device_run_points; /* points sorted per device run; 0: max(run_points, 2^22) */
   uint64_t run_points;      /* > 0: finite points per run of the reference's run limit */
   uint64_t max_runs;        /* > 0: more runs than this fail, as flush_run does (:742-746) */
   uint64_t spool_limit_bytes; /* 0: none; else the reference's spool extent rule: runs * 8 +

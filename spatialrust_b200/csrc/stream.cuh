@@ -106,12 +106,14 @@ __device__ __forceinline__ bool finite3(float x, float y, float z) {
 }
 
 // Per-axis min/max over the points whose three coordinates are finite (the
-// points the stream keeps) of the current run (ctl->n_points of them).
+// points the stream keeps) of the current run (ctl->n_points of them):
+// warp then block reductions, six atomics per block.
 __global__ void __launch_bounds__(256) k_stream_bounds(Control *ctl, const float *x, const float *y,
                                                        const float *z, Bounds *out) {
+  __shared__ uint32_t red[6][8];
   if (ld_relaxed_u32(&ctl->status)) return;
   const uint64_t n = ctl->n_points;
-  uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
+  uint32_t v6[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};  // mn xyz, mx xyz
   for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n;
        i += uint64_t(gridDim.x) * blockDim.x) {
     const float v[3] = {x[i], y[i], z[i]};
@@ -119,20 +121,31 @@ __global__ void __launch_bounds__(256) k_stream_bounds(Control *ctl, const float
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const uint32_t o = f2ord(v[a]);
-      mn[a] = min(mn[a], o);
-      mx[a] = max(mx[a], o);
+      v6[a] = min(v6[a], o);
+      v6[3 + a] = max(v6[3 + a], o);
     }
   }
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    mn[a] = __reduce_min_sync(FULL_MASK, mn[a]);
-    mx[a] = __reduce_max_sync(FULL_MASK, mx[a]);
+    v6[a] = __reduce_min_sync(FULL_MASK, v6[a]);
+    v6[3 + a] = __reduce_max_sync(FULL_MASK, v6[3 + a]);
   }
-  if ((threadIdx.x & 31u) == 0) {
-#pragma unroll
+  if (lane == 0)
+    for (int k = 0; k < 6; ++k) red[k][warp] = v6[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t warps = blockDim.x >> 5;
     for (int a = 0; a < 3; ++a) {
-      if (mn[a] != 0xffffffffu) atomicMin(&out->mn[a], mn[a]);
-      if (mn[a] != 0xffffffffu) atomicMax(&out->mx[a], mx[a]);
+      uint32_t mn = red[a][0], mx = red[3 + a][0];
+      for (uint32_t w = 1; w < warps; ++w) {
+        mn = min(mn, red[a][w]);
+        mx = max(mx, red[3 + a][w]);
+      }
+      if (mn != 0xffffffffu) {
+        atomicMin(&out->mn[a], mn);
+        atomicMax(&out->mx[a], mx);
+      }
     }
   }
 }
