@@ -223,6 +223,54 @@ srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
 srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float radius,
                                    float epsilon, float *cov, srcu_normal_stats *stats);
 
+/* ---- RANSAC plane segmentation ------------------------------------------- */
+
+/* GpuPlaneScore (crates/spatialrust-gpu/src/kernels/ransac_plane.rs:27-37). */
+typedef struct srcu_plane_score {
+  uint32_t inlier_count;
+  float normal[3];
+  float d;
+} srcu_plane_score;
+
+/* RansacPlaneConfig (crates/spatialrust-segmentation/src/plane.rs:55-93). */
+typedef struct srcu_ransac_params {
+  float distance_threshold; /* default 0.01 */
+  uint32_t max_iterations;  /* default 1000 (at most 2^26) */
+  uint64_t min_inliers;     /* default 3 */
+  uint64_t seed;            /* default 42 */
+} srcu_ransac_params;
+
+typedef struct srcu_ransac_result {
+  float normal[3];            /* the model: refined from the inliers (>= 3), else the hypothesis */
+  float d;
+  uint64_t inlier_count;
+  uint32_t hypotheses;        /* hypotheses scored */
+  uint32_t best_hypothesis;   /* index of the winning hypothesis (UINT32_MAX: none) */
+  float hypothesis_normal[3]; /* its plane, before refinement */
+  float hypothesis_d;
+} srcu_ransac_result;
+
+/* Replaces score_ransac_plane_hypotheses_gpu (ransac_plane.rs:104-263): the
+ * plane of each hypothesis (3 point indices, host memory) and its inlier count
+ * with the CPU path's f32 arithmetic (plane_ransac.rs:54-94, plane.rs:39-41);
+ * a degenerate triple scores all zeros.  scores: count entries, host memory.
+ * Synchronous. */
+srcu_status srcu_ransac_plane_scores(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                     const uint32_t *hypotheses, uint32_t count,
+                                     float distance_threshold, srcu_plane_score *scores);
+
+/* The Gpu(Cuda) arm of RansacPlaneSegmenter::segment_with_policy (plane.rs:
+ * 151-264, rejected today at plane.rs:259-261) with the CPU segmenter's
+ * results (plane.rs:266-345): the reference's seeded hypotheses, all scored on
+ * the device, the first hypothesis with the most inliers, its inlier mask
+ * (inlier_mask: n bytes, nullable, host or device memory as cloud->on_device)
+ * and the model refined from the inliers in FP64.  Fails as the reference does
+ * for empty clouds, fewer than 3 points and fewer than min_inliers inliers.
+ * Synchronous. */
+srcu_status srcu_ransac_plane_segment(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                      const srcu_ransac_params *params, srcu_ransac_result *result,
+                                      uint8_t *inlier_mask);
+
 /* ---- bounded streaming voxel centroids ------------------------------------ */
 
 /* Replaces StreamingVoxelSource (crates/spatialrust-pipeline/src/streaming.rs:
@@ -477,6 +525,7 @@ typedef enum srcu_kernel_id {
   SRCU_K_NORMALS,        /* radius neighbours + covariance + eigensolve */
   SRCU_K_CLUSTER,        /* Euclidean clustering: union-find over the radius grid */
   SRCU_K_LAS_DECODE,     /* LAS point records -> columns */
+  SRCU_K_RANSAC,         /* RANSAC plane hypotheses, scores, inlier mask and moments */
   SRCU_K_COUNT
 } srcu_kernel_id;
 

@@ -71,6 +71,9 @@ def _load():
     lib.oracle_las_decode.argtypes = [P, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, P, P,
                                       ctypes.c_int, P, P, P, P, P, P, P, P]
     lib.oracle_las_decode.restype = ctypes.c_int
+    lib.oracle_ransac_plane.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float, ctypes.c_uint32,
+                                        ctypes.c_uint64, ctypes.c_uint64, P, P, P, P]
+    lib.oracle_ransac_plane.restype = ctypes.c_longlong
     lib.oracle_brute_radius_counts.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float, P]
     lib.oracle_brute_radius_counts.restype = None
     lib.oracle_compute_bounds.argtypes = [P, P, P, ctypes.c_size_t, P, P]
@@ -327,6 +330,33 @@ def las_decode(records, point_format, record_length, scale, offset, origin=None)
     out = {k: v[:n] for k, v in out.items()}
     out["red"], out["green"], out["blue"] = rgb[:n], rgb[n:2 * n], rgb[2 * n:3 * n]
     return out
+
+
+def ransac_plane(x, y, z, distance_threshold=0.01, max_iterations=1000, min_inliers=3,
+                 seed=42) -> dict:
+    """RansacPlaneSegmenter::segment_cpu + finalize_plane_segmentation
+    (plane.rs:266-345): model (refined), hypothesis model, best hypothesis
+    index, inlier count and mask."""
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    n = x.shape[0]
+    model = np.zeros(4, np.float32)
+    hyp = np.zeros(4, np.float32)
+    best = np.zeros(1, np.uint32)
+    mask = np.zeros(max(n, 1), np.uint8)
+    rc = lib.oracle_ransac_plane(_ptr(x), _ptr(y), _ptr(z), n, ctypes.c_float(distance_threshold),
+                                 int(max_iterations), int(min_inliers), int(seed), _ptr(model),
+                                 _ptr(hyp), _ptr(best), _ptr(mask))
+    if rc == -1:
+        raise OracleError("cannot segment plane from empty point cloud")
+    if rc == -2:
+        raise OracleError("plane segmentation requires at least three points")
+    if rc == -5:
+        raise OracleError("RANSAC found fewer inliers than min_inliers")
+    if rc == -6:
+        raise OracleError("failed to refine plane model")
+    return dict(model=model, hypothesis=hyp, best_index=int(best[0]), inlier_count=int(rc),
+                mask=mask[:n].astype(bool))
 
 
 def brute_radius_counts(x, y, z, radius) -> np.ndarray:

@@ -1546,6 +1546,139 @@ int oracle_las_decode(const uint8_t *rec, size_t n, int format, int record_lengt
   return OR_OK;
 }
 
+/* ------------------------------------------------------------------------ */
+/* RANSAC plane segmentation (crates/spatialrust-segmentation/src/plane.rs,  */
+/* plane_ransac.rs)                                                          */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  uint64_t state;
+} or_rng;
+
+/* Rng (plane_ransac.rs:7-25) */
+static uint64_t or_rng_next(or_rng *r) {
+  r->state = r->state * 6364136223846793005ull + 1ull;
+  return r->state;
+}
+static uint64_t or_rng_index(or_rng *r, uint64_t upper) {
+  return ((or_rng_next(r) >> 32) * upper) >> 32;
+}
+
+/* plane_from_points (plane_ransac.rs:79-89), f32; returns 0 for None. */
+static int or_plane(const float *x, const float *y, const float *z, const uint32_t idx[3],
+                    float plane[4]) {
+  const float p0x = x[idx[0]], p0y = y[idx[0]], p0z = z[idx[0]];
+  const float v1x = x[idx[1]] - p0x, v1y = y[idx[1]] - p0y, v1z = z[idx[1]] - p0z;
+  const float v2x = x[idx[2]] - p0x, v2y = y[idx[2]] - p0y, v2z = z[idx[2]] - p0z;
+  float nx = v1y * v2z - v1z * v2y;
+  float ny = v1z * v2x - v1x * v2z;
+  float nz = v1x * v2y - v1y * v2x;
+  const float ls = nx * nx + ny * ny + nz * nz;
+  if (ls < 1e-12f) return 0;
+  const float len = sqrtf(ls);
+  if (len != 0.0f) {
+    nx = nx / len;
+    ny = ny / len;
+    nz = nz / len;
+  }
+  plane[0] = nx;
+  plane[1] = ny;
+  plane[2] = nz;
+  plane[3] = -(nx * p0x + ny * p0y + nz * p0z);
+  return 1;
+}
+
+/* distance_xyz (plane.rs:39-41) <= threshold */
+static int or_inlier(const float p[4], float x, float y, float z, float thr) {
+  return fabsf(p[0] * x + p[1] * y + p[2] * z + p[3]) <= thr;
+}
+
+/*
+ * RansacPlaneSegmenter::segment_cpu + finalize_plane_segmentation
+ * (plane.rs:266-345): hypotheses from the seeded LCG (sample_indices,
+ * plane_ransac.rs:27-43), the first plane with the most inliers, then
+ * refine_plane_from_inliers (plane_ransac.rs:96-150: FP64 sequential means and
+ * covariance, symmetric_eigen3, f32 normal normalized, d = -n.c).  Returns the
+ * inlier count (mask: n bytes) and writes the model, or -1 (empty), -2 (< 3
+ * points), -5 (fewer than min_inliers), -6 (no model).
+ */
+long long oracle_ransac_plane(const float *x, const float *y, const float *z, size_t n, float thr,
+                              uint32_t max_iterations, uint64_t min_inliers, uint64_t seed,
+                              float model[4], float hyp_model[4], uint32_t *best_index,
+                              uint8_t *mask) {
+  if (n == 0) return -1;
+  if (n < 3) return -2;
+  or_rng rng = {seed ? seed : 1};
+  long long best = 0;
+  int have = 0;
+  *best_index = UINT32_MAX;
+  for (uint32_t it = 0; it < max_iterations; ++it) {
+    uint32_t idx[3];
+    idx[0] = (uint32_t)or_rng_index(&rng, n);
+    idx[1] = (uint32_t)or_rng_index(&rng, n);
+    while (idx[1] == idx[0]) idx[1] = (uint32_t)or_rng_index(&rng, n);
+    idx[2] = (uint32_t)or_rng_index(&rng, n);
+    while (idx[2] == idx[0] || idx[2] == idx[1]) idx[2] = (uint32_t)or_rng_index(&rng, n);
+    float pl[4];
+    if (!or_plane(x, y, z, idx, pl)) continue;
+    long long c = 0;
+    for (size_t i = 0; i < n; ++i) c += or_inlier(pl, x[i], y[i], z[i], thr);
+    if (c > best) {
+      best = c;
+      have = 1;
+      memcpy(hyp_model, pl, sizeof(pl));
+      *best_index = it;
+    }
+  }
+  if ((uint64_t)best < min_inliers) return -5;
+  if (!have) return -6;
+  double mx = 0, my = 0, mz = 0;
+  for (size_t i = 0; i < n; ++i) {
+    mask[i] = (uint8_t)or_inlier(hyp_model, x[i], y[i], z[i], thr);
+    if (mask[i]) {
+      mx += (double)x[i];
+      my += (double)y[i];
+      mz += (double)z[i];
+    }
+  }
+  memcpy(model, hyp_model, 4 * sizeof(float));
+  if (best < 3) return best;
+  const double cnt = (double)best;
+  mx /= cnt;
+  my /= cnt;
+  mz /= cnt;
+  double c[6] = {0, 0, 0, 0, 0, 0};
+  for (size_t i = 0; i < n; ++i) {
+    if (!mask[i]) continue;
+    const double dx = (double)x[i] - mx, dy = (double)y[i] - my, dz = (double)z[i] - mz;
+    c[0] += dx * dx;
+    c[1] += dy * dy;
+    c[2] += dz * dz;
+    c[3] += dx * dy;
+    c[4] += dx * dz;
+    c[5] += dy * dz;
+  }
+  const double inv = 1.0 / cnt;
+  const double cov[3][3] = {{c[0] * inv, c[3] * inv, c[4] * inv},
+                            {c[3] * inv, c[1] * inv, c[5] * inv},
+                            {c[4] * inv, c[5] * inv, c[2] * inv}};
+  double vals[3], vecs[3][3];
+  rs_symmetric_eigen3(cov, vals, vecs, 32, 1e-12);
+  float nx = (float)vecs[0][0], ny = (float)vecs[1][0], nz = (float)vecs[2][0];
+  const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+  if (len != 0.0f) {
+    nx = nx / len;
+    ny = ny / len;
+    nz = nz / len;
+  }
+  const float cx = (float)mx, cy = (float)my, cz = (float)mz;
+  model[0] = nx;
+  model[1] = ny;
+  model[2] = nz;
+  model[3] = -(nx * cx + ny * cy + nz * cz);
+  return best;
+}
+
 /* Exposes the f32 closed-form smallest eigenpair for unit tests. */
 void oracle_smallest_eigenpair_f32(const float c[6], float normal[3], float *curv) {
   rs_smallest_eigenpair(c[0], c[1], c[2], c[3], c[4], c[5], normal, curv);

@@ -17,10 +17,13 @@ from .features import (GpuNormalEstimator, NormalEstimationConfig, NormalEstimat
 from .filtering import (AttributeAggregation, VoxelAggregationMode, VoxelGridDownsample,
                         VoxelGridDownsampleConfig)
 from .segmentation import (EuclideanClusterConfig, EuclideanClusterExtractor,
-                           EuclideanClusterResult, GpuEuclideanClusterExtractor)
+                           EuclideanClusterResult, GpuEuclideanClusterExtractor,
+                           GpuRansacPlaneSegmenter, PlaneModel, RansacPlaneConfig,
+                           RansacPlaneSegmentation, RansacPlaneSegmenter)
 from .streaming import (MemoryChunkSource, SpoolOptions, StreamingVoxelConfig,
                         StreamingVoxelSource)
 from .las import LasChunkSource, LasReader, read_las
+from .pipeline import MvpPipeline, MvpPipelineConfig, MvpPipelineReceipt, MvpPipelineResult
 from . import gpu
 
 __all__ = [
@@ -33,5 +36,7 @@ __all__ = [
     "VoxelGridDownsampleConfig", "build_output_cloud", "EuclideanClusterConfig",
     "EuclideanClusterExtractor", "EuclideanClusterResult", "GpuEuclideanClusterExtractor",
     "MemoryChunkSource", "SpoolOptions", "StreamingVoxelConfig", "StreamingVoxelSource",
-    "LasChunkSource", "LasReader", "read_las", "gpu",
+    "LasChunkSource", "LasReader", "read_las", "gpu", "GpuRansacPlaneSegmenter", "PlaneModel",
+    "RansacPlaneConfig", "RansacPlaneSegmentation", "RansacPlaneSegmenter", "MvpPipeline",
+    "MvpPipelineConfig", "MvpPipelineReceipt", "MvpPipelineResult",
 ]

@@ -189,9 +189,26 @@ class SrcuLasOut(ctypes.Structure):
                 ("on_device", ctypes.c_int32)]
 
 
+class SrcuPlaneScore(ctypes.Structure):
+    _fields_ = [("inlier_count", ctypes.c_uint32), ("normal", ctypes.c_float * 3),
+                ("d", ctypes.c_float)]
+
+
+class SrcuRansacParams(ctypes.Structure):
+    _fields_ = [("distance_threshold", ctypes.c_float), ("max_iterations", ctypes.c_uint32),
+                ("min_inliers", ctypes.c_uint64), ("seed", ctypes.c_uint64)]
+
+
+class SrcuRansacResult(ctypes.Structure):
+    _fields_ = [("normal", ctypes.c_float * 3), ("d", ctypes.c_float),
+                ("inlier_count", ctypes.c_uint64), ("hypotheses", ctypes.c_uint32),
+                ("best_hypothesis", ctypes.c_uint32), ("hypothesis_normal", ctypes.c_float * 3),
+                ("hypothesis_d", ctypes.c_float)]
+
+
 KERNEL_IDS = ["begin", "bounds", "voxel_plan", "voxel_hist", "voxel_sort", "voxel_segments",
               "unpack_keys", "cell_plan", "cell_hist", "cell_sort", "cells", "hash", "ranges",
-              "normals", "cluster", "las_decode"]
+              "normals", "cluster", "las_decode", "ransac"]
 
 
 # Every symbol include/srcuda.h declares, with its ctypes signature.
@@ -250,6 +267,10 @@ SIGNATURES = {
     "srcu_stream_voxel_fetch": ([_P, ctypes.c_uint64, ctypes.c_uint64,
                                  ctypes.POINTER(SrcuStreamVoxelOut)], ctypes.c_int),
     "srcu_stream_voxel_destroy": ([_P], None),
+    "srcu_ransac_plane_scores": ([_P, ctypes.POINTER(SrcuCloud), ctypes.c_void_p, ctypes.c_uint32,
+                                  ctypes.c_float, ctypes.POINTER(SrcuPlaneScore)], ctypes.c_int),
+    "srcu_ransac_plane_segment": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuRansacParams),
+                                   ctypes.POINTER(SrcuRansacResult), ctypes.c_void_p], ctypes.c_int),
     "srcu_las_decode": ([_P, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32,
                          ctypes.POINTER(SrcuLasFormat), ctypes.POINTER(SrcuLasOut)], ctypes.c_int),
     "srcu_server_create": ([ctypes.POINTER(SrcuServerConfig), ctypes.POINTER(ctypes.c_void_p)],
@@ -503,6 +524,44 @@ class Context:
         self._check(self._lib.srcu_euclidean_cluster_roots(self._h, ctypes.byref(cloud),
                                                            ctypes.c_float(cluster_tolerance), addr))
         return roots[:n]
+
+    def ransac_plane_segment(self, x, y, z, distance_threshold: float = 0.01,
+                             max_iterations: int = 1000, min_inliers: int = 3, seed: int = 42):
+        """(result dict, inlier mask): the CPU segmenter's answer, scored on the
+        device.  The mask is a numpy bool array (a CUDA uint8 tensor for
+        device inputs)."""
+        keep = _Keep()
+        cloud = make_cloud(x, y, z, (), keep)
+        n = int(cloud.n)
+        if cloud.on_device:
+            import torch
+            mask = torch.empty(max(n, 1), dtype=torch.uint8, device=torch.device("cuda", self.device))
+            addr = mask.data_ptr()
+        else:
+            mask = np.empty(max(n, 1), np.uint8)
+            addr = mask.ctypes.data
+        prm = SrcuRansacParams(ctypes.c_float(distance_threshold), int(max_iterations),
+                               int(min_inliers), int(seed))
+        res = SrcuRansacResult()
+        self._check(self._lib.srcu_ransac_plane_segment(self._h, ctypes.byref(cloud),
+                                                        ctypes.byref(prm), ctypes.byref(res), addr))
+        out = dict(normal=tuple(res.normal), d=float(res.d), inlier_count=int(res.inlier_count),
+                   hypotheses=int(res.hypotheses), best_hypothesis=int(res.best_hypothesis),
+                   hypothesis_normal=tuple(res.hypothesis_normal),
+                   hypothesis_d=float(res.hypothesis_d))
+        mask = mask[:n]
+        return out, (mask if cloud.on_device else mask.astype(bool))
+
+    def ransac_plane_scores(self, x, y, z, hypotheses, distance_threshold: float):
+        """[(inlier_count, (nx, ny, nz), d)] per hypothesis (triples of point indices)."""
+        keep = _Keep()
+        cloud = make_cloud(x, y, z, (), keep)
+        hyp = np.ascontiguousarray(hypotheses, np.uint32).reshape(-1, 3)
+        scores = (SrcuPlaneScore * max(len(hyp), 1))()
+        self._check(self._lib.srcu_ransac_plane_scores(self._h, ctypes.byref(cloud), hyp.ctypes.data,
+                                                       len(hyp), ctypes.c_float(distance_threshold),
+                                                       scores))
+        return [(int(s.inlier_count), tuple(s.normal), float(s.d)) for s in scores[:len(hyp)]]
 
     def plane_covariances(self, x, y, z, radius: float, epsilon: float, with_stats: bool = False):
         """(n, 6) plane-regularised covariances [c00, c11, c22, c01, c02, c12]

@@ -59,6 +59,8 @@ struct srcu_ctx {
   DevBuf stage_block;  // host interleaved records, copied once before deinterleaving
   // the buffers of the last destroyed streaming voxel, kept for the next one
   srcu_stream_voxel *parked_stream = nullptr;
+  // RANSAC plane scoring: hypotheses, planes, validity, counts, block partials, mask
+  DevBuf rs_hyp, rs_planes, rs_valid, rs_counts, rs_partials, rs_mask;
   uint32_t last_attrs = 0;  // attribute count of the last enqueued chain
   const float *frame_attr_ptrs[MAX_COLS] = {};
   // batch arrays (clouds of the last chain) and pinned staging for their parameters
@@ -161,7 +163,8 @@ const char *const kKernelNames[SRCU_K_COUNT] = {
     "k_begin",          "k_bounds",        "k_voxel_plan",  "(in k_sort<voxel>)",
     "k_sort<voxel>",    "k_voxel_segments", "k_unpack_voxel_keys", "k_cell_plan",
     "(in k_sort<cell>)", "k_sort<cell>",    "k_cells",       "k_column_insert",
-    "k_ranges",         "k_normals",       "k_cluster_union", "k_las_decode"};
+    "k_ranges",         "k_normals",       "k_cluster_union", "k_las_decode",
+    "k_ransac_score"};
 
 // Counts the launches of one kernel group and, when its bit is set in
 // prof_mask, brackets them with CUDA events on the context stream.
@@ -749,7 +752,9 @@ void srcu_destroy(srcu_ctx *ctx) {
   DevBuf *all[] = {&ctx->in_aos, &ctx->vaos, &ctx->keys[0], &ctx->keys[1], &ctx->vals[0], &ctx->vals[1], &ctx->lb_sort,
                    &ctx->lb_seg, &ctx->lb_cells, &ctx->vkeys, &ctx->vcounts, &ctx->vkeys3,
                    &ctx->pts, &ctx->pt_cell, &ctx->cell_key, &ctx->cell_start, &ctx->table, &ctx->ranges,
-                   &ctx->ncounts, &ctx->parent, &ctx->cov6, &ctx->stage_block};
+                   &ctx->ncounts, &ctx->parent, &ctx->cov6, &ctx->stage_block,
+                   &ctx->rs_hyp, &ctx->rs_planes, &ctx->rs_valid, &ctx->rs_counts,
+                   &ctx->rs_partials, &ctx->rs_mask};
   for (DevBuf *b : all) release(ctx, *b);
   for (auto &b : ctx->in) release(ctx, b);
   for (auto &b : ctx->vout) release(ctx, b);
@@ -1270,3 +1275,4 @@ int srcu_profile_read(srcu_ctx *ctx, srcu_kernel_stat *out, int max_entries, int
 // So do the bounded streaming voxel and the LAS record decoder.
 #include "stream.cu"
 #include "las.cu"
+#include "ransac.cu"

@@ -4,6 +4,7 @@ on the CUDA library (crates/spatialrust-gpu/src/lib.rs:38-54 exports them).
     estimate_normals_grid_gpu            kernels/normals_grid.rs:208-350
     euclidean_cluster_roots_gpu          kernels/euclidean_cluster.rs:62-71
     estimate_plane_covariances_grid_gpu  kernels/covariances_grid.rs:216-364
+    score_ransac_plane_hypotheses_gpu    kernels/ransac_plane.rs:104-263
 
 The reference takes a &WgpuRuntime first; here the device index is a
 keyword argument and the process-wide context of that device plays the
@@ -51,3 +52,14 @@ def estimate_plane_covariances_grid_gpu(x, y, z, radius: float, epsilon: float,
     if _len(x) and not radius > 0.0:  # covariances_grid.rs:228-233: empty input first
         raise InvalidArgument("grid radius must be positive")
     return _native.shared_context(device).plane_covariances(x, y, z, radius, epsilon)
+
+
+def score_ransac_plane_hypotheses_gpu(x, y, z, hypotheses, distance_threshold: float,
+                                      device: int = 0):
+    """[(inlier_count, (nx, ny, nz), d)] per hypothesis (GpuPlaneScore,
+    ransac_plane.rs:27-37): the plane through the three indexed points and its
+    inliers, in the CPU path's f32 arithmetic; a degenerate triple scores zeros."""
+    hyp = np.asarray(hypotheses, np.uint32).reshape(-1, 3)
+    if len(hyp) == 0:  # ransac_plane.rs:124-126
+        return []
+    return _native.shared_context(device).ransac_plane_scores(x, y, z, hyp, distance_threshold)

@@ -355,3 +355,31 @@ def test_stream_voxel_compensated_sum_beats_plain_sum():
     a[0] = 1.0
     r = oracle.stream_voxel(x, np.zeros_like(x), np.zeros_like(x), attrs=[a], leaf=1.0)
     assert r.attrs[0, 0] == (1.0 + 1e-13) / 1001
+
+
+# ---- RANSAC plane (crates/spatialrust-segmentation/src/plane.rs) ------------
+
+def plane_with_outliers():
+    pts = [[x, y, 0.0] for x in range(10) for y in range(10)] + [[0, 0, 5], [1, 1, 5]]
+    return np.array(pts, F)
+
+
+def test_ransac_segments_dominant_plane():
+    # plane.rs:372-386 (threshold 0.05, 500 iterations, min 50 inliers, seed 7)
+    p = plane_with_outliers()
+    r = oracle.ransac_plane(p[:, 0], p[:, 1], p[:, 2], 0.05, 500, 50, 7)
+    assert r["inlier_count"] == 100
+    assert int((~r["mask"]).sum()) == 2
+    assert abs(r["model"][2]) > 0.9
+    # extract_outliers_removes_plane (plane.rs:394-406)
+    assert np.all(p[~r["mask"], 2] > 1.0)
+
+
+def test_ransac_errors_follow_the_reference():
+    with pytest.raises(oracle.OracleError):
+        oracle.ransac_plane([], [], [], 0.05, 10, 3, 1)
+    with pytest.raises(oracle.OracleError):
+        oracle.ransac_plane([0, 1], [0, 0], [0, 0], 0.05, 10, 1, 1)
+    p = plane_with_outliers()
+    with pytest.raises(oracle.OracleError):  # min_inliers above the plane's 100
+        oracle.ransac_plane(p[:, 0], p[:, 1], p[:, 2], 0.05, 50, 101, 7)
