@@ -75,6 +75,8 @@ def parse():
                     help="skip the Euclidean cluster-roots measurement")
     ap.add_argument("--no-plane-cov", action="store_true",
                     help="skip the GICP plane-covariance leg")
+    ap.add_argument("--no-ransac", action="store_true",
+                    help="skip the RANSAC plane leg")
     ap.add_argument("--no-las-stream", action="store_true",
                     help="skip the LAS ingest -> streaming voxel leg")
     ap.add_argument("--no-serving", action="store_true",
@@ -466,6 +468,8 @@ def run_gpu(args):
         line["cluster"] = run_cluster(args, torch, dev, stream, cloud)
     if not args.no_plane_cov and rank == 0:
         line["plane_cov"] = run_plane_cov(args, torch, dev, stream, cloud)
+    if not args.no_ransac and rank == 0:
+        line["ransac"] = run_ransac(args, torch, dev, stream, cloud)
     if not args.no_las_stream and rank == 0:
         line["las_stream"] = run_las_stream(args, torch, dev, stream, cloud)
     if not args.no_serving:
@@ -708,6 +712,62 @@ def run_plane_cov(args, torch, dev, stream, cloud):
             value=n / cpu_s / 1e6, unit="Mpoints/s", cores=os.cpu_count() or 1, kind="port",
             sample=f"all {n} points once: KD-tree radius neighbourhoods, FP64 covariance and "
                    "Jacobi, C restatement of covariances_grid.rs:87-206")
+    ctx.close()
+    return out
+
+
+RANSAC_POINTS = 460_000   # the size of the reference's own full-cloud RANSAC measurement
+RANSAC_ITERS = 1000
+RANSAC_THRESHOLD = 0.01
+
+
+def run_ransac(args, torch, dev, stream, cloud):
+    """RANSAC plane segmentation (srcu_ransac_plane_segment) of the first 460k
+    points of the scan (ground plane + boxes + clutter), 1000 hypotheses,
+    threshold 0.01, seed 42, positions device-resident; CPU baseline: the
+    reference's CPU segmenter (C restatement, one thread) on the same points."""
+    import oracle
+    from spatialrust_b200 import _native
+    n = RANSAC_POINTS
+    x, y, z = (np.ascontiguousarray(a[:n]) for a in (cloud.x, cloud.y, cloud.z))
+    cols = [torch.from_numpy(a).to(dev) for a in (x, y, z)]
+    ctx = _native.Context(dev.index)
+    ctx.set_stream(stream.cuda_stream)
+
+    def step():
+        return ctx.ransac_plane_segment(*cols, RANSAC_THRESHOLD, RANSAC_ITERS, 3, 42)
+    for _ in range(3):
+        step()
+    ctx.profile_enable(["ransac"])
+    ctx.profile_read(reset=True)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 10
+    a.record(stream)
+    for _ in range(reps):
+        info, _ = step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    prof = ctx.profile_read(reset=True)["ransac"]
+    ctx.profile_enable([])
+    evals = n * RANSAC_ITERS
+    out = dict(workload=(f"georef scan, first {n} points: RANSAC plane, {RANSAC_ITERS} "
+                         f"hypotheses, threshold {RANSAC_THRESHOLD}, seed 42"),
+               points=n, ms=ms, kernels_ms=prof["total_ms"] / reps,
+               gevals_s=evals / ms / 1e6, inliers=info["inlier_count"],
+               timing="CUDA events around 10 synchronous calls (hypotheses, scoring, selection, "
+                      "mask, FP64 refine)")
+    if not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        ref = oracle.ransac_plane(x, y, z, RANSAC_THRESHOLD, RANSAC_ITERS, 3, 42)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = dict(
+            value=1e3 * cpu_s, unit="ms", cores=1, kind="port",
+            sample=f"the same {n} points, once: RansacPlaneSegmenter::segment_cpu "
+                   "(plane.rs:266-345), C restatement, one thread",
+            same_answer=bool(ref["inlier_count"] == info["inlier_count"]
+                             and ref["best_index"] == info["best_hypothesis"]))
     ctx.close()
     return out
 
