@@ -58,6 +58,10 @@ def test_stages_match_the_oracle_on_a_scan():
         plane=sr.RansacPlaneConfig(distance_threshold=0.05, max_iterations=200, seed=5),
         cluster=sr.EuclideanClusterConfig(cluster_tolerance=0.5, min_cluster_size=3))
     res = sr.MvpPipeline(cfg).run(cloud)
+    # the fused voxel -> normals call gives what the two stages give one after the other
+    two = sr.NormalEstimator(sr.NormalEstimationConfig.radius(0.4, viewpoint=(0, 0, 100))) \
+        .estimate(sr.VoxelGridDownsample(cfg.voxel).filter(cloud))
+    assert res.with_normals == two
     v = oracle.voxel_centroid(c.x, c.y, c.z, [c.intensity], leaf=0.2)
     assert np.array_equal(res.downsampled.field("x"), v.x)
     assert np.array_equal(res.downsampled.field("intensity"), v.fields[3])
