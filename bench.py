@@ -67,6 +67,8 @@ def parse():
                     help="scale of every cloud of the many-clouds measurement (profiling runs)")
     ap.add_argument("--only-batched", action="store_true",
                     help="run the many-clouds measurement alone and print its JSON (profiling runs)")
+    ap.add_argument("--only-ransac", action="store_true",
+                    help="run the RANSAC plane measurement alone (profiling runs)")
     ap.add_argument("--only-las", action="store_true",
                     help="run the LAS ingest -> streaming voxel measurement alone (profiling runs)")
     ap.add_argument("--no-shapes", action="store_true",
@@ -1147,6 +1149,15 @@ def main():
         stream = torch.cuda.Stream(dev)
         torch.cuda.set_stream(stream)
         print(json.dumps(run_batched(args, torch, dev, stream)), flush=True)
+        return
+    if args.only_ransac:
+        import torch
+        torch.cuda.set_device(0)
+        dev = torch.device("cuda", 0)
+        stream = torch.cuda.Stream(dev)
+        torch.cuda.set_stream(stream)
+        args.no_cpu_baseline = True
+        print(json.dumps(run_ransac(args, torch, dev, stream, workload_cloud())), flush=True)
         return
     if args.only_las:
         import torch
