@@ -122,8 +122,14 @@ srcu_status ransac_score(srcu_ctx *ctx, const srcu_cloud *cloud, const float **c
     k_ransac_planes<<<ceil_div(count, 256), 256, 0, ctx->stream>>>(
         cols[0], cols[1], cols[2], n, ptr<const uint32_t>(ctx->rs_hyp), count,
         ptr<float4>(ctx->rs_planes), ptr<uint32_t>(ctx->rs_valid), status);
-    k_ransac_score<<<ceil_div(n, RS_TILE), RS_THREADS, 0, ctx->stream>>>(
-        cols[0], cols[1], cols[2], n, ptr<const float4>(ctx->rs_planes), count, thr,
+    // enough blocks for every SM: point tiles x hypothesis chunks (>= 32 planes each)
+    const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n, RS_TILE));
+    const uint32_t want = uint32_t(ctx->num_sms) * 8;
+    const uint32_t chunks = std::max<uint32_t>(
+        1, std::min<uint32_t>(ceil_div(count, 32), ceil_div(want, tiles)));
+    const uint32_t per_chunk = ceil_div(count, chunks);
+    k_ransac_score<<<dim3(tiles, ceil_div(count, per_chunk)), RS_THREADS, 0, ctx->stream>>>(
+        cols[0], cols[1], cols[2], n, ptr<const float4>(ctx->rs_planes), count, per_chunk, thr,
         ptr<uint32_t>(ctx->rs_counts));
   }
   CU_TRY(cudaGetLastError());

@@ -66,11 +66,14 @@ __device__ __forceinline__ bool plane_inlier(float4 pl, float px, float py, floa
   return fabsf(s) <= thr;
 }
 
-// counts[h] += inliers of plane h among this block's RS_TILE points.
+// counts[h] += inliers of plane h among this block's RS_TILE points, for the
+// planes [blockIdx.y * per_chunk, +per_chunk): the second grid dimension
+// splits the hypotheses so that small clouds still fill every SM.
 __global__ void __launch_bounds__(RS_THREADS) k_ransac_score(const float *x, const float *y,
                                                              const float *z, uint64_t n,
                                                              const float4 *planes, uint32_t count,
-                                                             float thr, uint32_t *counts) {
+                                                             uint32_t per_chunk, float thr,
+                                                             uint32_t *counts) {
   __shared__ float4 sp[RS_PLANES];
   __shared__ uint32_t sc[RS_PLANES];
   float px[RS_PTS], py[RS_PTS], pz[RS_PTS];
@@ -84,8 +87,10 @@ __global__ void __launch_bounds__(RS_THREADS) k_ransac_score(const float *x, con
     pz[k] = in ? z[i] : 0.f;
   }
   const uint32_t lane = threadIdx.x & 31u;
-  for (uint32_t c0 = 0; c0 < count; c0 += RS_PLANES) {
-    const uint32_t m = min(uint32_t(RS_PLANES), count - c0);
+  const uint32_t c_begin = blockIdx.y * per_chunk;
+  const uint32_t c_end = min(count, c_begin + per_chunk);
+  for (uint32_t c0 = c_begin; c0 < c_end; c0 += RS_PLANES) {
+    const uint32_t m = min(uint32_t(RS_PLANES), c_end - c0);
     for (uint32_t j = threadIdx.x; j < m; j += RS_THREADS) {
       sp[j] = planes[c0 + j];
       sc[j] = 0;
