@@ -223,6 +223,15 @@ srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
 srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float radius,
                                    float epsilon, float *cov, srcu_normal_stats *stats);
 
+/* ---- failure path self-test ------------------------------------------------ */
+
+/* No counterpart in the reference.  Runs one device-side wait on a flag that
+ * nothing sets, bounded at max_polls polls about a microsecond apart (at most
+ * 2^21), so that the wait gives up the way every wait in this library does:
+ * the call returns SRCU_ERR_TIMEOUT and the context stays usable.  For
+ * health checks and tests of the error path; it never faults the GPU. */
+srcu_status srcu_selftest_bounded_wait(srcu_ctx *ctx, uint32_t max_polls);
+
 /* ---- RANSAC plane segmentation ------------------------------------------- */
 
 /* GpuPlaneScore (crates/spatialrust-gpu/src/kernels/ransac_plane.rs:27-37). */

@@ -267,6 +267,7 @@ SIGNATURES = {
     "srcu_stream_voxel_fetch": ([_P, ctypes.c_uint64, ctypes.c_uint64,
                                  ctypes.POINTER(SrcuStreamVoxelOut)], ctypes.c_int),
     "srcu_stream_voxel_destroy": ([_P], None),
+    "srcu_selftest_bounded_wait": ([_P, ctypes.c_uint32], ctypes.c_int),
     "srcu_ransac_plane_scores": ([_P, ctypes.POINTER(SrcuCloud), ctypes.c_void_p, ctypes.c_uint32,
                                   ctypes.c_float, ctypes.POINTER(SrcuPlaneScore)], ctypes.c_int),
     "srcu_ransac_plane_segment": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuRansacParams),
@@ -524,6 +525,10 @@ class Context:
         self._check(self._lib.srcu_euclidean_cluster_roots(self._h, ctypes.byref(cloud),
                                                            ctypes.c_float(cluster_tolerance), addr))
         return roots[:n]
+
+    def selftest_bounded_wait(self, max_polls: int = 1000):
+        """Runs a device wait that must give up: raises DeviceTimeout."""
+        self._check(self._lib.srcu_selftest_bounded_wait(self._h, int(max_polls)))
 
     def ransac_plane_segment(self, x, y, z, distance_threshold: float = 0.01,
                              max_iterations: int = 1000, min_inliers: int = 3, seed: int = 42):

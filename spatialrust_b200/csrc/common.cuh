@@ -198,6 +198,22 @@ __device__ __forceinline__ uint32_t block_exclusive_sum(uint32_t v, uint32_t *sc
   return warp_off + x - v;
 }
 
+// Self-test of the failure path: waits for *flag to become non-zero, polling
+// at most max_polls times about a microsecond apart, then gives up the way
+// every wait in this library does (status bit ST_TIMEOUT) and returns.
+template <class Ctl>
+__global__ void k_selftest_wait(Ctl *ctl, const uint32_t *flag, uint32_t max_polls) {
+  if (threadIdx.x != 0) return;
+  uint32_t polls = 0;
+  while (ld_relaxed_u32(flag) == 0) {
+    if (++polls > max_polls) {
+      atomicOr(&ctl->status, ST_TIMEOUT);
+      return;
+    }
+    __nanosleep(1000);
+  }
+}
+
 __device__ __forceinline__ uint32_t warp_exclusive_sum(uint32_t v, uint32_t *total) {
   const uint32_t lane = threadIdx.x & 31u;
   uint32_t x = v;

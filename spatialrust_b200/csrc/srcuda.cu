@@ -784,6 +784,20 @@ srcu_status srcu_set_stream(srcu_ctx *ctx, void *cuda_stream) {
   return SRCU_OK;
 }
 
+srcu_status srcu_selftest_bounded_wait(srcu_ctx *ctx, uint32_t max_polls) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  if (max_polls == 0 || max_polls > SPIN_LIMIT)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "max_polls must be in [1, %u]", SPIN_LIMIT);
+  CU_TRY(cudaSetDevice(ctx->device));
+  // the flag is a word of the control block that this call zeroes and nothing sets
+  uint32_t *flag = &ctx->ctl->work[63];
+  CU_TRY(cudaMemsetAsync(flag, 0, sizeof(uint32_t), ctx->stream));
+  CU_TRY(cudaMemsetAsync(&ctx->ctl->status, 0, sizeof(uint32_t), ctx->stream));
+  k_selftest_wait<<<1, 32, 0, ctx->stream>>>(ctx->ctl, flag, max_polls);
+  CU_TRY(cudaGetLastError());
+  return read_control(ctx);
+}
+
 srcu_status srcu_synchronize(srcu_ctx *ctx) {
   if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
   CU_TRY(cudaStreamSynchronize(ctx->stream));

@@ -340,6 +340,22 @@ __device__ void stream_reduce_short(Control *ctl, const SortedView &sv, const St
   out.kx[r] = kx;
   out.ky[r] = ky;
   out.kz[r] = kz;
+  if (j == i + 1) {
+    // one item (the common case): every column's value is its sum, and the
+    // column loads are independent, so they are all issued before any is used
+    const uint32_t v = sv.val(i);
+    out.cnt[r] = Records ? in.cnt[v] : 1ull;
+    for (uint32_t c0 = 0; c0 < in.nc; c0 += 4) {
+      double val[4];
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k)
+        if (c0 + k < in.nc) val[k] = stream_value<Records>(in, c0 + k, v);
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k)
+        if (c0 + k < in.nc) out.sum[c0 + k][r] = val[k];
+    }
+    return;
+  }
   unsigned long long cnt = j - i;
   if (Records) {
     cnt = 0;
