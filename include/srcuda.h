@@ -333,6 +333,8 @@ srcu_status srcu_stream_voxel_finish(srcu_stream_voxel *sv, srcu_stream_voxel_in
 /* Copies voxels [first, first + count) of the finished stream. */
 srcu_status srcu_stream_voxel_fetch(srcu_stream_voxel *sv, uint64_t first, uint64_t count,
                                     const srcu_stream_voxel_out *out);
+/* Ends a stream.  Its device buffers stay with the context for the context's next
+ * stream (srcu_destroy frees them); destroy every stream before its context. */
 void srcu_stream_voxel_destroy(srcu_stream_voxel *sv);
 
 /* ---- LAS point records ---------------------------------------------------- */
