@@ -223,6 +223,46 @@ srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
 srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float radius,
                                    float epsilon, float *cov, srcu_normal_stats *stats);
 
+/* ---- sort launch shapes and their tuning ------------------------------------ */
+
+/* The onesweep radix sort is built in several launch shapes -- keys per thread
+ * and the blocks per SM its registers are capped for; 8-bit digits throughout.
+ * A context picks one per sort from a table of input sizes, one table per sort
+ * kind (the voxel-key sort over the input points, the cell-key sort of the
+ * radius grid).  The built-in tables were measured by spatialrust_b200.autotune
+ * on a B200; srcu_set_sort_tuning installs others (the autotuner does so while
+ * it measures).  No counterpart in the reference (its wgpu bitonic sort has
+ * fixed workgroups). */
+#define SRCU_SORT_TUNING_MAX 32
+#define SRCU_SORT_VOXEL_KEYS 0
+#define SRCU_SORT_CELL_KEYS 1
+
+typedef struct srcu_sort_config {
+  uint32_t items_per_thread;
+  uint32_t blocks_per_sm;
+  uint32_t digit_bits;
+  uint32_t threads_per_block;
+} srcu_sort_config;
+
+/* Fills up to max_entries shapes; returns how many the library has. */
+int srcu_sort_configs(srcu_sort_config *out, int max_entries);
+/* Entry k of the `kind` table: sorts of at most max_points[k] keys use shape
+ * config[k] (ascending sizes; the last entry also covers every larger sort).
+ * count 0 restores the built-in table. */
+srcu_status srcu_set_sort_tuning(srcu_ctx *ctx, int32_t kind, const uint64_t *max_points,
+                                 const int32_t *config, uint32_t count);
+/* *count: capacity in, entries out. */
+srcu_status srcu_get_sort_tuning(srcu_ctx *ctx, int32_t kind, uint64_t *max_points,
+                                 int32_t *config, uint32_t *count);
+
+/* The normals kernel's neighbour gather: 1 stages each warp's candidate records
+ * (the x-strips of its 3x3 column block) in shared memory by non-multicast
+ * cp.async.bulk copies before the walk; 0 reads them through L1.  Both give
+ * identical results.  -1 restores the built-in choice (measured by the
+ * autotuner).  Plane covariances always read through L1. */
+srcu_status srcu_set_neighbor_staging(srcu_ctx *ctx, int32_t mode);
+int32_t srcu_get_neighbor_staging(srcu_ctx *ctx);
+
 /* ---- failure path self-test ------------------------------------------------ */
 
 /* No counterpart in the reference.  Runs one device-side wait on a flag that

@@ -268,6 +268,13 @@ SIGNATURES = {
                                  ctypes.POINTER(SrcuStreamVoxelOut)], ctypes.c_int),
     "srcu_stream_voxel_destroy": ([_P], None),
     "srcu_selftest_bounded_wait": ([_P, ctypes.c_uint32], ctypes.c_int),
+    "srcu_sort_configs": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "srcu_set_neighbor_staging": ([_P, ctypes.c_int32], ctypes.c_int),
+    "srcu_get_neighbor_staging": ([_P], ctypes.c_int32),
+    "srcu_set_sort_tuning": ([_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int32),
+                              ctypes.c_uint32], ctypes.c_int),
+    "srcu_get_sort_tuning": ([_P, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int32),
+                              ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
     "srcu_ransac_plane_scores": ([_P, ctypes.POINTER(SrcuCloud), ctypes.c_void_p, ctypes.c_uint32,
                                   ctypes.c_float, ctypes.POINTER(SrcuPlaneScore)], ctypes.c_int),
     "srcu_ransac_plane_segment": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuRansacParams),
@@ -287,6 +294,22 @@ SIGNATURES = {
 }
 
 _lib = None
+
+SORT_TUNING_MAX = 32
+SORT_KINDS = {"voxel": 0, "cell": 1}  # SRCU_SORT_VOXEL_KEYS, SRCU_SORT_CELL_KEYS
+
+
+class SrcuSortConfig(ctypes.Structure):
+    _fields_ = [("items_per_thread", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
+                ("digit_bits", ctypes.c_uint32), ("threads_per_block", ctypes.c_uint32)]
+
+
+def sort_configs() -> list:
+    """The sort launch shapes the library was built with, by index."""
+    lib = load()
+    arr = (SrcuSortConfig * 16)()
+    n = lib.srcu_sort_configs(arr, 16)
+    return [{f: int(getattr(arr[k], f)) for f, _ in SrcuSortConfig._fields_} for k in range(min(n, 16))]
 
 
 def library_path() -> str:
@@ -525,6 +548,40 @@ class Context:
         self._check(self._lib.srcu_euclidean_cluster_roots(self._h, ctypes.byref(cloud),
                                                            ctypes.c_float(cluster_tolerance), addr))
         return roots[:n]
+
+    def sort_tuning(self, kind: str | None = None):
+        """[(max_points, launch shape index)] this context sorts `kind` keys
+        with ("voxel" or "cell"); both as a dict when kind is None."""
+        if kind is None:
+            return {k: self.sort_tuning(k) for k in SORT_KINDS}
+        cap = SORT_TUNING_MAX
+        mp = (ctypes.c_uint64 * cap)()
+        cf = (ctypes.c_int32 * cap)()
+        cnt = ctypes.c_uint32(cap)
+        self._check(self._lib.srcu_get_sort_tuning(self._h, SORT_KINDS[kind], mp, cf,
+                                                   ctypes.byref(cnt)))
+        return [(int(mp[k]), int(cf[k])) for k in range(cnt.value)]
+
+    def set_sort_tuning(self, table, kind: str | None = None) -> None:
+        """Installs [(max_points, launch shape index)], ascending sizes, for
+        the `kind` sort ("voxel" or "cell"; both when None); the last entry
+        also covers larger sorts.  An empty table restores the built-in one."""
+        if kind is None:
+            for k in SORT_KINDS:
+                self.set_sort_tuning(table, k)
+            return
+        table = list(table)
+        mp = (ctypes.c_uint64 * max(1, len(table)))(*[int(m) for m, _ in table])
+        cf = (ctypes.c_int32 * max(1, len(table)))(*[int(c) for _, c in table])
+        self._check(self._lib.srcu_set_sort_tuning(self._h, SORT_KINDS[kind], mp, cf, len(table)))
+
+    def set_neighbor_staging(self, mode: int) -> None:
+        """1: the normals kernel stages candidate records in shared memory by
+        bulk copies; 0: it reads them through L1; -1: the built-in choice."""
+        self._check(self._lib.srcu_set_neighbor_staging(self._h, int(mode)))
+
+    def neighbor_staging(self) -> int:
+        return int(self._lib.srcu_get_neighbor_staging(self._h))
 
     def selftest_bounded_wait(self, max_polls: int = 1000):
         """Runs a device wait that must give up: raises DeviceTimeout."""

@@ -13,7 +13,7 @@ PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libsrcuda.so")
 SOURCES = [os.path.join(HERE, "srcuda.cu"), os.path.join(HERE, "server.cu")]
-HEADERS = [os.path.join(HERE, f) for f in os.listdir(HERE) if f.endswith((".cuh", ".cu"))] + [
+HEADERS = [os.path.join(HERE, f) for f in os.listdir(HERE) if f.endswith((".cuh", ".cu", ".h"))] + [
     os.path.join(ROOT, "include", "srcuda.h")]
 
 NVCC_FLAGS = [

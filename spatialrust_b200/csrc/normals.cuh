@@ -416,6 +416,32 @@ __global__ void __launch_bounds__(256) k_ranges(Control *ctl, const uint64_t *ce
 constexpr int NM_THREADS = 256;
 constexpr int NM_FLUSH = 32;  // f32 partial moments are folded into FP64 every NM_FLUSH candidates
 constexpr double NM_REFINE_GAP = 0.05;  // (l1 - l0) / trace below this -> FP64 moments
+constexpr uint32_t NM_STAGE = 256;  // candidate records staged per warp (4 KB), staged gather
+
+// Staged gather: one mbarrier per warp, completed by the bulk copies' bytes.
+__device__ __forceinline__ uint32_t nm_smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void nm_bar_init(uint64_t *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(nm_smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void nm_bar_expect(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(nm_smem_addr(bar)),
+               "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool nm_bar_try(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+               " selp.u32 %0, 1, 0, p;\n}\n" : "=r"(ok) : "r"(nm_smem_addr(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+// Non-multicast bulk copy global -> this CTA's shared memory (16-byte aligned
+// addresses, a multiple of 16 bytes).
+__device__ __forceinline__ void nm_bulk(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(nm_smem_addr(dst)), "l"(src), "r"(bytes), "r"(nm_smem_addr(bar)) : "memory");
+}
+__device__ const uint2 nm_no_ranges[9] = {};  // the walk of a lane whose cell is out of range
 
 // Covariance from moments about the query (S: sx sy sz sxx syy szz sxy sxz syz
 // over n points) and its smallest eigenpair, FP64.
@@ -497,7 +523,16 @@ __device__ __noinline__ void moments_fp64(const float4 *pts, const uint2 *rg, fl
 // the smallest eigenvector is needed.  Six floats per point in cov
 // ([c00, c11, c22, c01, c02, c12], the GpuCovariance layout); fewer than 3
 // points in the (self-inclusive) neighbourhood give (eps, eps, eps, 0, 0, 0).
-template <bool CountShell, bool PlaneCov = false>
+//
+// Staged: the warp's candidate records are brought into shared memory by
+// non-multicast bulk copies (cp.async.bulk on a per-warp mbarrier) before the
+// walk, one copy per x-strip of the 3x3 column block -- for each x offset, the
+// span over the warp's lanes of their three column ranges, which lie close
+// together in the cell-sorted records.  A strip that does not fit the warp's
+// NM_STAGE records is read from global memory as in the plain walk.  The plain
+// walk reads through L1 instead; which one a context runs is a tuning choice
+// (srcu_set_neighbor_staging).
+template <bool CountShell, bool PlaneCov = false, bool Staged = false>
 __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const float4 *pts,
                                                            const uint32_t *pt_cell,
                                                            const uint2 *ranges,
@@ -514,6 +549,18 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
   const uint32_t batches = (n + 31) / 32;
   const uint32_t warps = gridDim.x * (NM_THREADS / 32);
   unsigned long long n_valid = 0, n_invalid = 0, n_shell = 0, n_fp64 = 0;
+  float4 *sbuf = nullptr;  // this warp's staging buffer (Staged)
+  uint64_t *sbar = nullptr;
+  uint32_t phase = 0;
+  bool timed_out = false;
+  if constexpr (Staged) {
+    __shared__ float4 nm_stage[(NM_THREADS / 32) * NM_STAGE];
+    __shared__ __align__(8) uint64_t nm_bar[NM_THREADS / 32];
+    sbuf = nm_stage + (threadIdx.x >> 5) * NM_STAGE;
+    sbar = &nm_bar[threadIdx.x >> 5];
+    if (lane == 0) nm_bar_init(sbar);
+    __syncwarp();
+  }
 
   for (uint32_t b = blockIdx.x * (NM_THREADS / 32) + (threadIdx.x >> 5); b < batches; b += warps) {
     const uint32_t i = b * 32 + lane;
@@ -521,17 +568,22 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
     const uint32_t ii = active ? i : n - 1;
     const float4 qp = pts[ii];
     const uint32_t u = pt_cell[ii];
+    bool bad = false;
     if (u >= u_count) {  // cannot happen for a consistent cell table
       atomicOr(&ctl->status, ST_INTERNAL);
-      continue;
+      if constexpr (Staged) {
+        bad = true;  // the lane stays for the warp's collectives and walks nothing
+      } else {
+        continue;
+      }
     }
     uint32_t cb = 0;  // the query's cloud
-    if (bt.clouds > 1 && lb < 64) cb = uint32_t(cell_key[u] >> lb);
+    if (!bad && bt.clouds > 1 && lb < 64) cb = uint32_t(cell_key[u] >> lb);
     if (cb >= bt.clouds) cb = 0;
     const NormalParamsDev prm = bt.nparams[cb];
     const float r2 = bt.cplans[cb].r2;
     const float shell_tol = bt.cplans[cb].shell_tol;
-    const uint2 *rg = ranges + size_t(u) * 9;
+    const uint2 *rg = bad ? nm_no_ranges : ranges + size_t(u) * 9;
     float hits = 0.f;
     uint32_t shell = 0;
     double S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // sx sy sz sxx syy szz sxy sxz syz
@@ -567,35 +619,125 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
         F[k] = 0.f;
       }
     };
-    uint2 next = rg[0];
+    if constexpr (Staged) {
+      // Stage the warp's x-strips; shared index = record index + delta[d].
+      int32_t delta[3];
+      uint32_t staged = 0;
+      {
+        uint32_t lo[3], len[3], total = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          uint32_t a = 0xffffffffu, z = 0;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const uint2 g = rg[3 * d + k];
+            if (g.y > g.x) {
+              a = min(a, g.x);
+              z = max(z, g.y);
+            }
+          }
+          a = __reduce_min_sync(FULL_MASK, a);
+          z = __reduce_max_sync(FULL_MASK, z);
+          lo[d] = a;
+          len[d] = z > a ? z - a : 0;
+          delta[d] = int32_t(total) - int32_t(a);
+          if (len[d] > 0 && total + len[d] <= NM_STAGE) {
+            staged |= 1u << d;
+            total += len[d];
+          }
+        }
+        if (total > 0 && !timed_out) {
+          __syncwarp();  // every lane is done with the buffer's previous contents
+          if (lane == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            nm_bar_expect(sbar, total * 16u);
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+              if ((staged >> d) & 1u)
+                nm_bulk(sbuf + (int32_t(lo[d]) + delta[d]), pts + lo[d], len[d] * 16u, sbar);
+          }
+          uint32_t spins = 0;
+          bool gave_up = false;
+          while (!nm_bar_try(sbar, phase)) {
+            if (++spins > SPIN_LIMIT) {
+              gave_up = true;
+              break;
+            }
+          }
+          if (__any_sync(FULL_MASK, gave_up)) {
+            timed_out = true;  // read everything from global memory from now on
+            if (lane == 0) atomicOr(&ctl->status, ST_TIMEOUT);
+          } else {
+            phase ^= 1u;
+          }
+        }
+        if (timed_out) staged = 0;
+      }
+      auto walk = [&](auto load, uint32_t a, uint32_t z) {
+        uint32_t j = a;
+        for (; j + 2 <= z; j += 2) {
+          const float4 c0 = load(j);
+          const float4 c1 = load(j + 1);
+          visit(c0);
+          visit(c1);
+          since += 2;
+          if (since >= NM_FLUSH) {
+            since = 0;
+            flush();
+          }
+        }
+        if (j < z) {
+          visit(load(j));
+          if (++since >= NM_FLUSH) {
+            since = 0;
+            flush();
+          }
+        }
+      };
+      uint2 next = rg[0];
 #pragma unroll 1
-    for (int r = 0; r < 9; ++r) {
-      const uint2 range = next;
-      if (r < 8) next = rg[r + 1];  // the next column's range loads under this one
-      uint32_t j = range.x;
-      // two independent candidate loads in flight per step
-      for (; j + 2 <= range.y; j += 2) {
-        const float4 c0 = __ldg(pts + j);
-        const float4 c1 = __ldg(pts + j + 1);
-        visit(c0);
-        visit(c1);
-        since += 2;
-        if (since >= NM_FLUSH) {
-          since = 0;
-          flush();
+      for (int r = 0; r < 9; ++r) {
+        const uint2 range = next;
+        if (r < 8) next = rg[r + 1];
+        const int d = r / 3;
+        if ((staged >> d) & 1u) {
+          const float4 *sp = sbuf + delta[d];
+          walk([&](uint32_t j) { return sp[j]; }, range.x, range.y);
+        } else {
+          walk([&](uint32_t j) { return __ldg(pts + j); }, range.x, range.y);
         }
       }
-      if (j < range.y) {
-        visit(__ldg(pts + j));
-        if (++since >= NM_FLUSH) {
-          since = 0;
-          flush();
+    } else {
+      uint2 next = rg[0];
+#pragma unroll 1
+      for (int r = 0; r < 9; ++r) {
+        const uint2 range = next;
+        if (r < 8) next = rg[r + 1];  // the next column's range loads under this one
+        uint32_t j = range.x;
+        // two independent candidate loads in flight per step
+        for (; j + 2 <= range.y; j += 2) {
+          const float4 c0 = __ldg(pts + j);
+          const float4 c1 = __ldg(pts + j + 1);
+          visit(c0);
+          visit(c1);
+          since += 2;
+          if (since >= NM_FLUSH) {
+            since = 0;
+            flush();
+          }
+        }
+        if (j < range.y) {
+          visit(__ldg(pts + j));
+          if (++since >= NM_FLUSH) {
+            since = 0;
+            flush();
+          }
         }
       }
     }
 #pragma unroll
     for (int k = 0; k < 9; ++k) S[k] += double(F[k]);
-    if (!active) continue;
+    if (!active || bad) continue;
     // hits includes the query itself exactly once when it is finite.
     const bool finite = isfinite(qp.x) && isfinite(qp.y) && isfinite(qp.z);
     const uint32_t h = uint32_t(hits);
@@ -676,6 +818,13 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
     nz[qidx] = oz;
     curv[qidx] = oc;
     if (counts) counts[qidx] = prm.include_self ? n_eff : cnt;
+  }
+  if constexpr (Staged) {
+    if (timed_out) {  // a copy that was given up on may still land: wait for it, bounded
+      uint32_t spins = 0;
+      while (!nm_bar_try(sbar, phase) && ++spins <= SPIN_LIMIT) {
+      }
+    }
   }
   // one atomic per warp for the counters
 #pragma unroll

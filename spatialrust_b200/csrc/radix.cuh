@@ -37,14 +37,17 @@ constexpr int OS_TILE = OS_THREADS * OS_ITEMS;  // 4096 keys per tile
 constexpr int HIST_COPIES = 2;                  // shared histogram copies (by warp parity)
 constexpr int LB_WIDTH = 8;                     // look-back words read per step
 
+template <int TILE>
 struct OnesweepTileSmem {
-  uint64_t keys[OS_TILE];
-  uint32_t vals[OS_TILE];
+  uint64_t keys[TILE];
+  uint32_t vals[TILE];
 };
 
-struct OnesweepSmem {
+// Shared memory of one sort block for tiles of TILE keys.
+template <int TILE>
+struct OnesweepSmemT {
   union {
-    OnesweepTileSmem tile;
+    OnesweepTileSmem<TILE> tile;
     uint32_t hist[HIST_COPIES][MAX_DIGITS][RADIX_BINS];
   } u;
   uint32_t whist[OS_WARPS][RADIX_BINS];
@@ -57,6 +60,15 @@ struct OnesweepSmem {
   uint32_t num_active;
   uint32_t tile;
 };
+using OnesweepSmem = OnesweepSmemT<OS_TILE>;
+
+// The sort's launch shapes the library is built with: keys per thread and the
+// blocks per SM the registers are capped for (8-bit digits throughout).  The
+// autotuner picks among them per input size (srcu_set_sort_tuning).
+constexpr int SORT_CONFIGS = 4;
+constexpr int kSortItems[SORT_CONFIGS] = {16, 8, 12, 8};
+constexpr int kSortMinBlocks[SORT_CONFIGS] = {2, 3, 3, 4};
+constexpr int SORT_MIN_ITEMS = 8;  // the smallest tile sizes the look-back buffer
 
 // Ping-pong buffers of one sort.
 struct SortBuffers {
@@ -128,12 +140,14 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, uint32_t valid_mask)
   return peers;
 }
 
-template <class Src>
-__global__ void __launch_bounds__(OS_THREADS, 2) k_sort(Src src, Control *ctl, uint32_t *hist,
-                                                     SortBuffers buf, uint32_t epoch_off,
-                                                     int work_slot, SortState *st) {
+template <class Src, int ITEMS = OS_ITEMS, int MINB = 2>
+__global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl, uint32_t *hist,
+                                                        SortBuffers buf, uint32_t epoch_off,
+                                                        int work_slot, SortState *st) {
+  constexpr int TILE = OS_THREADS * ITEMS;
+  constexpr int WARP_ITEMS = ITEMS * 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  OnesweepSmem &sm = *reinterpret_cast<OnesweepSmem *>(smem_raw);
+  OnesweepSmemT<TILE> &sm = *reinterpret_cast<OnesweepSmemT<TILE> *>(smem_raw);
   if (ld_relaxed_u32(&ctl->status)) return;  // before any barrier: every block agrees
   src.prepare(ctl);
   const uint32_t n = src.count(ctl);
@@ -192,7 +206,7 @@ __global__ void __launch_bounds__(OS_THREADS, 2) k_sort(Src src, Control *ctl, u
   }
   __syncthreads();
   const uint32_t num_active = sm.num_active;
-  const uint32_t num_tiles = (n + OS_TILE - 1) / OS_TILE;
+  const uint32_t num_tiles = (n + TILE - 1) / TILE;
   const uint64_t idx_mask = (1ull << idx_bits) - 1;
 
   // ---- digit passes ------------------------------------------------------
@@ -217,14 +231,14 @@ __global__ void __launch_bounds__(OS_THREADS, 2) k_sort(Src src, Control *ctl, u
       __syncthreads();
       const uint32_t tile = sm.tile;
       if (tile >= num_tiles) break;
-      const uint32_t base = tile * OS_TILE;
-      const uint32_t wbase = base + warp * OS_WARP_ITEMS;
+      const uint32_t base = tile * TILE;
+      const uint32_t wbase = base + warp * WARP_ITEMS;
 
-      uint64_t k[OS_ITEMS];
-      uint32_t v[OS_ITEMS];
-      uint32_t rank[OS_ITEMS];
+      uint64_t k[ITEMS];
+      uint32_t v[ITEMS];
+      uint32_t rank[ITEMS];
 #pragma unroll
-      for (int i = 0; i < OS_ITEMS; ++i) {
+      for (int i = 0; i < ITEMS; ++i) {
         const uint32_t idx = wbase + uint32_t(i) * 32u + lane;
         k[i] = 0;
         v[i] = 0;
@@ -243,7 +257,7 @@ __global__ void __launch_bounds__(OS_THREADS, 2) k_sort(Src src, Control *ctl, u
       // warp with the same digit.  One leader per digit per step updates the
       // warp's counter, so no atomics are needed.
 #pragma unroll
-      for (int i = 0; i < OS_ITEMS; ++i) {
+      for (int i = 0; i < ITEMS; ++i) {
         const bool valid = (wbase + uint32_t(i) * 32u + lane) < n;
         const uint32_t d = uint32_t(k[i] >> shift) & 0xffu;
         const uint32_t peers = digit_peers(d, __ballot_sync(FULL_MASK, valid));
@@ -278,7 +292,7 @@ __global__ void __launch_bounds__(OS_THREADS, 2) k_sort(Src src, Control *ctl, u
       __syncthreads();
       // Scatter to shared memory in digit order.
 #pragma unroll
-      for (int i = 0; i < OS_ITEMS; ++i) {
+      for (int i = 0; i < ITEMS; ++i) {
         if ((wbase + uint32_t(i) * 32u + lane) < n) {
           const uint32_t d = uint32_t(k[i] >> shift) & 0xffu;
           const uint32_t pos = sm.tile_excl[d] + sm.whist[warp][d] + rank[i];
@@ -322,7 +336,7 @@ __global__ void __launch_bounds__(OS_THREADS, 2) k_sort(Src src, Control *ctl, u
       }
       sm.gbase[t] = sm.digit_start[t] + excl - texcl;
       __syncthreads();
-      const uint32_t tile_n = min(uint32_t(OS_TILE), n - base);
+      const uint32_t tile_n = min(uint32_t(TILE), n - base);
       for (uint32_t j = t; j < tile_n; j += OS_THREADS) {
         const uint64_t kk = sm.u.tile.keys[j];
         const uint32_t pos = sm.gbase[uint32_t(kk >> shift) & 0xffu] + j;

@@ -12,6 +12,7 @@
 #include "../../include/srcuda.h"
 #include "cluster.cuh"
 #include "normals.cuh"
+#include "sort_tuning.h"
 #include "voxel.cuh"
 
 using namespace srcu;
@@ -41,7 +42,15 @@ struct srcu_ctx {
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_voxel = nullptr;
   unsigned char *head_host = nullptr;
-  int occ_onesweep_v = 1, occ_onesweep_c = 1, occ_normals = 1, occ_seg = 1, occ_cells = 1;
+  int occ_normals = 1, occ_normals_staged = 1, occ_seg = 1, occ_cells = 1;
+  int neighbor_staging = 0;  // k_normals gathers through shared memory by bulk copies
+  // co-resident blocks per SM of each sort launch shape, voxel-key and cell-key sorts
+  int occ_sort_v[SORT_CONFIGS] = {}, occ_sort_c[SORT_CONFIGS] = {};
+  // sort launch shape by input size, per sort kind (SRCU_SORT_VOXEL_KEYS /
+  // SRCU_SORT_CELL_KEYS; sort_tuning.h, srcu_set_sort_tuning)
+  uint64_t tune_max_points[2][SRCU_SORT_TUNING_MAX] = {};
+  int32_t tune_config[2][SRCU_SORT_TUNING_MAX] = {};
+  uint32_t tune_count[2] = {};
   // input staging (host inputs are copied here)
   DevBuf in[MAX_COLS];
   // sort
@@ -235,7 +244,9 @@ srcu_status reserve(srcu_ctx *ctx, uint64_t n, uint32_t cols, bool host_input, b
   ST_TRY(ensure(ctx, ctx->keys[1], m * 8));
   ST_TRY(ensure(ctx, ctx->vals[0], m * 4));
   ST_TRY(ensure(ctx, ctx->vals[1], m * 4));
-  ST_TRY(ensure(ctx, ctx->lb_sort, size_t(ceil_div(m, OS_TILE)) * RADIX_BINS * 8, true));
+  // look-back words for the smallest tile any sort launch shape uses
+  ST_TRY(ensure(ctx, ctx->lb_sort,
+                size_t(ceil_div(m, OS_THREADS * SORT_MIN_ITEMS)) * RADIX_BINS * 8, true));
   ST_TRY(ensure(ctx, ctx->in_aos, m * 16));
   if (voxel) {
     ST_TRY(ensure(ctx, ctx->vaos, m * 16));
@@ -450,6 +461,96 @@ srcu_status launch_sort(srcu_ctx *ctx, const Src &src, uint64_t n_max, uint32_t 
   return SRCU_OK;
 }
 
+// One launch shape of the sort: C indexes kSortItems / kSortMinBlocks.
+template <class Src, int C>
+cudaError_t launch_sort_config(cudaStream_t stream, uint32_t grid_cap, const Src &src,
+                               Control *ctl, uint32_t *hist, const SortBuffers &sb,
+                               uint32_t epoch_off, int work_slot, SortState *st, uint64_t n_max) {
+  constexpr int TILE = OS_THREADS * kSortItems[C];
+  const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, TILE));
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(tiles, grid_cap));
+  Src s = src;
+  Control *c = ctl;
+  uint32_t *h = hist;
+  SortBuffers b = sb;
+  uint32_t e = epoch_off;
+  int w = work_slot;
+  SortState *ss = st;
+  void *args[] = {&s, &c, &h, &b, &e, &w, &ss};
+  return cudaLaunchCooperativeKernel(
+      reinterpret_cast<const void *>(&k_sort<Src, kSortItems[C], kSortMinBlocks[C]>), dim3(grid),
+      dim3(OS_THREADS), args, sizeof(OnesweepSmemT<TILE>), stream);
+}
+
+template <class Src, int C>
+cudaError_t sort_config_setup(int *occ) {
+  constexpr int TILE = OS_THREADS * kSortItems[C];
+  const void *kern = reinterpret_cast<const void *>(&k_sort<Src, kSortItems[C], kSortMinBlocks[C]>);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(sizeof(OnesweepSmemT<TILE>)));
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, OS_THREADS,
+                                                    sizeof(OnesweepSmemT<TILE>));
+  *occ = std::max(1, *occ);
+  return e;
+}
+
+template <class Src>
+cudaError_t sort_setup(int (&occ)[SORT_CONFIGS]) {
+  static_assert(SORT_CONFIGS == 4, "one setup per launch shape");
+  cudaError_t e = sort_config_setup<Src, 0>(&occ[0]);
+  if (e == cudaSuccess) e = sort_config_setup<Src, 1>(&occ[1]);
+  if (e == cudaSuccess) e = sort_config_setup<Src, 2>(&occ[2]);
+  if (e == cudaSuccess) e = sort_config_setup<Src, 3>(&occ[3]);
+  return e;
+}
+
+int sort_config_for(const srcu_ctx *ctx, int kind, uint64_t n) {
+  const uint32_t cnt = ctx->tune_count[kind];
+  for (uint32_t k = 0; k < cnt; ++k)
+    if (n <= ctx->tune_max_points[kind][k]) return ctx->tune_config[kind][k];
+  return cnt ? ctx->tune_config[kind][cnt - 1] : 0;
+}
+
+void builtin_sort_tuning(srcu_ctx *ctx, int kind) {
+  const uint32_t cnt = kind == SRCU_SORT_VOXEL_KEYS ? kVoxelSortTuneCount : kCellSortTuneCount;
+  const uint64_t *mp = kind == SRCU_SORT_VOXEL_KEYS ? kVoxelSortTuneMaxPoints : kCellSortTuneMaxPoints;
+  const int32_t *cf = kind == SRCU_SORT_VOXEL_KEYS ? kVoxelSortTuneConfig : kCellSortTuneConfig;
+  ctx->tune_count[kind] = cnt;
+  for (uint32_t k = 0; k < cnt; ++k) {
+    ctx->tune_max_points[kind][k] = mp[k];
+    ctx->tune_config[kind][k] = cf[k];
+  }
+}
+
+// The voxel-key and cell-key sorts, in the launch shape the context's tuning
+// table of that sort kind gives for n_max keys.
+template <class Src>
+srcu_status launch_sort_tuned(srcu_ctx *ctx, int kind, const Src &src, uint64_t n_max,
+                              uint32_t *hist, uint32_t epoch_off, int work_slot, SortState *st,
+                              const int (&occ)[SORT_CONFIGS], int sort_id) {
+  Launch l(ctx, sort_id);
+  const int c = sort_config_for(ctx, kind, n_max);
+  const uint32_t cap = uint32_t(ctx->num_sms) * uint32_t(occ[c]);
+  const SortBuffers sb = sort_buffers(ctx);
+  cudaError_t e;
+  switch (c) {
+    case 1:
+      e = launch_sort_config<Src, 1>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
+      break;
+    case 2:
+      e = launch_sort_config<Src, 2>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
+      break;
+    case 3:
+      e = launch_sort_config<Src, 3>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
+      break;
+    default:
+      e = launch_sort_config<Src, 0>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
+  }
+  CU_TRY(e);
+  return SRCU_OK;
+}
+
 template <int NC>
 void launch_segments_nc(srcu_ctx *ctx, const float **in, uint32_t grid, const Batch &bt) {
   Columns<NC> cols;
@@ -483,8 +584,8 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
   src.y = in[1];
   src.z = in[2];
   src.bt = bt;
-  ST_TRY(launch_sort(ctx, src, n, ctx->ctl->hist_v, EP_VSORT, WK_VSORT, &ctx->ctl->vsort,
-                     ctx->occ_onesweep_v, SRCU_K_VOXEL_SORT));
+  ST_TRY(launch_sort_tuned(ctx, SRCU_SORT_VOXEL_KEYS, src, n, ctx->ctl->hist_v, EP_VSORT, WK_VSORT, &ctx->ctl->vsort,
+                           ctx->occ_sort_v, SRCU_K_VOXEL_SORT));
   const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n, SEG_TILE));
   const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(ctx->occ_seg));
   Launch l(ctx, SRCU_K_VOXEL_SEGMENTS);
@@ -526,8 +627,8 @@ srcu_status enqueue_grid(srcu_ctx *ctx, const float *x, const float *y, const fl
   src.count_dev = count_dev;
   src.voxel_keys = voxel_keys;
   src.bt = bt;
-  ST_TRY(launch_sort(ctx, src, n_max, ctx->ctl->hist_c, EP_CSORT, WK_CSORT, &ctx->ctl->csort,
-                     ctx->occ_onesweep_c, SRCU_K_CELL_SORT));
+  ST_TRY(launch_sort_tuned(ctx, SRCU_SORT_CELL_KEYS, src, n_max, ctx->ctl->hist_c, EP_CSORT, WK_CSORT,
+                           &ctx->ctl->csort, ctx->occ_sort_c, SRCU_K_CELL_SORT));
   const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, CELL_TILE));
   const uint32_t grid_c = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(ctx->occ_cells));
   {
@@ -563,8 +664,13 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
   ST_TRY(enqueue_grid(ctx, x, y, z, aos, count_dev, n_max, bt, voxel_keys));
   const uint32_t grid_n = uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals);
   Launch l(ctx, SRCU_K_NORMALS);
-  auto kernel = ctx->count_shell ? k_normals<true> : k_normals<false>;
-  kernel<<<grid_n, NM_THREADS, 0, ctx->stream>>>(
+  auto kernel = ctx->neighbor_staging
+                    ? (ctx->count_shell ? k_normals<true, false, true> : k_normals<false, false, true>)
+                    : (ctx->count_shell ? k_normals<true> : k_normals<false>);
+  const uint32_t grid = ctx->neighbor_staging
+                            ? uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals_staged)
+                            : grid_n;
+  kernel<<<grid, NM_THREADS, 0, ctx->stream>>>(
       ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint2>(ctx->ranges),
       ptr<uint64_t>(ctx->cell_key), bt, count_dev, ptr<float>(ctx->nout[0]),
       ptr<float>(ctx->nout[1]), ptr<float>(ctx->nout[2]), ptr<float>(ctx->nout[3]),
@@ -717,25 +823,23 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
       cudaMallocHost(reinterpret_cast<void **>(&ctx->head_host), offsetof(Control, n_cells)) !=
           cudaSuccess)
     return bail(SRCU_ERR_CUDA);
-  // Kernels with more than 48 KB of dynamic shared memory opt in once.
-  if (cudaFuncSetAttribute(k_sort<VoxelKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           sizeof(OnesweepSmem)) != cudaSuccess ||
-      cudaFuncSetAttribute(k_sort<CellKeySrc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           sizeof(OnesweepSmem)) != cudaSuccess ||
-      false)
+  // Kernels with more than 48 KB of dynamic shared memory opt in once; every
+  // sort launch shape, with its co-resident block count.
+  if (sort_setup<VoxelKeySrc>(ctx->occ_sort_v) != cudaSuccess ||
+      sort_setup<CellKeySrc>(ctx->occ_sort_c) != cudaSuccess)
     return bail(SRCU_ERR_CUDA);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_v, k_sort<VoxelKeySrc>,
-                                                OS_THREADS, sizeof(OnesweepSmem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_onesweep_c, k_sort<CellKeySrc>,
-                                                OS_THREADS, sizeof(OnesweepSmem));
+  builtin_sort_tuning(ctx, SRCU_SORT_VOXEL_KEYS);
+  builtin_sort_tuning(ctx, SRCU_SORT_CELL_KEYS);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals, k_normals<true>, NM_THREADS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals_staged,
+                                                k_normals<true, false, true>, NM_THREADS, 0);
+  ctx->neighbor_staging = kNeighborStaging;
   if (configure_segment_kernels() != cudaSuccess) return bail(SRCU_ERR_CUDA);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_seg, k_voxel_segments<4>, SEG_THREADS,
                                                 segment_smem_bytes(4));
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_cells, k_cells, CELL_THREADS, 0);
-  ctx->occ_onesweep_v = std::max(1, ctx->occ_onesweep_v);
-  ctx->occ_onesweep_c = std::max(1, ctx->occ_onesweep_c);
   ctx->occ_normals = std::max(1, ctx->occ_normals);
+  ctx->occ_normals_staged = std::max(1, ctx->occ_normals_staged);
   ctx->occ_seg = std::max(1, ctx->occ_seg);
   ctx->occ_cells = std::max(1, ctx->occ_cells);
   if (cudaGetLastError() != cudaSuccess) return bail(SRCU_ERR_CUDA);
@@ -782,6 +886,69 @@ srcu_status srcu_set_stream(srcu_ctx *ctx, void *cuda_stream) {
   if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
   ctx->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->own_stream;
   return SRCU_OK;
+}
+
+int srcu_sort_configs(srcu_sort_config *out, int max_entries) {
+  for (int c = 0; c < SORT_CONFIGS && c < max_entries && out; ++c) {
+    out[c].items_per_thread = uint32_t(kSortItems[c]);
+    out[c].blocks_per_sm = uint32_t(kSortMinBlocks[c]);
+    out[c].digit_bits = RADIX_BITS;
+    out[c].threads_per_block = OS_THREADS;
+  }
+  return SORT_CONFIGS;
+}
+
+srcu_status srcu_set_sort_tuning(srcu_ctx *ctx, int32_t kind, const uint64_t *max_points,
+                                 const int32_t *config, uint32_t count) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  if (kind != SRCU_SORT_VOXEL_KEYS && kind != SRCU_SORT_CELL_KEYS)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "sort kind %d is not voxel keys (0) or cell keys (1)",
+                kind);
+  if (count == 0) {
+    builtin_sort_tuning(ctx, kind);
+    return SRCU_OK;
+  }
+  if (count > SRCU_SORT_TUNING_MAX || !max_points || !config)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "a sort tuning table has 1 to %d entries",
+                SRCU_SORT_TUNING_MAX);
+  for (uint32_t k = 0; k < count; ++k) {
+    if (config[k] < 0 || config[k] >= SORT_CONFIGS)
+      return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "sort launch shape %d is not 0-%d", config[k],
+                  SORT_CONFIGS - 1);
+    if (k > 0 && max_points[k] <= max_points[k - 1])
+      return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "sort tuning sizes must ascend");
+  }
+  ctx->tune_count[kind] = count;
+  for (uint32_t k = 0; k < count; ++k) {
+    ctx->tune_max_points[kind][k] = max_points[k];
+    ctx->tune_config[kind][k] = config[k];
+  }
+  return SRCU_OK;
+}
+
+srcu_status srcu_get_sort_tuning(srcu_ctx *ctx, int32_t kind, uint64_t *max_points,
+                                 int32_t *config, uint32_t *count) {
+  if (!ctx || !count || (kind != SRCU_SORT_VOXEL_KEYS && kind != SRCU_SORT_CELL_KEYS))
+    return SRCU_ERR_INVALID_ARGUMENT;
+  const uint32_t cap = *count;
+  *count = ctx->tune_count[kind];
+  for (uint32_t k = 0; k < ctx->tune_count[kind] && k < cap; ++k) {
+    if (max_points) max_points[k] = ctx->tune_max_points[kind][k];
+    if (config) config[k] = ctx->tune_config[kind][k];
+  }
+  return SRCU_OK;
+}
+
+srcu_status srcu_set_neighbor_staging(srcu_ctx *ctx, int32_t mode) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  if (mode < -1 || mode > 1)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "neighbour staging is -1 (built-in), 0 or 1");
+  ctx->neighbor_staging = mode < 0 ? kNeighborStaging : mode;
+  return SRCU_OK;
+}
+
+int32_t srcu_get_neighbor_staging(srcu_ctx *ctx) {
+  return ctx ? ctx->neighbor_staging : -1;
 }
 
 srcu_status srcu_selftest_bounded_wait(srcu_ctx *ctx, uint32_t max_polls) {
