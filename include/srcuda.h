@@ -83,6 +83,12 @@ typedef struct srcu_cloud {
 /* VoxelAggregationMode (voxel.rs:68-76) and AttributeAggregation (voxel.rs:78-86). */
 #define SRCU_VOXEL_CENTROID 0          /* mean of every point of the voxel */
 #define SRCU_VOXEL_APPROXIMATE_FIRST 1 /* the voxel's first point (input order) */
+/* Centroid + Average on a cloud whose only fields are x, y, z: the reference's
+ * plain-xyz fast path (filter_cpu_xyz_centroid_fast, voxel.rs:550-636) --
+ * f32 sums in input order, (sum * (1 / count)) in f32, voxels in the order of
+ * their first point.  srcu_voxel_centroid and srcu_voxel_normals only, with
+ * n_attrs == 0 and SRCU_ATTRIBUTE_AVERAGE. */
+#define SRCU_VOXEL_CENTROID_XYZ 2
 #define SRCU_ATTRIBUTE_AVERAGE 0
 #define SRCU_ATTRIBUTE_FIRST 1
 
@@ -103,7 +109,8 @@ typedef struct srcu_voxel_params {
 
 /* Voxel output.  Each column needs capacity >= input n (the voxel count is
  * never larger).  Voxels are emitted in ascending (ix, iy, iz) order, the
- * reference's output order for point_xyzi (voxel.rs:522-536). */
+ * reference's output order for point_xyzi (voxel.rs:522-536), or in
+ * first-seen order under SRCU_VOXEL_CENTROID_XYZ. */
 typedef struct srcu_voxel_out {
   float *x;
   float *y;

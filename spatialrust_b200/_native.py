@@ -81,6 +81,7 @@ class SrcuCloud(ctypes.Structure):
 
 SRCU_VOXEL_CENTROID = 0
 SRCU_VOXEL_APPROXIMATE_FIRST = 1
+SRCU_VOXEL_CENTROID_XYZ = 2  # the reference's plain-xyz fast path (voxel.rs:550-636)
 SRCU_ATTRIBUTE_AVERAGE = 0
 SRCU_ATTRIBUTE_FIRST = 1
 
@@ -495,7 +496,7 @@ class Context:
 
     def voxel_centroid(self, x, y, z, attrs=(), leaf: float = 1.0, origin=None,
                        want_keys: bool = False, approximate: bool = False,
-                       attribute_first: bool = False):
+                       attribute_first: bool = False, plain_xyz: bool = False):
         """Returns (columns [x, y, z, attrs...], keys (V,3) int64 or None, counts) as numpy.
         approximate / attribute_first select the reference's ApproximateFirst mode
         and First attribute policy (srcu_voxel_params)."""
@@ -510,7 +511,7 @@ class Context:
         vout = SrcuVoxelOut(outs[0].ctypes.data, outs[1].ctypes.data, outs[2].ctypes.data,
                             ctypes.cast(attr_out, ctypes.c_void_p),
                             keys.ctypes.data if keys is not None else 0, counts.ctypes.data, 0)
-        vp = _voxel_params(leaf, origin, approximate, attribute_first)
+        vp = _voxel_params(leaf, origin, approximate, attribute_first, plain_xyz)
         nv = ctypes.c_uint64(0)
         self._check(self._lib.srcu_voxel_centroid(self._h, ctypes.byref(cloud), ctypes.byref(vp),
                                                   ctypes.byref(vout), ctypes.byref(nv)))
@@ -647,7 +648,7 @@ class Context:
 
     def voxel_normals(self, x, y, z, attrs=(), leaf: float = 1.0, origin=None, radius: float = 0.5,
                       min_neighbors: int = 3, viewpoint=None, include_self: bool = False,
-                      want_keys: bool = False):
+                      want_keys: bool = False, plain_xyz: bool = False):
         """Voxel centroids then radius normals on them (MvpPipeline chain), numpy outputs."""
         keep = _Keep()
         cloud = make_cloud(x, y, z, attrs, keep)
@@ -663,7 +664,7 @@ class Context:
         nouts = [np.empty(max(n, 1), np.float32) for _ in range(4)]
         ncounts = np.empty(max(n, 1), np.uint32)
         nout = SrcuNormalOut(*[o.ctypes.data for o in nouts], ncounts.ctypes.data, 0)
-        vp = _voxel_params(leaf, origin)
+        vp = _voxel_params(leaf, origin, plain_xyz=plain_xyz)
         np_ = _normal_params(radius, min_neighbors, viewpoint, include_self)
         nv = ctypes.c_uint64(0)
         stats = SrcuNormalStats()
@@ -950,8 +951,9 @@ class Server:
 
 
 def _voxel_params(leaf, origin, approximate: bool = False,
-                  attribute_first: bool = False) -> SrcuVoxelParams:
-    mode = SRCU_VOXEL_APPROXIMATE_FIRST if approximate else SRCU_VOXEL_CENTROID
+                  attribute_first: bool = False, plain_xyz: bool = False) -> SrcuVoxelParams:
+    mode = (SRCU_VOXEL_APPROXIMATE_FIRST if approximate
+            else SRCU_VOXEL_CENTROID_XYZ if plain_xyz else SRCU_VOXEL_CENTROID)
     policy = SRCU_ATTRIBUTE_FIRST if attribute_first else SRCU_ATTRIBUTE_AVERAGE
     if origin is None:
         return SrcuVoxelParams(float(leaf), 0, c_float3(0, 0, 0), mode, policy)

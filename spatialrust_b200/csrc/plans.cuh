@@ -164,12 +164,14 @@ constexpr uint32_t EP_VSORT = 0;     // 8 passes
 constexpr uint32_t EP_VSEG = 8;
 constexpr uint32_t EP_CSORT = 16;    // 8 passes
 constexpr uint32_t EP_CELLS = 24;
+constexpr uint32_t EP_ORDER = 32;    // first-seen order sort of the plain-xyz path, 4 passes
 // Work-counter slots.
 constexpr int WK_VSORT = 0;   // 8 slots
 constexpr int WK_VSEG = 8;
 constexpr int WK_CSORT = 16;  // 8 slots
 constexpr int WK_CELLS = 24;
 constexpr int WK_NORMALS = 25;
+constexpr int WK_ORDER = 32;  // 4 slots
 
 __device__ __forceinline__ int64_t rs_sat_i64(float t) {
   if (isnan(t)) return 0;

@@ -57,6 +57,10 @@ struct srcu_ctx {
   DevBuf keys[2], vals[2], lb_sort, lb_seg, lb_cells;
   // voxel outputs: x, y, z, attrs..., packed keys, counts, unpacked keys
   DevBuf vout[MAX_COLS], vkeys, vcounts, vkeys3, vaos;
+  // plain-xyz path: gathered voxels (x, y, z, counts, keys) and first points
+  DevBuf xyz_tmp;
+  bool xyz_order = false;  // this chain emits voxels in first-seen order (plain xyz)
+  int occ_sort_order = 1;
   DevBuf in_aos;  // AoS (x, y, z, first attribute) copy of the chain's input
   // radius grid
   DevBuf pts, pt_cell, cell_key, cell_start, table, ranges;
@@ -564,6 +568,46 @@ void launch_segments_nc(srcu_ctx *ctx, const float **in, uint32_t grid, const Ba
       ptr<float4>(ctx->vaos), bt, ctx->agg_all);
 }
 
+// The plain-xyz path after the segment kernel: f32 centroids in input order,
+// then the voxels (columns, counts, keys, AoS copy) in first-seen order.
+srcu_status enqueue_first_seen(srcu_ctx *ctx, const float **in, uint64_t n) {
+  ST_TRY(ensure(ctx, ctx->xyz_tmp, std::max<uint64_t>(n, 1) * 28));
+  float *tx = ptr<float>(ctx->xyz_tmp);
+  float *ty = tx + n;
+  float *tz = ty + n;
+  uint32_t *tc = reinterpret_cast<uint32_t *>(tz + n);
+  uint64_t *tk = reinterpret_cast<uint64_t *>(tc + n);  // byte offset 16 n: 8-aligned
+  uint32_t *first = reinterpret_cast<uint32_t *>(tk + n);
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, 256), ctx->num_sms * 8));
+  {
+    Launch l(ctx, SRCU_K_VOXEL_SEGMENTS);
+    k_voxel_xyz_f32<<<grid, 256, 0, ctx->stream>>>(
+        ctx->ctl, sort_buffers(ctx), &ctx->ctl->vsort, in[0], in[1], in[2],
+        ptr<uint64_t>(ctx->vkeys), ptr<uint32_t>(ctx->vcounts), ptr<float>(ctx->vout[0]),
+        ptr<float>(ctx->vout[1]), ptr<float>(ctx->vout[2]), first);
+    CU_TRY(cudaGetLastError());
+  }
+  // The voxel sort is consumed: its histogram is reused, zeroed, by the order
+  // sort, whose state is the cell sort's (the cell sort, if any, comes after).
+  CU_TRY(cudaMemsetAsync(ctx->ctl->hist_v, 0, sizeof(ctx->ctl->hist_v), ctx->stream));
+  FirstSeenSrc src;
+  src.first = first;
+  src.bits = n > 1 ? bit_width_u64(n - 1) : 0u;
+  ST_TRY(launch_sort(ctx, src, n, ctx->ctl->hist_v, EP_ORDER, WK_ORDER, &ctx->ctl->csort,
+                     ctx->occ_sort_order, SRCU_K_VOXEL_SORT));
+  Launch l(ctx, SRCU_K_VOXEL_SEGMENTS);
+  k_voxel_first_seen_gather<<<grid, 256, 0, ctx->stream>>>(
+      ctx->ctl, sort_buffers(ctx), &ctx->ctl->csort, ptr<float>(ctx->vout[0]),
+      ptr<float>(ctx->vout[1]), ptr<float>(ctx->vout[2]), ptr<uint32_t>(ctx->vcounts),
+      ptr<uint64_t>(ctx->vkeys), tx, ty, tz, tc, tk);
+  k_voxel_copy_back<<<grid, 256, 0, ctx->stream>>>(
+      ctx->ctl, tx, ty, tz, tc, tk, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
+      ptr<float>(ctx->vout[2]), ptr<uint32_t>(ctx->vcounts), ptr<uint64_t>(ctx->vkeys),
+      ptr<float4>(ctx->vaos));
+  CU_TRY(cudaGetLastError());
+  return SRCU_OK;
+}
+
 // Voxel stage: bounds -> plan -> sort -> fused segment/centroid reduction.
 srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t n,
                           const Batch &bt) {
@@ -606,6 +650,7 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
     k_voxel_offsets<<<ceil_div(bt.clouds + 1, 128), 128, 0, ctx->stream>>>(
         ctx->ctl, ptr<uint64_t>(ctx->vkeys), bt);
   CU_TRY(cudaGetLastError());
+  if (ctx->xyz_order && bt.clouds == 1) ST_TRY(enqueue_first_seen(ctx, in, n));
   return SRCU_OK;
 }
 
@@ -691,6 +736,7 @@ void begin_chain(srcu_ctx *ctx, uint64_t n, const Batch &bt, int single,
     ctx->agg_all = to_dev(vp).agg;
     ctx->count_shell = np && np->count_shell;
   }
+  ctx->xyz_order = single && vp && vp->mode == SRCU_VOXEL_CENTROID_XYZ;
 }
 
 srcu_status read_control(srcu_ctx *ctx) {
@@ -723,10 +769,23 @@ srcu_status copy_out(srcu_ctx *ctx, void *dst, const void *src, size_t bytes, in
   return SRCU_OK;
 }
 
-srcu_status check_voxel_params(srcu_ctx *ctx, const srcu_voxel_params *vp) {
+// plain_cloud: the one cloud of a srcu_voxel_centroid / srcu_voxel_normals
+// call, the only calls that take SRCU_VOXEL_CENTROID_XYZ.
+srcu_status check_voxel_params(srcu_ctx *ctx, const srcu_voxel_params *vp,
+                               const srcu_cloud *plain_cloud = nullptr) {
   if (!vp) return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "voxel params are NULL");
   if (vp->leaf_size <= 0.0f)  // voxel.rs:260-264 (a NaN leaf is not rejected there either)
     return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "leaf_size must be greater than zero");
+  if (vp->mode == SRCU_VOXEL_CENTROID_XYZ) {
+    if (!plain_cloud)
+      return fail(ctx, SRCU_ERR_INVALID_ARGUMENT,
+                  "the plain-xyz voxel mode runs through srcu_voxel_centroid and "
+                  "srcu_voxel_normals only");
+    if (plain_cloud->n_attrs != 0 || vp->attribute_policy != SRCU_ATTRIBUTE_AVERAGE)
+      return fail(ctx, SRCU_ERR_INVALID_ARGUMENT,
+                  "the plain-xyz voxel mode takes clouds of x, y, z only, Average policy");
+    return SRCU_OK;
+  }
   if ((vp->mode != SRCU_VOXEL_CENTROID && vp->mode != SRCU_VOXEL_APPROXIMATE_FIRST) ||
       (vp->attribute_policy != SRCU_ATTRIBUTE_AVERAGE && vp->attribute_policy != SRCU_ATTRIBUTE_FIRST))
     return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "unknown voxel aggregation mode %d / policy %d",
@@ -826,7 +885,8 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
   // Kernels with more than 48 KB of dynamic shared memory opt in once; every
   // sort launch shape, with its co-resident block count.
   if (sort_setup<VoxelKeySrc>(ctx->occ_sort_v) != cudaSuccess ||
-      sort_setup<CellKeySrc>(ctx->occ_sort_c) != cudaSuccess)
+      sort_setup<CellKeySrc>(ctx->occ_sort_c) != cudaSuccess ||
+      sort_config_setup<FirstSeenSrc, 0>(&ctx->occ_sort_order) != cudaSuccess)
     return bail(SRCU_ERR_CUDA);
   builtin_sort_tuning(ctx, SRCU_SORT_VOXEL_KEYS);
   builtin_sort_tuning(ctx, SRCU_SORT_CELL_KEYS);
@@ -858,7 +918,7 @@ void srcu_destroy(srcu_ctx *ctx) {
                    &ctx->pts, &ctx->pt_cell, &ctx->cell_key, &ctx->cell_start, &ctx->table, &ctx->ranges,
                    &ctx->ncounts, &ctx->parent, &ctx->cov6, &ctx->stage_block,
                    &ctx->rs_hyp, &ctx->rs_planes, &ctx->rs_valid, &ctx->rs_counts,
-                   &ctx->rs_partials, &ctx->rs_mask};
+                   &ctx->rs_partials, &ctx->rs_mask, &ctx->xyz_tmp};
   for (DevBuf *b : all) release(ctx, *b);
   for (auto &b : ctx->in) release(ctx, b);
   for (auto &b : ctx->vout) release(ctx, b);
@@ -979,7 +1039,7 @@ srcu_status srcu_voxel_centroid(srcu_ctx *ctx, const srcu_cloud *cloud,
   if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
   if (out_voxels) *out_voxels = 0;
   ST_TRY(check_cloud(ctx, cloud));
-  ST_TRY(check_voxel_params(ctx, params));
+  ST_TRY(check_voxel_params(ctx, params, cloud));
   CU_TRY(cudaSetDevice(ctx->device));
   const uint64_t n = cloud->n;
   if (n == 0) return SRCU_OK;  // voxel.rs:257-259: empty input is returned unchanged
@@ -1151,7 +1211,7 @@ srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
   if (out_voxels) *out_voxels = 0;
   if (stats) memset(stats, 0, sizeof(*stats));
   ST_TRY(check_cloud(ctx, cloud));
-  ST_TRY(check_voxel_params(ctx, vparams));
+  ST_TRY(check_voxel_params(ctx, vparams, cloud));
   ST_TRY(check_normal_params(ctx, nparams));
   CU_TRY(cudaSetDevice(ctx->device));
   const uint64_t n = cloud->n;

@@ -518,6 +518,117 @@ inline cudaError_t configure_segment_kernels() {
   return e;
 }
 
+// ---- the reference's plain-xyz fast path --------------------------------------
+// filter_cpu_xyz_centroid_fast (crates/spatialrust-filtering/src/voxel.rs:550-636)
+// runs for clouds whose only fields are x, y, z: per voxel it sums x, y, z in
+// f32 in input order, emits sum * (1 / count) in f32, and emits the voxels in
+// the order of their first point.  After the segment kernel (same voxels, same
+// counts, key order), k_voxel_xyz_f32 recomputes those sums -- the stable sort
+// keeps each voxel's points in input order -- and records each voxel's first
+// point; a sort of the voxels by first point (FirstSeenSrc) and a gather then
+// put them in first-seen order.
+
+// One thread per voxel start among the sorted items.
+__global__ void k_voxel_xyz_f32(Control *ctl, SortBuffers sort, const SortState *sort_state,
+                                const float *x, const float *y, const float *z,
+                                const uint64_t *vkeys, const uint32_t *vcounts, float *ox,
+                                float *oy, float *oz, uint32_t *first) {
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint32_t n = uint32_t(ctl->n_points);
+  const uint32_t nv = uint32_t(ctl->n_voxels);
+  const SortedView sv = sorted_view(sort, *sort_state);
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+    const uint64_t key = sv.key(m);
+    if (m > 0 && sv.key(m - 1) == key) continue;
+    uint32_t lo = 0, hi = nv;  // the voxel of this key among the key-ordered voxels
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (vkeys[mid] < key) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo >= nv || vkeys[lo] != key || vcounts[lo] == 0 || vcounts[lo] > n - m) {
+      atomicOr(&ctl->status, ST_INTERNAL);  // cannot happen for a consistent chain
+      continue;
+    }
+    const uint32_t cnt = vcounts[lo];
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    uint32_t i0 = 0;
+    bool ok = true;
+    for (uint32_t q = 0; q < cnt; ++q) {
+      const uint32_t i = sv.val(m + q);
+      if (i >= n) {
+        ok = false;
+        break;
+      }
+      if (q == 0) i0 = i;
+      sx = __fadd_rn(sx, x[i]);
+      sy = __fadd_rn(sy, y[i]);
+      sz = __fadd_rn(sz, z[i]);
+    }
+    if (!ok) {
+      atomicOr(&ctl->status, ST_INTERNAL);
+      continue;
+    }
+    const float inv = 1.0f / float(cnt);  // IEEE division: the library is built without fast math
+    ox[lo] = __fmul_rn(sx, inv);
+    oy[lo] = __fmul_rn(sy, inv);
+    oz[lo] = __fmul_rn(sz, inv);
+    first[lo] = i0;
+  }
+}
+
+// Sort key of the first-seen order: each voxel's first point index.
+struct FirstSeenSrc {
+  const uint32_t *first;
+  uint32_t bits;  // bits of the largest point index
+  __device__ __forceinline__ void prepare(const Control *) {}
+  __device__ __forceinline__ uint32_t count(const Control *ctl) const {
+    return uint32_t(ctl->n_voxels);
+  }
+  __device__ __forceinline__ uint32_t key_bits() const { return bits; }
+  __device__ __forceinline__ uint64_t key(uint32_t v) const { return first[v]; }
+};
+
+// Voxel j of the first-seen order <- voxel val(j) of the key order.
+__global__ void k_voxel_first_seen_gather(Control *ctl, SortBuffers sort, const SortState *order,
+                                          const float *ix, const float *iy, const float *iz,
+                                          const uint32_t *icnt, const uint64_t *ikey, float *ox,
+                                          float *oy, float *oz, uint32_t *ocnt, uint64_t *okey) {
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint32_t nv = uint32_t(ctl->n_voxels);
+  const SortedView sv = sorted_view(sort, *order);
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nv; j += gridDim.x * blockDim.x) {
+    const uint32_t v = sv.val(j);
+    if (v >= nv) {
+      atomicOr(&ctl->status, ST_INTERNAL);
+      continue;
+    }
+    ox[j] = ix[v];
+    oy[j] = iy[v];
+    oz[j] = iz[v];
+    ocnt[j] = icnt[v];
+    okey[j] = ikey[v];
+  }
+}
+
+// The gathered voxels back into the chain's voxel buffers (and the AoS copy
+// the normals stage reads).
+__global__ void k_voxel_copy_back(const Control *ctl, const float *ix, const float *iy,
+                                  const float *iz, const uint32_t *icnt, const uint64_t *ikey,
+                                  float *ox, float *oy, float *oz, uint32_t *ocnt, uint64_t *okey,
+                                  float4 *aos) {
+  if (ld_relaxed_u32(&ctl->status)) return;
+  const uint32_t nv = uint32_t(ctl->n_voxels);
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nv; j += gridDim.x * blockDim.x) {
+    ox[j] = ix[j];
+    oy[j] = iy[j];
+    oz[j] = iz[j];
+    ocnt[j] = icnt[j];
+    okey[j] = ikey[j];
+    if (aos) aos[j] = make_float4(ix[j], iy[j], iz[j], 0.0f);
+  }
+}
+
 // Unpacks packed voxel keys into the reference's (ix, iy, iz) int64 triples.
 __global__ void k_unpack_voxel_keys(const Control *ctl, const uint64_t *packed, int64_t *out,
                                     Batch bt) {

@@ -101,6 +101,23 @@ def narrow(values: np.ndarray, dtype: DType) -> np.ndarray:
     return r.astype(dtype.numpy)
 
 
+def is_plain_xyz_f32_schema(schema) -> bool:
+    """voxel.rs:670-688: exactly three fields, F32 or F16, the three positions."""
+    fields = list(schema.fields)
+    return (len(fields) == 3 and all(f.dtype in (DType.F32, DType.F16) for f in fields)
+            and {f.semantic for f in fields} == set(POSITION_SEMANTICS))
+
+
+def uses_plain_xyz_path(schema, config: "VoxelGridDownsampleConfig") -> bool:
+    """Whether the reference's CPU dispatch (voxel.rs:314-330 -> 474-485) takes
+    filter_cpu_xyz_centroid_fast: Centroid + Average on a plain-xyz cloud.
+    The CUDA arm follows it (SRCU_VOXEL_CENTROID_XYZ): f32 sums, first-seen
+    voxel order."""
+    return (config.mode == VoxelAggregationMode.Centroid
+            and config.attribute_policy == AttributeAggregation.Average
+            and is_plain_xyz_f32_schema(schema))
+
+
 class VoxelGridDownsample:
     """Voxel-grid downsampling filter (voxel.rs:185-248)."""
 
@@ -143,7 +160,8 @@ class VoxelGridDownsample:
         cols, _, _ = ctx.voxel_centroid(
             x, y, z, attrs, leaf=cfg.leaf_size, origin=cfg.origin,
             approximate=cfg.mode == VoxelAggregationMode.ApproximateFirst,
-            attribute_first=cfg.attribute_policy == AttributeAggregation.First)
+            attribute_first=cfg.attribute_policy == AttributeAggregation.First,
+            plain_xyz=uses_plain_xyz_path(input.schema, cfg))
         out = {}
         pos_names = {f.semantic: f.name for f in input.schema.fields if f.semantic in POSITION_SEMANTICS}
         out[pos_names[FieldSemantic.PositionX]] = cols[0]

@@ -20,7 +20,8 @@ from .core import (POSITION_SEMANTICS, Auto, ExecutionPolicy, ExecutionReceipt, 
                    InvalidArgument, PointCloud, TransferDirection)
 from .features import NormalEstimationConfig, NormalEstimator, build_output_cloud
 from .filtering import (AttributeAggregation, VoxelAggregationMode, VoxelGridDownsample,
-                        VoxelGridDownsampleConfig, _widen, narrow, resolve_cuda_policy)
+                        VoxelGridDownsampleConfig, _widen, narrow, resolve_cuda_policy,
+                        uses_plain_xyz_path)
 from .segmentation import (EuclideanClusterConfig, EuclideanClusterExtractor,
                            EuclideanClusterResult, RansacPlaneConfig, RansacPlaneSegmentation,
                            RansacPlaneSegmenter)
@@ -111,7 +112,7 @@ class MvpPipeline:
         out = _native.shared_context(self._device).voxel_normals(
             x, y, z, attrs, leaf=c.voxel.leaf_size, origin=c.voxel.origin,
             radius=normal_config.search_radius, min_neighbors=normal_config.min_neighbors,
-            viewpoint=normal_config.viewpoint)
+            viewpoint=normal_config.viewpoint, plain_xyz=uses_plain_xyz_path(input.schema, c.voxel))
         cols = out["columns"]
         pos = {f.semantic: f.name for f in input.schema.fields if f.semantic in POSITION_SEMANTICS}
         vcols = {pos[FieldSemantic.PositionX]: cols[0], pos[FieldSemantic.PositionY]: cols[1],

@@ -102,3 +102,15 @@ def test_c0_occupancy_matches_expectation(oracle_lib):
     # 25^3 voxels, 6.4 points each on average: ~15.6k occupied
     assert 15_500 < len(r.x) <= 15_625
     assert int(r.counts.sum()) == 100_000
+
+
+def test_plain_xyz_dispatch_follows_the_reference():
+    from spatialrust_b200 import _native
+    from spatialrust_b200.filtering import uses_plain_xyz_path
+    cfg = sr.VoxelGridDownsampleConfig.centroid(0.5)
+    assert uses_plain_xyz_path(sr.StandardSchemas.point_xyz(), cfg)
+    assert not uses_plain_xyz_path(sr.StandardSchemas.point_xyzi(), cfg)
+    assert not uses_plain_xyz_path(sr.StandardSchemas.point_xyz(),
+                                   sr.VoxelGridDownsampleConfig.approximate(0.5))
+    assert _native._voxel_params(0.5, None, plain_xyz=True).mode == _native.SRCU_VOXEL_CENTROID_XYZ
+    assert _native._voxel_params(0.5, None).mode == _native.SRCU_VOXEL_CENTROID
