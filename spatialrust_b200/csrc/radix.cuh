@@ -51,6 +51,7 @@ struct OnesweepSmemT {
     uint32_t hist[HIST_COPIES][MAX_DIGITS][RADIX_BINS];
   } u;
   uint32_t whist[OS_WARPS][RADIX_BINS];
+  uint32_t match[OS_WARPS][RADIX_BINS];  // per-warp peer masks, zero between uses
   uint32_t digit_start[RADIX_BINS];
   uint32_t tile_excl[RADIX_BINS];
   uint32_t gbase[RADIX_BINS];
@@ -127,19 +128,6 @@ __device__ __forceinline__ void grid_barrier(SortState *st, uint32_t *status) {
   __syncthreads();
 }
 
-// Lanes holding the same 8-bit digit, from eight ballots (a fixed-cost
-// replacement for __match_any_sync, about twice as fast on sm_100).
-__device__ __forceinline__ uint32_t digit_peers(uint32_t d, uint32_t valid_mask) {
-  uint32_t peers = valid_mask;
-#pragma unroll
-  for (int b = 0; b < RADIX_BITS; ++b) {
-    const uint32_t bit = (d >> b) & 1u;
-    const uint32_t bb = __ballot_sync(FULL_MASK, bit);
-    peers &= bit ? bb : ~bb;
-  }
-  return peers;
-}
-
 template <class Src, int ITEMS = OS_ITEMS, int MINB = 2>
 __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl, uint32_t *hist,
                                                         SortBuffers buf, uint32_t epoch_off,
@@ -161,6 +149,7 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
   // ---- phase 1: digit histograms ----------------------------------------
   for (uint32_t i = t; i < HIST_COPIES * MAX_DIGITS * RADIX_BINS; i += OS_THREADS)
     (&sm.u.hist[0][0][0])[i] = 0;
+  for (uint32_t i = t; i < OS_WARPS * RADIX_BINS; i += OS_THREADS) (&sm.match[0][0])[i] = 0;
   __syncthreads();
   {
     // The keys are computed once, here, and kept in the ping-pong buffer that
@@ -254,13 +243,25 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
         }
       }
       // Warp-private multi-split: rank each item among earlier items of the
-      // warp with the same digit.  One leader per digit per step updates the
-      // warp's counter, so no atomics are needed.
+      // warp with the same digit.  The lanes sharing a digit (its peers) come
+      // from one shared-memory atomicOr per lane into the warp's mask for that
+      // digit, or, when every valid lane holds the same digit (the high digits
+      // of spatially coherent keys), from the valid mask alone.  One leader per
+      // digit per step updates the warp's counter and clears the mask.
 #pragma unroll
       for (int i = 0; i < ITEMS; ++i) {
         const bool valid = (wbase + uint32_t(i) * 32u + lane) < n;
         const uint32_t d = uint32_t(k[i] >> shift) & 0xffu;
-        const uint32_t peers = digit_peers(d, __ballot_sync(FULL_MASK, valid));
+        const uint32_t vmask = __ballot_sync(FULL_MASK, valid);
+        const uint32_t d0 = __shfl_sync(FULL_MASK, d, 0);
+        const bool uniform = __all_sync(FULL_MASK, !valid || d == d0);
+        uint32_t peers = vmask;
+        if (!uniform) {  // peers from shared-memory masks: one atomic per lane
+          if (valid) atomicOr(&sm.match[warp][d], 1u << lane);
+          __syncwarp();
+          peers = valid ? sm.match[warp][d] : 0u;
+          __syncwarp();
+        }
         uint32_t prev = 0;
         uint32_t leader = 0;
         if (valid) {
@@ -268,6 +269,7 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
           if (lane == leader) {
             prev = sm.whist[warp][d];
             sm.whist[warp][d] = prev + uint32_t(__popc(peers));
+            if (!uniform) sm.match[warp][d] = 0u;
           }
         }
         prev = __shfl_sync(FULL_MASK, prev, leader);

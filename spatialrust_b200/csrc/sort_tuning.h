@@ -12,77 +12,77 @@
 //
 // Measured sort ms (georeferenced scan, leaf 0.1, radius 0.5; L2 flushed before every chain):
 //   voxel-key sort       keys    16x2     8x3    12x3     8x4
-//                      65536  0.0609  0.0472  0.0557  0.0470
-//                      92682  0.0623  0.0480  0.0556  0.0485
-//                     131072  0.0624  0.0498  0.0578  0.0498
-//                     185364  0.0642  0.0516  0.0587  0.0520
-//                     262144  0.0664  0.0536  0.0603  0.0539
-//                     370728  0.0666  0.0584  0.0629  0.0586
-//                     524288  0.0696  0.0642  0.0683  0.0642
-//                     741455  0.0764  0.0779  0.0738  0.0772
-//                    1048576  0.0827  0.0918  0.0918  0.1071
-//                    1482910  0.1100  0.1150  0.1070  0.1274
-//                    2097152  0.1308  0.1404  0.1407  0.1609
-//                    2965821  0.1739  0.1799  0.1659  0.1998
-//                    4194304  0.2338  0.2427  0.2259  0.2647
-//                    5931642  0.3242  0.3285  0.3041  0.3499
-//                    8388608  0.4434  0.4447  0.4117  0.4638
-//                   11863283  0.6092  0.6128  0.5608  0.6309
-//                   16777216  0.8398  0.8483  0.7703  0.8710
-//                   23726566  1.1608  1.1787  1.0690  1.2085
-//                   33554432  1.6223  1.6466  1.4860  1.6870
+//                      65536  0.0589  0.0453  0.0537  0.0476
+//                      92682  0.0597  0.0463  0.0535  0.0490
+//                     131072  0.0605  0.0481  0.0546  0.0500
+//                     185364  0.0622  0.0501  0.0562  0.0520
+//                     262144  0.0643  0.0519  0.0582  0.0542
+//                     370728  0.0645  0.0563  0.0599  0.0586
+//                     524288  0.0667  0.0623  0.0644  0.0644
+//                     741455  0.0723  0.0724  0.0705  0.0745
+//                    1048576  0.0790  0.0851  0.0824  0.0908
+//                    1482910  0.1052  0.1067  0.0988  0.1096
+//                    2097152  0.1276  0.1289  0.1265  0.1356
+//                    2965821  0.1670  0.1673  0.1544  0.1708
+//                    4194304  0.2251  0.2272  0.2059  0.2251
+//                    5931642  0.3117  0.3083  0.2784  0.3038
+//                    8388608  0.4236  0.4195  0.3752  0.4048
+//                   11863283  0.5822  0.5777  0.5129  0.5484
+//                   16777216  0.8046  0.8001  0.7058  0.7505
+//                   23726566  1.1152  1.1109  0.9771  1.0369
+//                   33554432  1.5592  1.5515  1.3612  1.4412
 //   cell-key sort       keys    16x2     8x3    12x3     8x4
-//                      65325  0.0534  0.0403  0.0455  0.0412
-//                      92252  0.0542  0.0410  0.0463  0.0416
-//                     130231  0.0551  0.0417  0.0478  0.0428
-//                     183630  0.0551  0.0431  0.0480  0.0432
-//                     258683  0.0562  0.0451  0.0495  0.0451
-//                     364390  0.0564  0.0475  0.0502  0.0488
-//                     511610  0.0590  0.0533  0.0555  0.0535
-//                     716353  0.0639  0.0636  0.0603  0.0640
-//                     998975  0.0691  0.0737  0.0744  0.0872
-//                    1386254  0.0910  0.0917  0.0825  0.0983
-//                    1913842  0.1088  0.1083  0.1124  0.1275
-//                    2610072  0.1358  0.1384  0.1314  0.1508
-//                    3512442  0.1664  0.1721  0.1646  0.1925
-//                    4648599  0.2132  0.2152  0.2011  0.2373
-//                    6011810  0.2763  0.2685  0.2482  0.2890
-//                    7569816  0.3437  0.3297  0.3032  0.3468
-//                    8875163  0.3965  0.3793  0.3492  0.3952
-//                   10515699  0.4595  0.4416  0.4036  0.4590
-//                   12236880  0.5264  0.5067  0.4606  0.5245
+//                      65325  0.0516  0.0391  0.0456  0.0410
+//                      92252  0.0519  0.0397  0.0468  0.0415
+//                     130231  0.0533  0.0409  0.0474  0.0428
+//                     183630  0.0535  0.0412  0.0479  0.0433
+//                     258683  0.0543  0.0435  0.0491  0.0453
+//                     364390  0.0545  0.0468  0.0502  0.0490
+//                     511610  0.0572  0.0522  0.0550  0.0546
+//                     716353  0.0617  0.0597  0.0596  0.0614
+//                     998975  0.0677  0.0699  0.0680  0.0731
+//                    1386254  0.0865  0.0856  0.0791  0.0872
+//                    1913842  0.1053  0.1027  0.1027  0.1069
+//                    2610072  0.1304  0.1308  0.1215  0.1276
+//                    3512442  0.1620  0.1636  0.1532  0.1617
+//                    4648599  0.2073  0.2054  0.1897  0.2028
+//                    6011810  0.2662  0.2595  0.2391  0.2541
+//                    7569816  0.3320  0.3200  0.2931  0.3076
+//                    8875163  0.3815  0.3684  0.3341  0.3505
+//                   10515699  0.4414  0.4255  0.3838  0.4019
+//                   12236880  0.5016  0.4851  0.4356  0.4555
 // Normals kernel ms per chain, neighbour gather through L1 / staged:
 //       65536    0.023 /  0.026
 //       92682    0.027 /  0.032
-//      131072    0.033 /  0.038
-//      185364    0.050 /  0.063
-//      262144    0.064 /  0.079
-//      370728    0.092 /  0.113
+//      131072    0.032 /  0.039
+//      185364    0.051 /  0.062
+//      262144    0.064 /  0.078
+//      370728    0.091 /  0.112
 //      524288    0.118 /  0.140
-//      741455    0.147 /  0.171
-//     1048576    0.194 /  0.213
-//     1482910    0.288 /  0.302
-//     2097152    0.411 /  0.442
-//     2965821    0.644 /  0.669
-//     4194304    1.037 /  1.067
-//     5931642    1.664 /  1.722
-//     8388608    2.382 /  2.416
-//    11863283    3.477 /  3.478
-//    16777216    4.445 /  4.489
-//    23726566    5.981 /  5.908
-//    33554432    7.549 /  7.403
+//      741455    0.145 /  0.168
+//     1048576    0.195 /  0.212
+//     1482910    0.286 /  0.301
+//     2097152    0.410 /  0.448
+//     2965821    0.641 /  0.672
+//     4194304    1.039 /  1.055
+//     5931642    1.666 /  1.713
+//     8388608    2.388 /  2.436
+//    11863283    3.489 /  3.480
+//    16777216    4.426 /  4.486
+//    23726566    5.936 /  5.917
+//    33554432    7.543 /  7.378
 #pragma once
 
 #include <cstdint>
 
 namespace srcu {
 
-constexpr uint32_t kVoxelSortTuneCount = 6;
-constexpr uint64_t kVoxelSortTuneMaxPoints[] = {623486ull, 881743ull, 1246973ull, 1763487ull, 2493948ull, UINT64_MAX};
-constexpr int32_t kVoxelSortTuneConfig[] = {3, 2, 0, 2, 0, 2};
-constexpr uint32_t kCellSortTuneCount = 6;
-constexpr uint64_t kCellSortTuneMaxPoints[] = {605386ull, 845942ull, 1176789ull, 1628825ull, 2235009ull, UINT64_MAX};
-constexpr int32_t kCellSortTuneConfig[] = {1, 2, 0, 2, 1, 2};
+constexpr uint32_t kVoxelSortTuneCount = 4;
+constexpr uint64_t kVoxelSortTuneMaxPoints[] = {623486ull, 881743ull, 1246973ull, UINT64_MAX};
+constexpr int32_t kVoxelSortTuneConfig[] = {1, 2, 0, 2};
+constexpr uint32_t kCellSortTuneCount = 3;
+constexpr uint64_t kCellSortTuneMaxPoints[] = {845942ull, 1176789ull, UINT64_MAX};
+constexpr int32_t kCellSortTuneConfig[] = {1, 0, 2};
 // 1: the normals kernel gathers candidates through shared memory (bulk copies)
 constexpr int32_t kNeighborStaging = 0;
 
