@@ -43,6 +43,7 @@ WORKLOAD = "georef_scan_2M_xyzi: voxel leaf 0.1 + leaf 0.5, each -> radius norma
 METRIC = "M points/s voxel+normals (2M georeferenced point_xyzi, leaf 0.1 & 0.5, r 0.5)"
 UNIT = "Mpoints/s"
 L2_FLUSH_BYTES = 256 << 20
+PROFILE_PASSES = 5  # untimed per-group profile passes (median)
 # DRAM bytes (read + write) per launch of the dominant kernel group on this
 # workload, mean over the leaf-0.1 and leaf-0.5 chains, from one ncu capture
 # (profiles/k_normals_georef2M_leaf0.1.md); ncu cannot run inside the bench.
@@ -359,28 +360,31 @@ def run_gpu(args):
         nstats.append(c.frame_check()[1])
         infos.append(c.chain_info())
 
-    # untimed profile pass: which kernel group dominates, with the two chains
-    # run one after the other so every group's time is its own
+    # untimed profile passes: which kernel group dominates, with the two chains
+    # run one after the other so every group's time is its own.  Per group the
+    # median over the passes, so that one late launch does not pick the group.
     for c in ctxs:
         c.profile_read(reset=True)
         c.profile_enable(_native.KERNEL_IDS)
         c.set_stream(stream.cuda_stream)
-    for _ in range(3):
+    passes = []
+    for _ in range(PROFILE_PASSES):
         flush.zero_()
         for c, leaf in zip(ctxs, LEAVES):
             c.voxel_normals_enqueue(dcloud, leaf, None, RADIUS, 3, VIEWPOINT, count_shell=False)
-    torch.cuda.synchronize()
-    prof = [c.profile_read(reset=True) for c in ctxs]
+        torch.cuda.synchronize()
+        passes.append([c.profile_read(reset=True) for c in ctxs])
     for c, s in zip(ctxs, leaf_streams):
         c.set_stream(s.cuda_stream)
-    group_ms = {g: sum(p[g]["total_ms"] for p in prof) for g in _native.KERNEL_IDS}
-    iso_group = {g: (sum(p[g]["total_ms"] for p in prof),
-                     sum(p[g]["timed_regions"] for p in prof)) for g in _native.KERNEL_IDS}
+    group_ms = {g: statistics.median(sum(p[g]["total_ms"] for p in ps) for ps in passes)
+                for g in _native.KERNEL_IDS}  # ms per step (both leaves)
+    iso_group = {g: (group_ms[g], sum(p[g]["timed_regions"] for p in passes[0]))
+                 for g in _native.KERNEL_IDS}  # (ms, launches) per step
     dominant = max(group_ms, key=group_ms.get)
     if args.profile_all and rank == 0:
         tot = sum(group_ms.values())
         for g, ms in sorted(group_ms.items(), key=lambda kv: -kv[1]):
-            print(f"  {g:16s} {ms / 3:9.4f} ms/step  {100 * ms / tot:5.1f}%", file=sys.stderr)
+            print(f"  {g:16s} {ms:9.4f} ms/step  {100 * ms / tot:5.1f}%", file=sys.stderr)
     for c in ctxs:
         c.profile_enable([dominant])
 
@@ -439,7 +443,7 @@ def run_gpu(args):
                     peak_source="MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
                     else "fallback 6650 GB/s",
                     algorithmic_bytes_per_launch=dom_bytes, avg_launch_ms=avg_launch_ms,
-                    isolated_split_ms={g: round(ms / 3, 4) for g, ms in
+                    isolated_split_ms={g: round(ms, 4) for g, ms in
                                        sorted(group_ms.items(), key=lambda kv: -kv[1]) if ms > 0},
                     timing=("CUDA events around each launch of the group in the timed region, "
                             "where the two leaf chains share the GPU" if not args.serial_leaves

@@ -109,13 +109,15 @@ def measure(sizes=SAMPLE_POINTS, reps: int = 10, warmup: int = 3, seed: int = 1,
 
 
 def samples(result: dict, kind: str) -> list:
-    """[(keys, [ms per shape])], ascending: the voxel sorts at their point
-    counts (kind "voxel") or the cell sorts at their voxel counts ("cell")."""
+    """[(size, [ms per shape])], ascending, for the voxel sorts (kind "voxel")
+    or the cell sorts ("cell").  The size is the chain's point count for both:
+    the library picks a cell sort's shape before the voxel count is known on
+    the host, from the same upper bound."""
     n_cfg = len(result["configs"])
     by = {}
     for r in result["runs"]:
         keys, ms = ((r["points"], r["voxel_sort_ms"]) if kind == "voxel"
-                    else (r["voxels"], r["cell_sort_ms"]))
+                    else (r["points"], r["cell_sort_ms"]))
         by.setdefault(keys, [None] * n_cfg)[r["config"]] = ms
     out = [(k, ms) for k, ms in by.items() if all(m is not None for m in ms)]
     return sorted(out, key=lambda t: t[0])
@@ -180,7 +182,7 @@ def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> s
         cfgs = result["configs"]
         shapes = "  ".join(f"{c['items_per_thread']:>4}x{c['blocks_per_sm']}" for c in cfgs)
         for kind in ("voxel", "cell"):
-            lines.append(f"//   {kind}-key sort       keys  {shapes}")
+            lines.append(f"//   {kind}-key sort     points  {shapes}")
             for keys, ms in samples(result, kind):
                 lines.append(f"//   {'':14} {keys:>9}  " + "  ".join(f"{m:6.4f}" for m in ms))
         if result.get("staging"):

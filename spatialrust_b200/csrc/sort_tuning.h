@@ -11,7 +11,7 @@
 // through L1 (0).
 //
 // Measured sort ms (georeferenced scan, leaf 0.1, radius 0.5; L2 flushed before every chain):
-//   voxel-key sort       keys    16x2     8x3    12x3     8x4
+//   voxel-key sort     points    16x2     8x3    12x3     8x4
 //                      65536  0.0589  0.0453  0.0537  0.0476
 //                      92682  0.0597  0.0463  0.0535  0.0490
 //                     131072  0.0605  0.0481  0.0546  0.0500
@@ -31,26 +31,26 @@
 //                   16777216  0.8046  0.8001  0.7058  0.7505
 //                   23726566  1.1152  1.1109  0.9771  1.0369
 //                   33554432  1.5592  1.5515  1.3612  1.4412
-//   cell-key sort       keys    16x2     8x3    12x3     8x4
-//                      65325  0.0516  0.0391  0.0456  0.0410
-//                      92252  0.0519  0.0397  0.0468  0.0415
-//                     130231  0.0533  0.0409  0.0474  0.0428
-//                     183630  0.0535  0.0412  0.0479  0.0433
-//                     258683  0.0543  0.0435  0.0491  0.0453
-//                     364390  0.0545  0.0468  0.0502  0.0490
-//                     511610  0.0572  0.0522  0.0550  0.0546
-//                     716353  0.0617  0.0597  0.0596  0.0614
-//                     998975  0.0677  0.0699  0.0680  0.0731
-//                    1386254  0.0865  0.0856  0.0791  0.0872
-//                    1913842  0.1053  0.1027  0.1027  0.1069
-//                    2610072  0.1304  0.1308  0.1215  0.1276
-//                    3512442  0.1620  0.1636  0.1532  0.1617
-//                    4648599  0.2073  0.2054  0.1897  0.2028
-//                    6011810  0.2662  0.2595  0.2391  0.2541
-//                    7569816  0.3320  0.3200  0.2931  0.3076
-//                    8875163  0.3815  0.3684  0.3341  0.3505
-//                   10515699  0.4414  0.4255  0.3838  0.4019
-//                   12236880  0.5016  0.4851  0.4356  0.4555
+//   cell-key sort     points    16x2     8x3    12x3     8x4
+//                      65536  0.0516  0.0391  0.0456  0.0410
+//                      92682  0.0519  0.0397  0.0468  0.0415
+//                     131072  0.0533  0.0409  0.0474  0.0428
+//                     185364  0.0535  0.0412  0.0479  0.0433
+//                     262144  0.0543  0.0435  0.0491  0.0453
+//                     370728  0.0545  0.0468  0.0502  0.0490
+//                     524288  0.0572  0.0522  0.0550  0.0546
+//                     741455  0.0617  0.0597  0.0596  0.0614
+//                    1048576  0.0677  0.0699  0.0680  0.0731
+//                    1482910  0.0865  0.0856  0.0791  0.0872
+//                    2097152  0.1053  0.1027  0.1027  0.1069
+//                    2965821  0.1304  0.1308  0.1215  0.1276
+//                    4194304  0.1620  0.1636  0.1532  0.1617
+//                    5931642  0.2073  0.2054  0.1897  0.2028
+//                    8388608  0.2662  0.2595  0.2391  0.2541
+//                   11863283  0.3320  0.3200  0.2931  0.3076
+//                   16777216  0.3815  0.3684  0.3341  0.3505
+//                   23726566  0.4414  0.4255  0.3838  0.4019
+//                   33554432  0.5016  0.4851  0.4356  0.4555
 // Normals kernel ms per chain, neighbour gather through L1 / staged:
 //       65536    0.023 /  0.026
 //       92682    0.027 /  0.032
@@ -81,7 +81,7 @@ constexpr uint32_t kVoxelSortTuneCount = 4;
 constexpr uint64_t kVoxelSortTuneMaxPoints[] = {623486ull, 881743ull, 1246973ull, UINT64_MAX};
 constexpr int32_t kVoxelSortTuneConfig[] = {1, 2, 0, 2};
 constexpr uint32_t kCellSortTuneCount = 3;
-constexpr uint64_t kCellSortTuneMaxPoints[] = {845942ull, 1176789ull, UINT64_MAX};
+constexpr uint64_t kCellSortTuneMaxPoints[] = {881743ull, 1246973ull, UINT64_MAX};
 constexpr int32_t kCellSortTuneConfig[] = {1, 0, 2};
 // 1: the normals kernel gathers candidates through shared memory (bulk copies)
 constexpr int32_t kNeighborStaging = 0;

@@ -21,13 +21,13 @@ def test_samples_and_boundaries():
                 (400_000, 200_000): [1.0, 2.0, 3.0, 1.5],
                 (800_000, 300_000): [1.0, 2.0, 3.0, 1.5]})
     v, c = autotune.samples(res, "voxel"), autotune.samples(res, "cell")
-    assert [k for k, _ in v] == [100_000, 400_000, 800_000]
-    assert [k for k, _ in c] == [50_000, 200_000, 300_000]
+    # both kinds are keyed by the chain's point count (the launch-time bound)
+    assert [k for k, _ in v] == [k for k, _ in c] == [100_000, 400_000, 800_000]
     assert v[0][1] == [1.5, 0.75, 2.25, 1.125] and c[0][1] == [0.5, 0.25, 0.75, 0.375]
     # shape 1 up to the first sample, shape 0 from the second: the boundary is
     # their geometric mean
     assert autotune.choose(res, "voxel") == [(200_000, 1), (BIG, 0)]
-    assert autotune.choose(res, "cell") == [(100_000, 1), (BIG, 0)]
+    assert autotune.choose(res, "cell") == [(200_000, 1), (BIG, 0)]
 
 
 def test_hysteresis_keeps_the_smaller_sizes_shape():
