@@ -9,7 +9,7 @@ import pytest
 
 import oracle
 import spatialrust_b200 as sr
-from spatialrust_b200 import _native, synthetic
+from spatialrust_b200 import synthetic
 
 pytestmark = pytest.mark.gpu
 F = np.float32

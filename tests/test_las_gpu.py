@@ -6,7 +6,6 @@ import numpy as np
 import pytest
 
 import oracle
-import spatialrust_b200 as sr
 from spatialrust_b200 import las, synthetic
 from spatialrust_b200.streaming import SpoolOptions, StreamingVoxelConfig, StreamingVoxelSource
 

@@ -72,7 +72,6 @@ def test_tuning_table_arguments(cuda_ctx):
     assert cuda_ctx.sort_tuning() == {"voxel": default["voxel"], "cell": [(1000, 2)]}
     cuda_ctx.set_sort_tuning([])
     assert cuda_ctx.sort_tuning() == default
-    import ctypes
     assert cuda_ctx._lib.srcu_set_sort_tuning(cuda_ctx._h, 2, None, None, 0) == _native.SRCU_ERR_INVALID_ARGUMENT
 
 
