@@ -279,6 +279,18 @@ int32_t srcu_get_neighbor_staging(srcu_ctx *ctx);
  * health checks and tests of the error path; it never faults the GPU. */
 srcu_status srcu_selftest_bounded_wait(srcu_ctx *ctx, uint32_t max_polls);
 
+/* ---- epoch of the look-back tags (tests) ------------------------------------ */
+
+/* No counterpart in the reference.  Every chain tags the look-back words and
+ * hash slots it publishes with a 32-bit epoch that advances by 64 per chain
+ * (or graph replay).  Before the epoch would wrap, the context clears every
+ * tagged array and restarts the epoch at 0, so a tag never repeats while an
+ * old word may carry it.  These two calls exist for tests of that restart:
+ * set_epoch (a multiple of 64) places a context just below the wrap;
+ * get_epoch synchronises and returns the epoch and how many restarts ran. */
+srcu_status srcu_debug_set_epoch(srcu_ctx *ctx, uint32_t epoch);
+srcu_status srcu_debug_get_epoch(srcu_ctx *ctx, uint32_t *epoch, uint64_t *restarts);
+
 /* ---- RANSAC plane segmentation ------------------------------------------- */
 
 /* GpuPlaneScore (crates/spatialrust-gpu/src/kernels/ransac_plane.rs:27-37). */
@@ -628,6 +640,10 @@ int srcu_profile_read(srcu_ctx *ctx, srcu_kernel_stat *out, int max_entries, int
 srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud, const srcu_voxel_params *params,
                                         const srcu_voxel_out *out, uint64_t *out_voxels,
                                         void *cuda_stream);
+/* Test hooks for the epoch restart of that scratch on the current device
+ * (the same rule as srcu_debug_set_epoch / srcu_debug_get_epoch). */
+srcu_status srcu_noalloc_debug_set_epoch(uint32_t epoch);
+srcu_status srcu_noalloc_debug_get_epoch(uint32_t *epoch, uint64_t *restarts);
 
 #ifdef __cplusplus
 }

@@ -60,8 +60,11 @@ def _load():
     lib.oracle_radius_normals_ref.restype = ctypes.c_int
     lib.oracle_radius_normals_fp64.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float,
                                                ctypes.c_uint32, ctypes.c_int, P, ctypes.c_double,
-                                               ctypes.c_int, P, P, P, P, P, P, P]
+                                               ctypes.c_int, P, P, P, P, P, P, P, ctypes.c_int]
     lib.oracle_radius_normals_fp64.restype = ctypes.c_int
+    lib.oracle_grid_normals_wgsl.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float, ctypes.c_int,
+                                             P, ctypes.c_int, P, P, P, P, P]
+    lib.oracle_grid_normals_wgsl.restype = ctypes.c_int
     lib.oracle_plane_covariances.argtypes = [P, P, P, ctypes.c_size_t, ctypes.c_float,
                                              ctypes.c_double, ctypes.c_int, P, P, P]
     lib.oracle_plane_covariances.restype = ctypes.c_int
@@ -228,8 +231,13 @@ def radius_normals_ref(x, y, z, radius, min_neighbors=3, viewpoint=None, threads
 
 
 def radius_normals_fp64(x, y, z, radius, min_neighbors=3, viewpoint=None, shell_rel=1e-6,
-                        threads=0) -> NormalResult:
-    """FP64 oracle: exact f32-predicate neighbour sets, FP64 covariance and Jacobi."""
+                        threads=0, include_self=False) -> NormalResult:
+    """FP64 oracle: exact f32-predicate neighbour sets, FP64 covariance and Jacobi.
+
+    include_self: the wgpu grid estimator's semantics (normals_grid.rs:86-197,
+    normal_gpu.rs:33-83): the query is in its own neighbourhood (counts
+    include it), fewer than 3 points give (0, 0, 1) turned toward the
+    viewpoint with curvature 0, min_neighbors is ignored."""
     lib = _load()
     x, y, z = _f32(x), _f32(y), _f32(z)
     n = x.shape[0]
@@ -240,12 +248,34 @@ def radius_normals_fp64(x, y, z, radius, min_neighbors=3, viewpoint=None, shell_
     rc = lib.oracle_radius_normals_fp64(_ptr(x), _ptr(y), _ptr(z), n, ctypes.c_float(radius),
                                         min_neighbors, int(viewpoint is not None), _ptr(vp),
                                         ctypes.c_double(shell_rel), threads,
-                                        *[_ptr(o) for o in outs], _ptr(counts), _ptr(shell))
+                                        *[_ptr(o) for o in outs], _ptr(counts), _ptr(shell),
+                                        int(bool(include_self)))
     if rc != 0:
         raise OracleError(f"oracle_radius_normals_fp64 failed: {rc}")
     nx, ny, nz, curv, gap = [o[:n] for o in outs]
     valid = int(np.count_nonzero(~np.isnan(nx)))
     return NormalResult(nx, ny, nz, curv, counts[:n], valid, n - valid, gap, shell[:n].astype(bool))
+
+
+def grid_normals_wgsl(x, y, z, radius, viewpoint=None, threads=0) -> NormalResult:
+    """The wgpu grid estimator's f32 arithmetic (NORMALS_GRID_WGSL,
+    normals_grid.rs:86-197, 16-sweep Jacobi) and GpuNormalEstimator's
+    orientation (normal_gpu.rs:63-70); sums in KD-tree order, so equal to the
+    shader up to f32 rounding.  counts include the query."""
+    lib = _load()
+    x, y, z = _f32(x), _f32(y), _f32(z)
+    n = x.shape[0]
+    outs = [np.empty(max(n, 1), np.float32) for _ in range(4)]
+    counts = np.zeros(max(n, 1), np.uint32)
+    vp = np.asarray(viewpoint if viewpoint is not None else (0, 0, 0), np.float32)
+    rc = lib.oracle_grid_normals_wgsl(_ptr(x), _ptr(y), _ptr(z), n, ctypes.c_float(radius),
+                                      int(viewpoint is not None), _ptr(vp), threads,
+                                      *[_ptr(o) for o in outs], _ptr(counts))
+    if rc != 0:
+        raise OracleError(f"oracle_grid_normals_wgsl failed: {rc}")
+    nx, ny, nz, curv = [o[:n] for o in outs]
+    valid = int(np.count_nonzero(counts[:n] >= 3))
+    return NormalResult(nx, ny, nz, curv, counts[:n], valid, n - valid)
 
 
 @dataclass

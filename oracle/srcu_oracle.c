@@ -936,6 +936,7 @@ typedef struct {
   uint32_t min_neighbors;
   int has_vp;
   float vp[3];
+  int include_self;
   double *nx, *ny, *nz, *curv, *gap;
   uint32_t *counts;
   uint8_t *shell;
@@ -948,6 +949,15 @@ typedef struct {
  * smallest eigenvector, sign toward the viewpoint (normal.rs:408-421, in FP64).
  * gap = (l1 - l0) / max(l2, tiny) flags ill-conditioned normals.
  * shell[i] = 1 when some other point has |d2 - r2| <= shell_rel * r2.
+ *
+ * include_self: the semantics of the reference's wgpu grid estimator
+ * (NORMALS_GRID_WGSL, crates/spatialrust-gpu/src/kernels/normals_grid.rs:
+ * 86-197, behind GpuNormalEstimator::estimate, normal_gpu.rs:33-83): the query
+ * belongs to its own neighbourhood (its d2 is 0 when it is finite), a
+ * neighbourhood of fewer than 3 points gives the normal (0, 0, 1) and
+ * curvature 0 (normals_grid.rs:129-132), min_neighbors plays no part, and
+ * every normal -- the fallback included -- is turned toward the viewpoint
+ * (normal_gpu.rs:63-70).  counts[i] then includes the query.
  */
 static void *fp64_worker(void *arg) {
   fp64_job *j = (fp64_job *)arg;
@@ -964,9 +974,9 @@ static void *fp64_worker(void *arg) {
     double sx = 0, sy = 0, sz = 0;
     for (size_t k = 0; k < found.len; ++k) {
       uint32_t p = found.idx[k];
-      if (p == (uint32_t)i) continue;
+      if (p == (uint32_t)i && !j->include_self) continue;
       float d2 = kd_sq_dist(j->x[p], j->y[p], j->z[p], qx, qy, qz);
-      if (fabs((double)d2 - (double)r2) <= j->shell_rel * (double)r2) shell = 1;
+      if (p != (uint32_t)i && fabs((double)d2 - (double)r2) <= j->shell_rel * (double)r2) shell = 1;
       if (d2 <= r2) {
         cnt++;
         sx += j->x[p];
@@ -979,12 +989,19 @@ static void *fp64_worker(void *arg) {
     j->nx[i] = j->ny[i] = j->nz[i] = NAN;
     j->curv[i] = 0.0;
     j->gap[i] = 0.0;
-    if (cnt < j->min_neighbors || cnt == 0) continue;
+    if (j->include_self ? cnt < 3 : (cnt < j->min_neighbors || cnt == 0)) {
+      if (j->include_self) { /* normals_grid.rs:129-132, oriented as normal_gpu.rs:63-70 */
+        j->nx[i] = 0.0;
+        j->ny[i] = 0.0;
+        j->nz[i] = (j->has_vp && j->vp[2] < qz) ? -1.0 : 1.0;
+      }
+      continue;
+    }
     double mx = sx / cnt, my = sy / cnt, mz = sz / cnt;
     double c[3][3] = {{0}};
     for (size_t k = 0; k < found.len; ++k) {
       uint32_t p = found.idx[k];
-      if (p == (uint32_t)i) continue;
+      if (p == (uint32_t)i && !j->include_self) continue;
       float d2 = kd_sq_dist(j->x[p], j->y[p], j->z[p], qx, qy, qz);
       if (!(d2 <= r2)) continue;
       double dx = j->x[p] - mx, dy = j->y[p] - my, dz = j->z[p] - mz;
@@ -1032,7 +1049,8 @@ static void *fp64_worker(void *arg) {
 int oracle_radius_normals_fp64(const float *x, const float *y, const float *z, size_t n,
                                float radius, uint32_t min_neighbors, int has_vp, const float *vp,
                                double shell_rel, int threads, double *nx, double *ny, double *nz,
-                               double *curv, double *gap, uint32_t *counts, uint8_t *shell) {
+                               double *curv, double *gap, uint32_t *counts, uint8_t *shell,
+                               int include_self) {
   if (n == 0) return OR_OK;
   if (radius < 0.0f) return OR_ERR_INVALID;
   kd_tree tree;
@@ -1056,6 +1074,7 @@ int oracle_radius_normals_fp64(const float *x, const float *y, const float *z, s
     j->min_neighbors = min_neighbors;
     j->has_vp = has_vp;
     if (has_vp) memcpy(j->vp, vp, sizeof(float) * 3);
+    j->include_self = include_self;
     j->nx = nx;
     j->ny = ny;
     j->nz = nz;
@@ -1068,6 +1087,167 @@ int oracle_radius_normals_fp64(const float *x, const float *y, const float *z, s
     fp64_worker(&jobs[0]);
   } else {
     for (size_t w = 0; w < njobs; ++w) pthread_create(&tids[w], NULL, fp64_worker, &jobs[w]);
+    for (size_t w = 0; w < njobs; ++w) pthread_join(tids[w], NULL);
+  }
+  free(jobs);
+  free(tids);
+  kd_free(&tree);
+  return OR_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* The wgpu grid estimator's arithmetic, in f32                              */
+/* ------------------------------------------------------------------------ */
+
+/* rotate() of NORMALS_GRID_WGSL (normals_grid.rs:46-80): one Jacobi rotation
+ * zeroing a[p][q], applied to the rows and columns of a and the columns of v. */
+static void wgsl_rotate(float a[3][3], float v[3][3], int p, int q) {
+  const float apq = a[p][q];
+  if (fabsf(apq) < 1e-20f) return;
+  const float app = a[p][p], aqq = a[q][q];
+  const float phi = 0.5f * (aqq - app) / apq;
+  float t;
+  if (phi >= 0.0f) t = 1.0f / (phi + sqrtf(1.0f + phi * phi));
+  else t = -1.0f / (-phi + sqrtf(1.0f + phi * phi));
+  const float c = 1.0f / sqrtf(1.0f + t * t);
+  const float s = t * c;
+  for (int r = 0; r < 3; ++r) {
+    const float arp = a[r][p], arq = a[r][q];
+    a[r][p] = c * arp - s * arq;
+    a[r][q] = s * arp + c * arq;
+  }
+  for (int r = 0; r < 3; ++r) {
+    const float apr = a[p][r], aqr = a[q][r];
+    a[p][r] = c * apr - s * aqr;
+    a[q][r] = s * apr + c * aqr;
+  }
+  for (int r = 0; r < 3; ++r) {
+    const float vrp = v[r][p], vrq = v[r][q];
+    v[r][p] = c * vrp - s * vrq;
+    v[r][q] = s * vrp + c * vrq;
+  }
+}
+
+typedef struct {
+  const kd_tree *tree;
+  const float *x, *y, *z;
+  size_t start, end;
+  float r2;
+  int has_vp;
+  float vp[3];
+  float *nx, *ny, *nz, *curv;
+  uint32_t *counts;
+} wgsl_job;
+
+/* main() of NORMALS_GRID_WGSL (normals_grid.rs:86-197) on the neighbour set
+ * of the f32 predicate with the query included, then GpuNormalEstimator's
+ * host-side orientation (normal_gpu.rs:63-70, orient_normal_towards_viewpoint
+ * normal.rs:408-421 with Vec3::dot / normalize, vec.rs:66-100).  f32 mean and
+ * covariance sums (undivided), 16 sweeps of (0,1), (0,2), (1,2) rotations,
+ * the smallest diagonal entry's column.  The shader visits the 27 cells in
+ * its own order; sums here run in KD-tree order, so results agree with the
+ * shader to f32 rounding, not bit for bit. */
+static void *wgsl_worker(void *arg) {
+  wgsl_job *j = (wgsl_job *)arg;
+  u32_vec found = {0};
+  for (size_t i = j->start; i < j->end; ++i) {
+    found.len = 0;
+    const float px = j->x[i], py = j->y[i], pz = j->z[i];
+    if (j->tree->root != KD_INVALID) kd_radius(j->tree, j->tree->root, px, py, pz, j->r2, &found);
+    float mean[3] = {0, 0, 0}, count = 0.0f;
+    for (size_t k = 0; k < found.len; ++k) {
+      const uint32_t q = found.idx[k];
+      mean[0] += j->x[q];
+      mean[1] += j->y[q];
+      mean[2] += j->z[q];
+      count += 1.0f;
+    }
+    j->counts[i] = (uint32_t)found.len;
+    float n[3] = {0.0f, 0.0f, 1.0f}, curvature = 0.0f;
+    if (count >= 3.0f) {
+      for (int a = 0; a < 3; ++a) mean[a] = mean[a] / count;
+      float c00 = 0, c11 = 0, c22 = 0, c01 = 0, c02 = 0, c12 = 0;
+      for (size_t k = 0; k < found.len; ++k) {
+        const uint32_t q = found.idx[k];
+        const float dx = j->x[q] - mean[0], dy = j->y[q] - mean[1], dz = j->z[q] - mean[2];
+        c00 = c00 + dx * dx;
+        c11 = c11 + dy * dy;
+        c22 = c22 + dz * dz;
+        c01 = c01 + dx * dy;
+        c02 = c02 + dx * dz;
+        c12 = c12 + dy * dz;
+      }
+      float a[3][3] = {{c00, c01, c02}, {c01, c11, c12}, {c02, c12, c22}};
+      float v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+      for (int sweep = 0; sweep < 16; ++sweep) {
+        wgsl_rotate(a, v, 0, 1);
+        wgsl_rotate(a, v, 0, 2);
+        wgsl_rotate(a, v, 1, 2);
+      }
+      const float eig[3] = {a[0][0], a[1][1], a[2][2]};
+      int m = 0;
+      if (eig[1] < eig[m]) m = 1;
+      if (eig[2] < eig[m]) m = 2;
+      float len = sqrtf(v[0][m] * v[0][m] + v[1][m] * v[1][m] + v[2][m] * v[2][m]);
+      if (len < 1e-20f) len = 1e-20f;
+      for (int a2 = 0; a2 < 3; ++a2) n[a2] = v[a2][m] / len;
+      const float trace = eig[0] + eig[1] + eig[2];
+      if (trace > 0.0f) curvature = eig[m] / trace;
+    }
+    if (j->has_vp) {
+      const float wx = j->vp[0] - px, wy = j->vp[1] - py, wz = j->vp[2] - pz;
+      if (n[0] * wx + n[1] * wy + n[2] * wz < 0.0f) {
+        n[0] = -n[0];
+        n[1] = -n[1];
+        n[2] = -n[2];
+      }
+      const float l = sqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      if (l != 0.0f)
+        for (int a2 = 0; a2 < 3; ++a2) n[a2] = n[a2] / l;
+    }
+    j->nx[i] = n[0];
+    j->ny[i] = n[1];
+    j->nz[i] = n[2];
+    j->curv[i] = curvature;
+  }
+  free(found.idx);
+  return NULL;
+}
+
+int oracle_grid_normals_wgsl(const float *x, const float *y, const float *z, size_t n,
+                             float radius, int has_vp, const float *vp, int threads, float *nx,
+                             float *ny, float *nz, float *curv, uint32_t *counts) {
+  if (n == 0) return OR_OK;
+  if (radius < 0.0f) return OR_ERR_INVALID;
+  kd_tree tree;
+  if (kd_build(&tree, x, y, z, n) != OR_OK) return OR_ERR_NOMEM;
+  size_t avail = threads > 0 ? (size_t)threads : (size_t)sysconf(_SC_NPROCESSORS_ONLN);
+  size_t workers = n < 4096 ? 1 : (avail < n / 1024 ? avail : (n / 1024 ? n / 1024 : 1));
+  size_t chunk = (n + workers - 1) / workers;
+  size_t njobs = (n + chunk - 1) / chunk;
+  wgsl_job *jobs = (wgsl_job *)calloc(njobs, sizeof(wgsl_job));
+  pthread_t *tids = (pthread_t *)calloc(njobs, sizeof(pthread_t));
+  for (size_t w = 0; w < njobs; ++w) {
+    wgsl_job *j = &jobs[w];
+    j->tree = &tree;
+    j->x = x;
+    j->y = y;
+    j->z = z;
+    j->start = w * chunk;
+    j->end = j->start + chunk < n ? j->start + chunk : n;
+    j->r2 = radius * radius; /* GridUniform.radius_sq, normals_grid.rs:263 */
+    j->has_vp = has_vp;
+    if (has_vp) memcpy(j->vp, vp, sizeof(float) * 3);
+    j->nx = nx;
+    j->ny = ny;
+    j->nz = nz;
+    j->curv = curv;
+    j->counts = counts;
+  }
+  if (njobs == 1) {
+    wgsl_worker(&jobs[0]);
+  } else {
+    for (size_t w = 0; w < njobs; ++w) pthread_create(&tids[w], NULL, wgsl_worker, &jobs[w]);
     for (size_t w = 0; w < njobs; ++w) pthread_join(tids[w], NULL);
   }
   free(jobs);

@@ -292,6 +292,12 @@ SIGNATURES = {
     "srcu_server_release": ([_P, ctypes.c_uint64], ctypes.c_int),
     "srcu_server_stats_get": ([_P, ctypes.POINTER(SrcuServerStats)], ctypes.c_int),
     "srcu_server_stats_reset": ([_P], ctypes.c_int),
+    "srcu_debug_set_epoch": ([_P, ctypes.c_uint32], ctypes.c_int),
+    "srcu_debug_get_epoch": ([_P, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)],
+                             ctypes.c_int),
+    "srcu_noalloc_debug_set_epoch": ([ctypes.c_uint32], ctypes.c_int),
+    "srcu_noalloc_debug_get_epoch": ([ctypes.POINTER(ctypes.c_uint32),
+                                      ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
 }
 
 _lib = None
@@ -583,6 +589,17 @@ class Context:
 
     def neighbor_staging(self) -> int:
         return int(self._lib.srcu_get_neighbor_staging(self._h))
+
+    def debug_set_epoch(self, epoch: int) -> None:
+        """Test hook: places the look-back epoch (a multiple of 64)."""
+        self._check(self._lib.srcu_debug_set_epoch(self._h, int(epoch)))
+
+    def debug_epoch(self) -> tuple:
+        """(epoch, restarts) after synchronising."""
+        e = ctypes.c_uint32(0)
+        r = ctypes.c_uint64(0)
+        self._check(self._lib.srcu_debug_get_epoch(self._h, ctypes.byref(e), ctypes.byref(r)))
+        return int(e.value), int(r.value)
 
     def selftest_bounded_wait(self, max_polls: int = 1000):
         """Runs a device wait that must give up: raises DeviceTimeout."""

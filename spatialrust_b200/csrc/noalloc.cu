@@ -54,6 +54,11 @@ struct NoallocDevice {
   int num_sms = 0;
   int occ_sort = 1;
   int occ_seg = 1;
+  // Host mirror of the scratch control block's epoch: each call's k_begin
+  // advances it by EPOCHS_PER_RUN.  Before it would wrap, the look-back words
+  // are cleared and it restarts at 0, as epoch_guard does for a context.
+  uint32_t epoch_host = 0;
+  uint64_t epoch_restarts = 0;
 };
 
 NoallocDevice g_noalloc_dev[NA_MAX_DEVICES];
@@ -127,6 +132,9 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
   for (uint32_t a = 0; a < cloud->n_attrs; ++a)
     if (!cloud->attrs || !cloud->attrs[a] || !out->attrs || !out->attrs[a])
       return SRCU_ERR_MISSING_FIELD;
+  // An error left pending by the caller's own CUDA work is theirs: report it
+  // before queueing anything, and leave it in place for them to read.
+  if (cudaPeekAtLastError() != cudaSuccess) return SRCU_ERR_CUDA;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= NA_MAX_DEVICES) {
     cudaGetLastError();
@@ -139,6 +147,20 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
   }
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
   unsigned char *b = dev->base;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (dev->epoch_host > kEpochLast) {
+      if (cudaMemsetAsync(b + NA_LB_SORT, 0, NA_VKEYS - NA_LB_SORT, s) != cudaSuccess ||
+          cudaMemsetAsync(b + NA_CTL + offsetof(Control, epoch), 0, sizeof(uint32_t), s) !=
+              cudaSuccess) {
+        cudaGetLastError();
+        return SRCU_ERR_CUDA;
+      }
+      dev->epoch_host = 0;
+      ++dev->epoch_restarts;
+    }
+    dev->epoch_host += EPOCHS_PER_RUN;
+  }
   Control *ctl = reinterpret_cast<Control *>(b + NA_CTL);
   SortBuffers sb;
   sb.keys[0] = reinterpret_cast<uint64_t *>(b + NA_KEYS0);
@@ -223,5 +245,50 @@ extern "C" srcu_status srcu_voxel_centroid_noalloc(const srcu_cloud *cloud,
   if (status & ST_KEY_OVERFLOW) return SRCU_ERR_KEY_OVERFLOW;
   if (status) return SRCU_ERR_CUDA;
   if (out_voxels) *out_voxels = voxels;
+  return SRCU_OK;
+}
+
+// Test hooks for the epoch restart of the scratch on the current device.
+extern "C" srcu_status srcu_noalloc_debug_set_epoch(uint32_t epoch) {
+  if (epoch % EPOCHS_PER_RUN != 0) return SRCU_ERR_INVALID_ARGUMENT;
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= NA_MAX_DEVICES) {
+    cudaGetLastError();
+    return SRCU_ERR_NO_DEVICE;
+  }
+  NoallocDevice *dev = nullptr;
+  const srcu_status st = noalloc_setup(device, &dev);
+  if (st != SRCU_OK) return st;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpy(dev->base + NA_CTL + offsetof(Control, epoch), &epoch, sizeof(epoch),
+                 cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    return SRCU_ERR_CUDA;
+  }
+  dev->epoch_host = epoch;
+  return SRCU_OK;
+}
+
+extern "C" srcu_status srcu_noalloc_debug_get_epoch(uint32_t *epoch, uint64_t *restarts) {
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= NA_MAX_DEVICES) {
+    cudaGetLastError();
+    return SRCU_ERR_NO_DEVICE;
+  }
+  NoallocDevice *dev = nullptr;
+  const srcu_status st = noalloc_setup(device, &dev);
+  if (st != SRCU_OK) return st;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  uint32_t e = 0;
+  if (cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpy(&e, dev->base + NA_CTL + offsetof(Control, epoch), sizeof(e),
+                 cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return SRCU_ERR_CUDA;
+  }
+  if (e != dev->epoch_host) return SRCU_ERR_CUDA;
+  if (epoch) *epoch = e;
+  if (restarts) *restarts = dev->epoch_restarts;
   return SRCU_OK;
 }

@@ -778,10 +778,14 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
       oc = sum > 0.0 ? float(e.l0 / sum) : 0.0f;
       ++n_valid;
     } else {
+      // include_self: (0, 0, 1) (normals_grid.rs:129-132), turned toward the
+      // viewpoint as GpuNormalEstimator turns every normal (normal_gpu.rs:
+      // 63-70): the f32 dot with vp - q is fl(vp.z - q.z), negative exactly
+      // when vp.z < q.z.
       const float nanv = __int_as_float(0x7fc00000);
       ox = prm.include_self ? 0.0f : nanv;
       oy = prm.include_self ? 0.0f : nanv;
-      oz = prm.include_self ? 1.0f : nanv;
+      oz = prm.include_self ? ((prm.has_viewpoint && prm.vp[2] < qp.z) ? -1.0f : 1.0f) : nanv;
       oc = 0.0f;
       ++n_invalid;
     }

@@ -36,6 +36,11 @@ struct srcu_ctx {
   std::string err;
   Control *ctl = nullptr;       // device
   Control *ctl_host = nullptr;  // pinned mirror for read-back
+  // Host mirror of ctl->epoch (epoch_guard), restarts of it, and whether a
+  // chain is being captured into a graph (its epoch advances at launch).
+  uint32_t epoch_host = 0;
+  uint64_t epoch_restarts = 0;
+  bool capturing = false;
   // Side stream for read-backs that overlap later kernels of the same chain,
   // the event that releases them, and a pinned copy of the control-block head
   // (epoch, status, point and voxel counts) read once the voxel stage is done.
@@ -724,10 +729,39 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
   return SRCU_OK;
 }
 
+// Keeps look-back and hash tags unique.  Every chain's k_begin advances the
+// device epoch by EPOCHS_PER_RUN and tags the words it publishes with
+// epoch + offset (offset < EPOCHS_PER_RUN); a word counts as published only
+// when its tag equals the reader's.  If the 32-bit epoch wrapped, a word left
+// behind 2^26 chains earlier (on a tile index no chain has written since)
+// would carry the current tag and be read as a published prefix.  So before
+// the chain whose tags would pass 2^32 - 1, every epoch-tagged array is
+// cleared and the epoch restarts at 0 (tag 0, the tag of a cleared word, is
+// never used: the first chain after a restart runs at EPOCHS_PER_RUN).  The
+// host mirrors the device epoch exactly -- k_begin is its only writer and
+// each chain or graph replay runs one k_begin -- so the restart is issued on
+// the host, in stream order, before that chain.
+constexpr uint32_t kEpochLast = 0xffffffffu - 2 * EPOCHS_PER_RUN + 1;  // last epoch a chain may start from
+
+srcu_status epoch_guard(srcu_ctx *ctx) {
+  if (ctx->epoch_host > kEpochLast) {
+    DevBuf *tagged[] = {&ctx->lb_sort, &ctx->lb_seg, &ctx->lb_cells, &ctx->table};
+    for (DevBuf *b : tagged)
+      if (b->p) CU_TRY(cudaMemsetAsync(b->p, 0, b->bytes, ctx->stream));
+    CU_TRY(cudaMemsetAsync(&ctx->ctl->epoch, 0, sizeof(uint32_t), ctx->stream));
+    ctx->epoch_host = 0;
+    ++ctx->epoch_restarts;
+  }
+  ctx->epoch_host += EPOCHS_PER_RUN;
+  return SRCU_OK;
+}
+
 // Starts a chain over one cloud (parameters written by k_begin itself) or
 // a staged batch (single == 0).
-void begin_chain(srcu_ctx *ctx, uint64_t n, const Batch &bt, int single,
-                 const srcu_voxel_params *vp, const srcu_normal_params *np) {
+srcu_status begin_chain(srcu_ctx *ctx, uint64_t n, const Batch &bt, int single,
+                        const srcu_voxel_params *vp, const srcu_normal_params *np) {
+  // a captured chain advances the epoch when its graph is launched
+  if (!ctx->capturing) ST_TRY(epoch_guard(ctx));
   Launch l(ctx, SRCU_K_BEGIN);
   k_begin<<<1, 256, 0, ctx->stream>>>(ctx->ctl, n, bt, cloud_bits_for(bt.clouds), single,
                                       to_dev(vp), to_dev(np));
@@ -737,6 +771,7 @@ void begin_chain(srcu_ctx *ctx, uint64_t n, const Batch &bt, int single,
     ctx->count_shell = np && np->count_shell;
   }
   ctx->xyz_order = single && vp && vp->mode == SRCU_VOXEL_CENTROID_XYZ;
+  return SRCU_OK;
 }
 
 srcu_status read_control(srcu_ctx *ctx) {
@@ -1050,7 +1085,7 @@ srcu_status srcu_voxel_centroid(srcu_ctx *ctx, const srcu_cloud *cloud,
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, cloud, cols));
   const Batch bt = make_batch(ctx, 1);
-  begin_chain(ctx, n, bt, 1, params, nullptr);
+  ST_TRY(begin_chain(ctx, n, bt, 1, params, nullptr));
   ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
   if (out && out->keys) ST_TRY(unpack_keys(ctx, n));
   ST_TRY(read_control(ctx));
@@ -1078,7 +1113,7 @@ srcu_status srcu_radius_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, &xyz, cols));
   const Batch bt = make_batch(ctx, 1);
-  begin_chain(ctx, n, bt, 1, nullptr, params);
+  ST_TRY(begin_chain(ctx, n, bt, 1, nullptr, params));
   const uint32_t grid_b = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4),
                                                                     uint32_t(ctx->num_sms) * 8));
   {
@@ -1116,7 +1151,7 @@ srcu_status srcu_euclidean_cluster_roots(srcu_ctx *ctx, const srcu_cloud *cloud,
   srcu_normal_params np{};
   np.radius = cluster_tolerance;  // the grid of a radius search with r = tolerance
   np.min_neighbors = 1;
-  begin_chain(ctx, n, bt, 1, nullptr, &np);
+  ST_TRY(begin_chain(ctx, n, bt, 1, nullptr, &np));
   const uint32_t grid_b = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4),
                                                                     uint32_t(ctx->num_sms) * 8));
   {
@@ -1177,7 +1212,7 @@ srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float
   np.radius = radius;
   np.min_neighbors = 3;
   np.include_self = 1;
-  begin_chain(ctx, n, bt, 1, nullptr, &np);
+  ST_TRY(begin_chain(ctx, n, bt, 1, nullptr, &np));
   const uint32_t grid_b = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4),
                                                                     uint32_t(ctx->num_sms) * 8));
   {
@@ -1223,7 +1258,7 @@ srcu_status srcu_voxel_normals(srcu_ctx *ctx, const srcu_cloud *cloud,
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, cloud, cols));
   const Batch bt = make_batch(ctx, 1);
-  begin_chain(ctx, n, bt, 1, vparams, nparams);
+  ST_TRY(begin_chain(ctx, n, bt, 1, vparams, nparams));
   ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
   // The centroids are final once the voxel stage is done: their read-back
   // runs on the side stream while the normal kernels run.  The host learns V
@@ -1275,7 +1310,7 @@ srcu_status srcu_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
   const float *cols[MAX_COLS];
   ST_TRY(stage_input(ctx, cloud, cols));
   const Batch bt = make_batch(ctx, 1);
-  begin_chain(ctx, n, bt, 1, vparams, nparams);
+  ST_TRY(begin_chain(ctx, n, bt, 1, vparams, nparams));
   if (n > 0) {
     ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
     ST_TRY(enqueue_normals(ctx, ptr<float>(ctx->vout[0]), ptr<float>(ctx->vout[1]),
@@ -1313,7 +1348,7 @@ static srcu_status batch_enqueue(srcu_ctx *ctx, const srcu_cloud *points, const 
   ST_TRY(stage_input(ctx, points, cols));
   if (stage) ST_TRY(stage_batch(ctx, count, offsets, vparams, nparams));
   const Batch bt = make_batch(ctx, count);
-  begin_chain(ctx, n, bt, 0, nullptr, nullptr);
+  ST_TRY(begin_chain(ctx, n, bt, 0, nullptr, nullptr));
   ctx->agg_all = to_dev(&vparams[0]).agg;
   for (uint32_t b = 1; b < count; ++b)
     if (to_dev(&vparams[b]).agg != ctx->agg_all) ctx->agg_all = -1;
@@ -1369,7 +1404,9 @@ srcu_status srcu_chain_graph_create(srcu_ctx *ctx, const srcu_cloud *points,
   cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
   srcu_status st = SRCU_OK;
   if (e == cudaSuccess) {
+    ctx->capturing = true;
     st = batch_enqueue(ctx, points, off, cnt, vparams, nparams, false);
+    ctx->capturing = false;
     e = cudaStreamEndCapture(ctx->stream, &g->graph);
   }
   ctx->prof_mask = mask;
@@ -1388,6 +1425,7 @@ srcu_status srcu_chain_graph_create(srcu_ctx *ctx, const srcu_cloud *points,
 
 srcu_status srcu_graph_launch(srcu_ctx *ctx, srcu_graph *g) {
   if (!ctx || !g) return SRCU_ERR_INVALID_ARGUMENT;
+  ST_TRY(epoch_guard(ctx));  // the graph's k_begin advances the epoch once
   CU_TRY(cudaGraphLaunch(g->exec, ctx->stream));
   ctx->last_clouds = g->clouds;
   ctx->last_attrs = g->attrs;
@@ -1471,6 +1509,31 @@ srcu_status srcu_chain_info_get(srcu_ctx *ctx, srcu_chain_info *info) {
   CellPlan first{};
   CU_TRY(cudaMemcpy(&first, ctx->b_cplans.p, sizeof(CellPlan), cudaMemcpyDeviceToHost));
   info->cell_size = first.h;
+  return SRCU_OK;
+}
+
+srcu_status srcu_debug_set_epoch(srcu_ctx *ctx, uint32_t epoch) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  if (epoch % EPOCHS_PER_RUN != 0)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "the epoch must be a multiple of %u", EPOCHS_PER_RUN);
+  CU_TRY(cudaSetDevice(ctx->device));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  CU_TRY(cudaMemcpy(&ctx->ctl->epoch, &epoch, sizeof(epoch), cudaMemcpyHostToDevice));
+  ctx->epoch_host = epoch;
+  return SRCU_OK;
+}
+
+srcu_status srcu_debug_get_epoch(srcu_ctx *ctx, uint32_t *epoch, uint64_t *restarts) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  CU_TRY(cudaSetDevice(ctx->device));
+  CU_TRY(cudaStreamSynchronize(ctx->stream));
+  uint32_t dev = 0;
+  CU_TRY(cudaMemcpy(&dev, &ctx->ctl->epoch, sizeof(dev), cudaMemcpyDeviceToHost));
+  if (dev != ctx->epoch_host)
+    return fail(ctx, SRCU_ERR_CUDA, "device epoch %u differs from the host mirror %u", dev,
+                ctx->epoch_host);
+  if (epoch) *epoch = dev;
+  if (restarts) *restarts = ctx->epoch_restarts;
   return SRCU_OK;
 }
 

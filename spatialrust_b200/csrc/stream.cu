@@ -133,7 +133,7 @@ srcu_status sv_flush(srcu_stream_voxel *sv) {
   ST_TRY(reserve(ctx, n, 0, false, false, false));
   ST_TRY(reserve_batch(ctx, 1));
   const Batch bt = make_batch(ctx, 1);
-  begin_chain(ctx, n, bt, 1, nullptr, nullptr);
+  ST_TRY(begin_chain(ctx, n, bt, 1, nullptr, nullptr));
   const float *x = ptr<const float>(sv->run[0]);
   const float *y = ptr<const float>(sv->run[1]);
   const float *z = ptr<const float>(sv->run[2]);
@@ -202,7 +202,7 @@ srcu_status sv_finish(srcu_stream_voxel *sv) {
   ST_TRY(ensure(ctx, sv->okeys, r * 24));
   ST_TRY(reserve(ctx, r, 0, false, false, false));
   ST_TRY(reserve_batch(ctx, 1));
-  begin_chain(ctx, r, make_batch(ctx, 1), 1, nullptr, nullptr);
+  ST_TRY(begin_chain(ctx, r, make_batch(ctx, 1), 1, nullptr, nullptr));
   {
     Launch l(ctx, SRCU_K_VOXEL_PLAN);
     k_stream_merge_plan<<<1, 32, 0, ctx->stream>>>(ctx->ctl, ptr<StreamPlan>(sv->plan),

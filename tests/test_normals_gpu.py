@@ -4,65 +4,32 @@ Bar: neighbour counts are exact (the f32 predicate is evaluated exactly as the
 reference's KD-tree does, kdtree.rs:544-549); normals are within 1e-4 rad of
 the FP64 oracle, sign-matched by viewpoint, for every point whose covariance
 is not near-degenerate (relative eigengap >= GAP_MIN; those are counted and
-reported); curvature within 1e-5."""
+reported, and their share is bounded); curvature within 1e-5 (normal_parity.py)."""
 import numpy as np
 import pytest
 
+import normal_parity
 import oracle
 import spatialrust_b200 as sr
 from spatialrust_b200 import synthetic
 
 pytestmark = pytest.mark.gpu
 F = np.float32
-ANGLE_TOL = 1e-4  # rad
-CURV_TOL = 1e-5
-GAP_MIN = 1e-3
+ANGLE_TOL = normal_parity.ANGLE_TOL
+GAP_MIN = normal_parity.GAP_MIN
+angle_errors = normal_parity.angle_errors
 
 
-def angle_between(a, b):
-    """Angle in radians via atan2(|a x b|, a . b) -- accurate near 0, unlike
-    arccos of a dot product, which turns float32 rounding into ~1e-4 rad."""
-    a = a.astype(np.float64)
-    a = a / np.linalg.norm(a, axis=1, keepdims=True)
-    b = b / np.linalg.norm(b, axis=1, keepdims=True)
-    return np.arctan2(np.linalg.norm(np.cross(a, b), axis=1), np.sum(a * b, axis=1))
-
-
-def angle_errors(gpu, ref, points, viewpoint):
-    """Angle between GPU and FP64 normals; sign-free where the viewpoint does
-    not decide the sign robustly (or no viewpoint is given)."""
-    err = angle_between(gpu, ref)
-    sign_free = np.minimum(err, np.pi - err)
-    if viewpoint is None:
-        return sign_free
-    view = np.asarray(viewpoint, np.float64)[None, :] - points.astype(np.float64)
-    cos_view = np.abs(np.sum(ref * view, axis=1)) / np.linalg.norm(view, axis=1)
-    ambiguous = cos_view < 1e-3
-    err[ambiguous] = sign_free[ambiguous]
-    return err
-
-
-def check_normals(ctx, x, y, z, radius, min_neighbors=3, viewpoint=None, report=None):
-    nx, ny, nz, curv, counts, stats = ctx.radius_normals(x, y, z, radius, min_neighbors, viewpoint)
-    ref = oracle.radius_normals_fp64(x, y, z, radius, min_neighbors, viewpoint)
-    assert np.array_equal(counts, ref.counts), \
-        f"{np.count_nonzero(counts != ref.counts)} neighbour counts differ"
-    valid = ~np.isnan(ref.nx)
-    assert np.array_equal(~np.isnan(nx), valid)
-    assert stats["valid_count"] == int(valid.sum())
-    assert stats["invalid_count"] == int((~valid).sum())
-    assert np.all(curv[~valid] == 0)
-    g = np.stack([nx, ny, nz], 1)[valid]
-    pts = np.stack([x, y, z], 1)[valid]
-    err = angle_errors(g, ref.normals[valid], pts, viewpoint)
-    well = ref.gap[valid] >= GAP_MIN
+def check_normals(ctx, x, y, z, radius, min_neighbors=3, viewpoint=None, report=None,
+                  include_self=False, ill_max=1e-3):
+    nx, ny, nz, curv, counts, stats = ctx.radius_normals(x, y, z, radius, min_neighbors, viewpoint,
+                                                         include_self)
+    ref = oracle.radius_normals_fp64(x, y, z, radius, min_neighbors, viewpoint,
+                                     include_self=include_self)
+    rep = normal_parity.check_against_fp64(nx, ny, nz, curv, counts, ref, x, y, z, viewpoint,
+                                           stats, ill_max=ill_max, include_self=include_self)
     if report is not None:
-        report.update(max_err=float(err[well].max()) if well.any() else 0.0,
-                      ill_conditioned=int((~well).sum()), shell=int(ref.shell.sum()),
-                      valid=int(valid.sum()))
-    if well.any():
-        assert err[well].max() <= ANGLE_TOL, f"max angle error {err[well].max():.3e} rad"
-    assert np.max(np.abs(curv[valid] - ref.curvature[valid])) <= CURV_TOL
+        report.update(rep)
     return nx, ny, nz, curv, counts, stats
 
 
@@ -146,6 +113,36 @@ def test_include_self_semantics(cuda_ctx):
                                                           include_self=True)
     assert nx.tolist() == [0, 0, 0] and nz.tolist() == [1, 1, 1] and curv.tolist() == [0, 0, 0]
     assert counts.tolist() == [1, 2, 2]
+    # GpuNormalEstimator turns the fallback toward the viewpoint too (normal_gpu.rs:63-70)
+    nx, ny, nz, curv, counts, _ = cuda_ctx.radius_normals(x, np.zeros(3, F), np.zeros(3, F), 1.0,
+                                                          viewpoint=(0, 0, -5), include_self=True)
+    assert nz.tolist() == [-1, -1, -1] and curv.tolist() == [0, 0, 0]
+
+
+def test_include_self_georeferenced_scan(cuda_ctx):
+    # the wgpu grid semantics on a 300k-point scan against the FP64 oracle's
+    # include_self mode: counts = oracle counts (query included), the fallback
+    # set and its (0, 0, +-1) exact, normals within 1e-4 rad
+    # (r 0.6 on a sparse scan: ~9 points per neighbourhood, 36k fallbacks,
+    # 642 ill-conditioned neighbourhoods of 3-5 nearly collinear points)
+    c = synthetic.georef_scan(300_000, seed=9)
+    rep = {}
+    check_normals(cuda_ctx, c.x, c.y, c.z, 0.6, viewpoint=(0, 0, 100), include_self=True,
+                  report=rep, ill_max=3.5e-3)
+    assert 250_000 < rep["solved"] < c.n  # both branches exercised
+    print("include_self scan:", rep)
+
+
+def test_include_self_shapes_crop_no_viewpoint(cuda_ctx):
+    c = synthetic.shapes_scene(5_000_000, seed=2)
+    xyz = c.xyz()
+    lo = xyz[7] - 8.0
+    p = xyz[np.all((xyz >= lo) & (xyz < lo + 16), axis=1)]
+    assert p.shape[0] > 20_000
+    rep = {}
+    check_normals(cuda_ctx, p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy(), 0.3,
+                  include_self=True, report=rep)
+    print("include_self shapes crop:", rep)
 
 
 def test_zero_radius_counts_duplicates(cuda_ctx):
@@ -215,14 +212,11 @@ def test_voxel_then_normals_chain(cuda_ctx):
     assert np.array_equal(out["keys"], vox.keys) and np.array_equal(out["counts"], vox.counts)
     for g, r in zip(out["columns"], vox.fields):
         assert np.max(np.abs(g - r)) <= 1e-6
-    ref = oracle.radius_normals_fp64(vox.x, vox.y, vox.z, 0.5, 3, (0, 0, 100))
-    assert np.array_equal(out["neighbor_counts"], ref.counts)
-    valid = ~np.isnan(ref.nx)
-    g = np.stack([out["nx"], out["ny"], out["nz"]], 1)[valid]
-    pts = np.stack([vox.x, vox.y, vox.z], 1)[valid]
-    err = angle_errors(g, ref.normals[valid], pts, (0, 0, 100))
-    well = ref.gap[valid] >= GAP_MIN
-    assert err[well].max() <= ANGLE_TOL
+    gx, gy, gz = out["columns"][:3]  # the normals stage's own input
+    ref = oracle.radius_normals_fp64(gx, gy, gz, 0.5, 3, (0, 0, 100))
+    normal_parity.check_against_fp64(out["nx"], out["ny"], out["nz"], out["curvature"],
+                                     out["neighbor_counts"], ref, gx, gy, gz, (0, 0, 100),
+                                     out["stats"], label="chain")
 
 
 def test_device_enqueue_matches_sync_path(cuda_ctx):

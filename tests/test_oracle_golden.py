@@ -270,6 +270,55 @@ def test_grid_planar_patch_vertical_normal():
     assert np.all(r.curvature < 1e-3)
 
 
+def test_wgsl_restatement_grid_known_answers():
+    # normals_grid.rs:359-377 (no viewpoint: |nz| > 0.99, curvature < 1e-3) and
+    # normal_gpu.rs:127-152 (viewpoint (0, 0, 10): nz > 0.99) on the 12x12 grid,
+    # through the restatement of the shader's own f32 arithmetic
+    xs, ys = np.meshgrid(np.arange(12, dtype=np.float32), np.arange(12, dtype=np.float32), indexing="ij")
+    x = xs.ravel() * F(0.1)
+    y = ys.ravel() * F(0.1)
+    z = np.zeros_like(x)
+    r = oracle.grid_normals_wgsl(x, y, z, 0.25)
+    assert np.all(np.abs(r.nz) > 0.99) and np.all(r.curvature < 1e-3)
+    assert np.all(r.counts >= 5)  # the query and its 4-neighbours at least
+    r = oracle.grid_normals_wgsl(x, y, z, 0.25, (0.0, 0.0, 10.0))
+    assert np.all(r.nz > 0.99)
+    f = oracle.radius_normals_fp64(x, y, z, 0.25, viewpoint=(0.0, 0.0, 10.0), include_self=True)
+    assert np.array_equal(f.counts, r.counts) and np.all(f.nz > 0.99)
+
+
+def test_include_self_semantics_of_the_oracles():
+    # normals_grid.rs:129-132: fewer than 3 points (query included) -> (0, 0, 1),
+    # curvature 0; turned toward the viewpoint by normal_gpu.rs:63-70
+    x = np.array([0.0, 10.0, 10.5, 20.0, 20.3, 20.6, 40.0], np.float32)
+    zeros = np.zeros_like(x)
+    for vp, sign in ((None, 1.0), ((0.0, 0.0, -5.0), -1.0), ((0.0, 0.0, 5.0), 1.0)):
+        f = oracle.radius_normals_fp64(x, zeros, zeros, 1.0, viewpoint=vp, include_self=True)
+        w = oracle.grid_normals_wgsl(x, zeros, zeros, 1.0, vp)
+        assert f.counts.tolist() == [1, 2, 2, 3, 3, 3, 1] == w.counts.tolist()
+        for k in (0, 1, 2, 6):  # fallback points
+            assert (f.nx[k], f.ny[k], f.nz[k], f.curvature[k]) == (0.0, 0.0, sign, 0.0)
+            assert (w.nx[k], w.ny[k], w.nz[k], w.curvature[k]) == (0.0, 0.0, sign, 0.0)
+    # a non-finite query finds nothing, itself included
+    xn = np.array([0.0, 0.1, np.nan, 0.2], np.float32)
+    f = oracle.radius_normals_fp64(xn, np.zeros(4, F), np.zeros(4, F), 0.5, include_self=True)
+    assert f.counts.tolist() == [3, 3, 0, 3]
+
+
+def test_include_self_counts_are_plain_counts_plus_one():
+    rng = np.random.default_rng(17)
+    p = rng.random((4000, 3), dtype=np.float32)
+    a = oracle.radius_normals_fp64(p[:, 0], p[:, 1], p[:, 2], 0.08, 3)
+    b = oracle.radius_normals_fp64(p[:, 0], p[:, 1], p[:, 2], 0.08, 3, include_self=True)
+    w = oracle.grid_normals_wgsl(p[:, 0], p[:, 1], p[:, 2], 0.08)
+    assert np.array_equal(b.counts, a.counts + 1) and np.array_equal(w.counts, b.counts)
+    # where both solve, the shader's f32 Jacobi agrees with the FP64 solve on
+    # well-conditioned neighbourhoods (loose: 16 f32 sweeps, f32 sums)
+    ok = (b.counts >= 3) & (b.gap >= 0.1)
+    cosang = np.abs(np.sum(b.normals[ok] * np.stack([w.nx, w.ny, w.nz], 1)[ok], axis=1))
+    assert np.degrees(np.arccos(np.clip(cosang, -1, 1))).max() < 0.5
+
+
 def test_kdtree_radius_matches_brute_force():
     # kdtree.rs:654 (radius search vs brute force)
     rng = np.random.default_rng(11)
