@@ -90,6 +90,15 @@ def parse():
     return ap.parse_args()
 
 
+def bench_config(world: int) -> dict:
+    """The workload, identical in both arms' lines."""
+    return dict(workload=WORKLOAD, points=N_POINTS, leaves=list(LEAVES), radius=RADIUS,
+                viewpoint=list(VIEWPOINT), parallelism=f"replicas x{world}")
+
+
+VOXEL_GROUPS = ("begin", "bounds", "voxel_plan", "voxel_sort", "voxel_segments")
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -191,7 +200,7 @@ def run_reference(args):
         impl="reference", metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus,
         steps=args.steps, warmup=args.warmup, ms_per_step=t * 1e3, higher_is_better=True,
         scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
-        config=dict(workload=WORKLOAD, points=len(crop[0]), sample_of=N_POINTS),
+        config=bench_config(args.gpus),
         cpu_baseline=dict(value=value, unit=UNIT, cores=threads, kind="port",
                           sample=(f"each step: {len(crop[0])} of the {N_POINTS} points "
                                   + ("(the whole cloud)" if side is None else
@@ -302,6 +311,31 @@ def algorithmic_bytes(group: str, info: dict, n_attrs: int = 1) -> float:
     return 0.0
 
 
+def summary(line: dict) -> dict:
+    """The line's key figures, printed last (a reader of the line's tail sees them)."""
+    out = dict(value=round(line["value"], 1), e2e=round(line["e2e"]["value"], 1),
+               e2e_pageable=round(line["e2e_pageable"]["value"], 1),
+               roofline_frac=round(line["roofline"]["frac"], 4),
+               roofline_voxel_frac=[round(x["frac"], 4) for x in line["roofline_voxel"]["leaves"]])
+    b = line.get("batched")
+    if b:
+        out["batched"] = {k: (round(b[k], 3) if isinstance(b.get(k), float) else b.get(k))
+                          for k in ("plain_ms", "batched_ms", "graph_ms", "speedup",
+                                    "graph_speedup") if k in b}
+    sh = line.get("shapes")
+    if sh:
+        out["shapes"] = dict(ms=round(sh["ms"], 3), mpts_s=round(sh["mpts_s"], 1))
+    sv = line.get("serving")
+    if sv and sv.get("rates"):
+        top = sv["rates"][-1]
+        out["serving"] = {k: round(top[k], 3) for k in ("offered_req_s", "achieved_req_s",
+                                                        "frame_p50_ms", "frame_p99_ms")}
+    cb = line.get("cpu_baseline")
+    if cb:
+        out["cpu_baseline"] = dict(value=round(cb["value"], 3), cores=cb["cores"])
+    return out
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -378,6 +412,9 @@ def run_gpu(args):
         c.set_stream(s.cuda_stream)
     group_ms = {g: statistics.median(sum(p[g]["total_ms"] for p in ps) for ps in passes)
                 for g in _native.KERNEL_IDS}  # ms per step (both leaves)
+    # the voxel chain of each leaf alone: kernel time of its groups, median over passes
+    voxel_chain_ms = [statistics.median(sum(ps[k][g]["total_ms"] for g in VOXEL_GROUPS)
+                                        for ps in passes) for k in range(len(LEAVES))]
     iso_group = {g: (group_ms[g], sum(p[g]["timed_regions"] for p in passes[0]))
                  for g in _native.KERNEL_IDS}  # (ms, launches) per step
     dominant = max(group_ms, key=group_ms.get)
@@ -419,8 +456,10 @@ def run_gpu(args):
     ms_per_step = max_ms / args.steps
     value = job_mpts(world, N_POINTS, ms_per_step)
 
-    # end to end through the C ABI with pinned host buffers
+    # end to end through the C ABI with pinned host buffers, then with plain
+    # (pageable) numpy buffers as a Rust caller's Vecs are
     e2e = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream)
+    e2e_pageable = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=False)
 
     peaks = {}
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -451,20 +490,34 @@ def run_gpu(args):
                     isolated_avg_launch_ms=iso_launch_ms, isolated_achieved=iso_achieved,
                     isolated_frac=iso_achieved / hbm,
                     step_share=group_ms[dominant] / max(sum(group_ms.values()), 1e-9))
+    # The voxel downsample alone against the HBM roofline: compulsory bytes
+    # 16 B/point read + 28 B/voxel written (centroid + intensity, packed key,
+    # count) over its kernels' time (bounds, plan, sort, segments), per leaf.
+    vox_bytes = [N_POINTS * 16.0 + i["voxels"] * 28.0 for i in infos]
+    roofline_voxel = dict(
+        bound="hbm", unit="GB/s", peak=hbm,
+        leaves=[dict(leaf=leaf, voxels=i["voxels"], algorithmic_bytes=b, chain_ms=ms,
+                     achieved=b / (ms / 1e3) / 1e9, frac=b / (ms / 1e3) / 1e9 / hbm,
+                     split_ms={g: round(statistics.median(ps[k][g]["total_ms"] for ps in passes), 4)
+                               for g in VOXEL_GROUPS})
+                for k, (leaf, i, b, ms) in enumerate(zip(LEAVES, infos, vox_bytes, voxel_chain_ms))],
+        timing=("each leaf's voxel chain alone (the isolated profile passes): CUDA events around "
+                "each of its kernel groups, summed, median over the passes"),
+        byte_model="16 B/point read + 28 B/voxel written")
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
         warmup=args.warmup, ms_per_step=ms_per_step, higher_is_better=True, scaling="weak",
         vs_baseline=None, dtype="f32", data="synthetic",
-        config=dict(workload=WORKLOAD, points=N_POINTS, leaves=list(LEAVES), radius=RADIUS,
-                    voxels=[i["voxels"] for i in infos], cells=[i["cells"] for i in infos],
-                    sort_passes=[[i["voxel_sort_passes"], i["cell_sort_passes"]] for i in infos],
-                    normals=[{k: st[k] for k in ("valid_count", "invalid_count", "fp64_eigensolves")}
-                             for st in nstats],
-                    l2="flushed by a 256 MB write before every timed step (outside the events)",
-                    parallelism=f"replicas x{world}",
-                    leaf_chains=("one stream, one after the other" if args.serial_leaves else
-                                 "two streams (one context each), forked and joined every step")),
-        e2e=e2e, roofline=roofline, clocks=clock, gpu_launches=int(launches),
+        config=bench_config(world),
+        details=dict(voxels=[i["voxels"] for i in infos], cells=[i["cells"] for i in infos],
+                     sort_passes=[[i["voxel_sort_passes"], i["cell_sort_passes"]] for i in infos],
+                     normals=[{k: st[k] for k in ("valid_count", "invalid_count", "fp64_eigensolves")}
+                              for st in nstats],
+                     l2="flushed by a 256 MB write before every timed step (outside the events)",
+                     leaf_chains=("one stream, one after the other" if args.serial_leaves else
+                                  "two streams (one context each), forked and joined every step")),
+        e2e=e2e, e2e_pageable=e2e_pageable, roofline=roofline, roofline_voxel=roofline_voxel,
+        clocks=clock, gpu_launches=int(launches),
     )
     if not args.no_batched:
         line["batched"] = run_batched(args, torch, dev, stream)
@@ -482,6 +535,7 @@ def run_gpu(args):
         line["serving"] = run_serving(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cloud)
+    line["summary"] = summary(line)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -1070,13 +1124,14 @@ def run_serving(args, device):
     return out
 
 
-def run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream):
-    """Synchronous srcu_voxel_normals calls with pinned host inputs and outputs,
-    one call per leaf.  Unless --serial-leaves, the two calls of a step are
-    made from two host threads on their own contexts and streams, so one
-    call's transfers overlap the other's kernels.  Device time: every leaf
-    stream waits on the start event, and the timing stream joins them all
-    before the end event."""
+def run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=True):
+    """Synchronous srcu_voxel_normals calls with host inputs and outputs, one
+    call per leaf: pinned buffers, or (pinned=False) plain numpy arrays in
+    pageable memory, as the reference's Rust arm passes its Vecs.  Unless
+    --serial-leaves, the two calls of a step are made from two host threads on
+    their own contexts and streams, so one call's transfers overlap the other's
+    kernels.  Device time: every leaf stream waits on the start event, and the
+    timing stream joins them all before the end event."""
     import threading
 
     from spatialrust_b200 import _native
@@ -1086,15 +1141,19 @@ def run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream):
     for c, s in zip(ctxs, streams):
         c.set_stream(s.cuda_stream)
     n = cloud.n
-    pin = [torch.from_numpy(a).pin_memory() for a in (cloud.x, cloud.y, cloud.z, cloud.intensity)]
+
+    def host(a):  # a torch CPU tensor: pinned, or a view of a pageable numpy array
+        return a.pin_memory() if pinned else a
+
+    pin = [host(torch.from_numpy(a.copy())) for a in (cloud.x, cloud.y, cloud.z, cloud.intensity)]
     keep = _native._Keep()
     attr_in = keep.add((ctypes.c_void_p * 1)(pin[3].data_ptr()))
     hcloud = _native.SrcuCloud(pin[0].data_ptr(), pin[1].data_ptr(), pin[2].data_ptr(),
                                ctypes.cast(attr_in, ctypes.c_void_p), 1, 0, n)
     outs = []
     for _ in LEAVES:
-        vcols = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(4)]
-        ncols = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(4)]
+        vcols = [host(torch.empty(n, dtype=torch.float32)) for _ in range(4)]
+        ncols = [host(torch.empty(n, dtype=torch.float32)) for _ in range(4)]
         attr_out = keep.add((ctypes.c_void_p * 1)(vcols[3].data_ptr()))
         # the reference's output schema: centroid columns and the four normal
         # columns (no per-voxel or neighbour counts)
@@ -1157,8 +1216,9 @@ def run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream):
     d2h = sum(v * (16 + 16) for v in voxels)
     return dict(value=N_POINTS / (ms / 1e3) / 1e6, unit=UNIT, ms_per_step=ms,
                 h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
-                api=("srcu_voxel_normals (include/srcuda.h), pinned host buffers, one call per "
-                     "leaf" + ("" if serial else ", the two calls from two host threads")))
+                api=("srcu_voxel_normals (include/srcuda.h), "
+                     + ("pinned" if pinned else "pageable (plain numpy)") + " host buffers, one "
+                     "call per leaf" + ("" if serial else ", the two calls from two host threads")))
 
 
 def main():

@@ -163,6 +163,10 @@ int srcu_abi_version(void);
 srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out);
 void srcu_destroy(srcu_ctx *ctx);
 const char *srcu_last_error(const srcu_ctx *ctx);
+/* The element counts behind the last SRCU_ERR_LENGTH_MISMATCH on this context
+ * (SpatialError::BufferLengthMismatch { expected, found }, error.rs:27-32);
+ * both 0 when the last failure was of another kind. */
+srcu_status srcu_last_length_mismatch(const srcu_ctx *ctx, uint64_t *expected, uint64_t *found);
 
 /* Runs subsequent work on a caller stream (a cudaStream_t); NULL restores the
  * context's own stream. */

@@ -292,6 +292,8 @@ SIGNATURES = {
     "srcu_server_release": ([_P, ctypes.c_uint64], ctypes.c_int),
     "srcu_server_stats_get": ([_P, ctypes.POINTER(SrcuServerStats)], ctypes.c_int),
     "srcu_server_stats_reset": ([_P], ctypes.c_int),
+    "srcu_last_length_mismatch": ([_P, ctypes.POINTER(ctypes.c_uint64),
+                                   ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
     "srcu_debug_set_epoch": ([_P, ctypes.c_uint32], ctypes.c_int),
     "srcu_debug_get_epoch": ([_P, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)],
                              ctypes.c_int),

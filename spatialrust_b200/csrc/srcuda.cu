@@ -41,14 +41,16 @@ struct srcu_ctx {
   uint32_t epoch_host = 0;
   uint64_t epoch_restarts = 0;
   bool capturing = false;
+  // the counts behind the last SRCU_ERR_LENGTH_MISMATCH (srcu_last_length_mismatch)
+  uint64_t mismatch_expected = 0, mismatch_found = 0;
   // Side stream for read-backs that overlap later kernels of the same chain,
   // the event that releases them, and a pinned copy of the control-block head
   // (epoch, status, point and voxel counts) read once the voxel stage is done.
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_voxel = nullptr;
   unsigned char *head_host = nullptr;
-  int occ_normals = 1, occ_normals_staged = 1, occ_seg = 1, occ_cells = 1;
-  int neighbor_staging = 0;  // k_normals gathers through shared memory by bulk copies
+  int occ_normals = 1, occ_normals_staged = 1, occ_normals_flat = 1, occ_seg = 1, occ_cells = 1;
+  int neighbor_staging = 0;  // k_normals' neighbour walk: WALK_L1, WALK_STAGED or WALK_FLAT
   // co-resident blocks per SM of each sort launch shape, voxel-key and cell-key sorts
   int occ_sort_v[SORT_CONFIGS] = {}, occ_sort_c[SORT_CONFIGS] = {};
   // sort launch shape by input size, per sort kind (SRCU_SORT_VOXEL_KEYS /
@@ -106,6 +108,7 @@ void stream_voxel_free(srcu_stream_voxel *sv);
 namespace {
 
 srcu_status fail(srcu_ctx *c, srcu_status st, const char *fmt, ...) {
+  if (c) c->mismatch_expected = c->mismatch_found = 0;
   char buf[512];
   va_list ap;
   va_start(ap, fmt);
@@ -714,12 +717,17 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
   ST_TRY(enqueue_grid(ctx, x, y, z, aos, count_dev, n_max, bt, voxel_keys));
   const uint32_t grid_n = uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals);
   Launch l(ctx, SRCU_K_NORMALS);
-  auto kernel = ctx->neighbor_staging
-                    ? (ctx->count_shell ? k_normals<true, false, true> : k_normals<false, false, true>)
+  const int walk = ctx->neighbor_staging;
+  auto kernel = walk == WALK_STAGED
+                    ? (ctx->count_shell ? k_normals<true, false, WALK_STAGED>
+                                        : k_normals<false, false, WALK_STAGED>)
+                : walk == WALK_FLAT
+                    ? (ctx->count_shell ? k_normals<true, false, WALK_FLAT>
+                                        : k_normals<false, false, WALK_FLAT>)
                     : (ctx->count_shell ? k_normals<true> : k_normals<false>);
-  const uint32_t grid = ctx->neighbor_staging
-                            ? uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals_staged)
-                            : grid_n;
+  const uint32_t grid = walk == WALK_STAGED ? uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals_staged)
+                        : walk == WALK_FLAT ? uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals_flat)
+                                            : grid_n;
   kernel<<<grid, NM_THREADS, 0, ctx->stream>>>(
       ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint2>(ctx->ranges),
       ptr<uint64_t>(ctx->cell_key), bt, count_dev, ptr<float>(ctx->nout[0]),
@@ -927,7 +935,9 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
   builtin_sort_tuning(ctx, SRCU_SORT_CELL_KEYS);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals, k_normals<true>, NM_THREADS, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals_staged,
-                                                k_normals<true, false, true>, NM_THREADS, 0);
+                                                k_normals<true, false, WALK_STAGED>, NM_THREADS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals_flat,
+                                                k_normals<true, false, WALK_FLAT>, NM_THREADS, 0);
   ctx->neighbor_staging = kNeighborStaging;
   if (configure_segment_kernels() != cudaSuccess) return bail(SRCU_ERR_CUDA);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_seg, k_voxel_segments<4>, SEG_THREADS,
@@ -935,6 +945,7 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_cells, k_cells, CELL_THREADS, 0);
   ctx->occ_normals = std::max(1, ctx->occ_normals);
   ctx->occ_normals_staged = std::max(1, ctx->occ_normals_staged);
+  ctx->occ_normals_flat = std::max(1, ctx->occ_normals_flat);
   ctx->occ_seg = std::max(1, ctx->occ_seg);
   ctx->occ_cells = std::max(1, ctx->occ_cells);
   if (cudaGetLastError() != cudaSuccess) return bail(SRCU_ERR_CUDA);
@@ -976,6 +987,13 @@ void srcu_destroy(srcu_ctx *ctx) {
 }
 
 const char *srcu_last_error(const srcu_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+srcu_status srcu_last_length_mismatch(const srcu_ctx *ctx, uint64_t *expected, uint64_t *found) {
+  if (!ctx || !expected || !found) return SRCU_ERR_INVALID_ARGUMENT;
+  *expected = ctx->mismatch_expected;
+  *found = ctx->mismatch_found;
+  return SRCU_OK;
+}
 
 srcu_status srcu_set_stream(srcu_ctx *ctx, void *cuda_stream) {
   if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
@@ -1036,8 +1054,8 @@ srcu_status srcu_get_sort_tuning(srcu_ctx *ctx, int32_t kind, uint64_t *max_poin
 
 srcu_status srcu_set_neighbor_staging(srcu_ctx *ctx, int32_t mode) {
   if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
-  if (mode < -1 || mode > 1)
-    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "neighbour staging is -1 (built-in), 0 or 1");
+  if (mode < -1 || mode > WALK_FLAT)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "the neighbour walk is -1 (built-in), 0, 1 or 2");
   ctx->neighbor_staging = mode < 0 ? kNeighborStaging : mode;
   return SRCU_OK;
 }
@@ -1223,9 +1241,11 @@ srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float
   ST_TRY(enqueue_grid(ctx, cols[0], cols[1], cols[2], ptr<const float4>(ctx->in_aos), nullptr, n,
                       bt, nullptr));
   {
-    const uint32_t grid_n = uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals);
+    const bool flat = ctx->neighbor_staging == WALK_FLAT;
+    const uint32_t grid_n =
+        uint32_t(ctx->num_sms) * uint32_t(flat ? ctx->occ_normals_flat : ctx->occ_normals);
     Launch l(ctx, SRCU_K_NORMALS);
-    k_normals<false, true><<<grid_n, NM_THREADS, 0, ctx->stream>>>(
+    (flat ? k_normals<false, true, WALK_FLAT> : k_normals<false, true>)<<<grid_n, NM_THREADS, 0, ctx->stream>>>(
         ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint2>(ctx->ranges),
         ptr<uint64_t>(ctx->cell_key), bt, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
         dst, epsilon);
@@ -1331,9 +1351,13 @@ static srcu_status batch_enqueue(srcu_ctx *ctx, const srcu_cloud *points, const 
     return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "batch enqueue needs device-resident points");
   if (count == 0 || !offsets || !vparams || !nparams)
     return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "a batch needs count >= 1, offsets and parameters");
-  if (offsets[0] != 0 || offsets[count] != points->n)
-    return fail(ctx, SRCU_ERR_LENGTH_MISMATCH, "offsets must run from 0 to the point count %llu",
-                (unsigned long long)points->n);
+  if (offsets[0] != 0 || offsets[count] != points->n) {
+    fail(ctx, SRCU_ERR_LENGTH_MISMATCH, "offsets must run from 0 to the point count %llu",
+         (unsigned long long)points->n);
+    ctx->mismatch_expected = offsets[0] != 0 ? 0 : points->n;
+    ctx->mismatch_found = offsets[0] != 0 ? offsets[0] : offsets[count];
+    return SRCU_ERR_LENGTH_MISMATCH;
+  }
   for (uint32_t b = 0; b < count; ++b) {
     if (offsets[b + 1] < offsets[b])
       return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing (cloud %u)", b);
