@@ -483,6 +483,15 @@ srcu_status srcu_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
                                        const srcu_voxel_params *vparams,
                                        const srcu_normal_params *nparams);
 
+/* The voxel stage alone (VoxelGridDownsample on a device-resident cloud):
+ * bounds, key plan, sort and the fused segment reduction, enqueued on the
+ * context stream without host synchronisation.  The centroids stay in the
+ * context's buffers (srcu_frame_view_get: x, y, z, attrs, counts,
+ * voxel_count; the normal pointers are not written); srcu_frame_check reads
+ * the status and V.  Same conditions as srcu_voxel_normals_enqueue. */
+srcu_status srcu_voxel_centroid_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                        const srcu_voxel_params *vparams);
+
 typedef struct srcu_frame_view {
   const float *x, *y, *z;        /* device: centroids (capacity n) */
   const float *const *attrs;     /* host array of device column pointers */

@@ -401,6 +401,9 @@ extern "C" {
     pub fn srcu_graph_destroy(graph: *mut srcu_graph);
     /// Enqueues the voxel -> normals chain on the context stream for a cloud already on the device, without any host synchronisation; results stay in ...
     pub fn srcu_voxel_normals_enqueue(ctx: *mut srcu_ctx, cloud: *const srcu_cloud, vparams: *const srcu_voxel_params, nparams: *const srcu_normal_params) -> srcu_status;
+    /// The voxel stage alone (VoxelGridDownsample on a device-resident cloud): bounds, key plan,
+    /// sort and the fused segment reduction, enqueued without host synchronisation.
+    pub fn srcu_voxel_centroid_enqueue(ctx: *mut srcu_ctx, cloud: *const srcu_cloud, vparams: *const srcu_voxel_params) -> srcu_status;
     /// Device pointers of the last enqueued chain's results.
     pub fn srcu_frame_view_get(ctx: *mut srcu_ctx, view: *mut srcu_frame_view) -> srcu_status;
     /// Synchronises and checks the device status word of the last enqueue.

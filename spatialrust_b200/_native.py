@@ -234,6 +234,8 @@ SIGNATURES = {
                             ctypes.POINTER(SrcuNormalStats)], ctypes.c_int),
     "srcu_voxel_normals_enqueue": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuVoxelParams),
                                     ctypes.POINTER(SrcuNormalParams)], ctypes.c_int),
+    "srcu_voxel_centroid_enqueue": ([_P, ctypes.POINTER(SrcuCloud), ctypes.POINTER(SrcuVoxelParams)],
+                                    ctypes.c_int),
     "srcu_frame_view_get": ([_P, ctypes.POINTER(SrcuFrameView)], ctypes.c_int),
     "srcu_frame_check": ([_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(SrcuNormalStats)],
                          ctypes.c_int),
@@ -705,6 +707,13 @@ class Context:
         np_ = _normal_params(radius, min_neighbors, viewpoint, include_self, count_shell)
         self._check(self._lib.srcu_voxel_normals_enqueue(self._h, ctypes.byref(cloud),
                                                          ctypes.byref(vp), ctypes.byref(np_)))
+
+    def voxel_centroid_enqueue(self, cloud: SrcuCloud, leaf: float, origin=None,
+                               approximate: bool = False, attribute_first: bool = False):
+        """The voxel stage alone on a device-resident cloud, no host sync."""
+        vp = _voxel_params(leaf, origin, approximate, attribute_first)
+        self._check(self._lib.srcu_voxel_centroid_enqueue(self._h, ctypes.byref(cloud),
+                                                          ctypes.byref(vp)))
 
     def batch_voxel_normals_enqueue(self, points: SrcuCloud, offsets, leaves, radii,
                                     min_neighbors: int = 3, viewpoints=None,

@@ -10,9 +10,10 @@ the input points) then radius normals (cell-key sort over the centroids) on a
 georeferenced scan -- at one input size per size class, and picks per class
 the shape with the least sort time.  Digit width stays at 8 bits: one digit
 bin per thread of a 256-thread block is what the ranking and the look-back
-are laid out for.  It also times the normals kernel's two neighbour gathers
-(candidate records staged in shared memory by bulk copies, or read through
-L1) over the same sizes and keeps the faster one.
+are laid out for.  It also times the normals kernel's three neighbour walks
+(range by range through L1, range by range from shared memory filled by bulk
+copies, each lane's ranges as one list with packed f32x2 arithmetic) over the
+same sizes and keeps the fastest.
 
     python -m spatialrust_b200.autotune                 # measure, print the table
     python -m spatialrust_b200.autotune --write         # ... and rewrite csrc/sort_tuning.h
@@ -41,6 +42,7 @@ SAMPLE_POINTS = tuple(int(round(2 ** (16 + k / 2))) for k in range(19))
 LEAF = 0.1
 RADIUS = 0.5
 HYSTERESIS = 0.02  # keep the smaller size's shape unless another is this much faster
+WALK_MODES = (0, 1, 2)  # srcu_set_neighbor_staging: L1, staged, flat
 TABLE_MAX = 32     # SRCU_SORT_TUNING_MAX
 BIG = (1 << 64) - 1
 L2_FLUSH_BYTES = 256 << 20  # written before every timed chain: inputs start outside L2
@@ -94,7 +96,7 @@ def measure(sizes=SAMPLE_POINTS, reps: int = 10, warmup: int = 3, seed: int = 1,
                 runs.append(dict(points=n, voxels=int(ctx.chain_info()["voxels"]), config=c,
                                  voxel_sort_ms=t["voxel_sort"], cell_sort_ms=t["cell_sort"]))
             ctx.set_sort_tuning([])
-            for mode in (0, 1):
+            for mode in WALK_MODES:
                 ctx.set_neighbor_staging(mode)
                 t = timed(["normals"])
                 staging.append(dict(points=n, voxels=int(ctx.chain_info()["voxels"]), staging=mode,
@@ -148,17 +150,23 @@ def choose(result: dict, kind: str, hysteresis: float = HYSTERESIS) -> list:
 
 
 def choose_staging(result: dict) -> int:
-    """1 when staging the neighbour gather in shared memory made the normals
-    kernel faster on average over the measured sizes (geometric mean of the
-    staged / plain time ratios, each size weighted equally), else 0 (also
-    without measurements)."""
+    """The neighbour walk whose normals time, relative to walk 0 (L1), has the
+    smallest geometric mean over the measured sizes (each size weighted
+    equally); 0 when no other walk is faster on that mean, or without
+    measurements."""
     by_n = {}
     for r in result.get("staging", []):
         by_n.setdefault(r["points"], {})[r["staging"]] = r["normals_ms"]
-    ratios = [per[1] / per[0] for per in by_n.values() if 0 in per and 1 in per and per[0] > 0]
-    if not ratios:
-        return 0
-    return 1 if float(np.mean(np.log(ratios))) < 0.0 else 0
+    best, best_score = 0, 0.0
+    for mode in sorted({m for per in by_n.values() for m in per}):
+        ratios = [per[mode] / per[0] for per in by_n.values()
+                  if 0 in per and mode in per and per[0] > 0]
+        if not ratios:
+            continue
+        score = float(np.mean(np.log(ratios)))
+        if score < best_score:
+            best, best_score = mode, score
+    return best
 
 
 def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> str:
@@ -171,9 +179,9 @@ def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> s
         "// cell-key sort over the radius-grid points.  Entry k applies to sorts of at",
         "// most k*SortTuneMaxPoints[k] keys (the last entry to every larger sort);",
         "// k*SortTuneConfig[k] indexes kSortItems / kSortMinBlocks in radix.cuh.",
-        "// kNeighborStaging: whether the normals kernel",
-        "// stages candidate records in shared memory by bulk copies (1) or reads them",
-        "// through L1 (0).",
+        "// kNeighborStaging: the normals kernel's neighbour walk -- range by range",
+        "// through L1 (0), range by range from shared memory filled by bulk copies (1),",
+        "// or each lane's ranges as one list with packed f32x2 arithmetic (2).",
     ]
     if result is not None:
         lines.append("//")
@@ -186,12 +194,13 @@ def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> s
             for keys, ms in samples(result, kind):
                 lines.append(f"//   {'':14} {keys:>9}  " + "  ".join(f"{m:6.4f}" for m in ms))
         if result.get("staging"):
-            lines.append("// Normals kernel ms per chain, neighbour gather through L1 / staged:")
+            lines.append("// Normals kernel ms per chain, neighbour walk L1 / staged / flat:")
             by_n = {}
             for r in result["staging"]:
                 by_n.setdefault(r["points"], {})[r["staging"]] = r["normals_ms"]
             for n, per in sorted(by_n.items()):
-                lines.append(f"//   {n:>9}   {per.get(0, float('nan')):6.3f} / {per.get(1, float('nan')):6.3f}")
+                lines.append(f"//   {n:>9}   " + " / ".join(
+                    f"{per.get(m, float('nan')):6.3f}" for m in WALK_MODES))
     lines += [
         "#pragma once",
         "",
@@ -210,7 +219,7 @@ def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> s
                 str(c) for _, c in table) + "};",
         ]
     lines += [
-        "// 1: the normals kernel gathers candidates through shared memory (bulk copies)",
+        "// the normals kernel's neighbour walk (srcu_set_neighbor_staging)",
         f"constexpr int32_t kNeighborStaging = {int(staging)};",
         "",
         "}  // namespace srcu",

@@ -563,8 +563,10 @@ __device__ __noinline__ void moments_fp64(const float4 *pts, const uint2 *rg, fl
 //
 // Moments are taken about the query point (d = p - q, the predicate's own
 // differences): count, sum d, sum d d^T, accumulated in f32 for NM_FLUSH
-// candidates and then folded into FP64; C = S2/n - (S1/n)(S1/n)^T and its
-// eigensolve are FP64.
+// candidates and then folded into FP64.  C = S2/n - (S1/n)(S1/n)^T is
+// assembled in FP64 and solved in FP32 (closed form); when the gap l1 - l0 is
+// under NM_REFINE_GAP of the trace, the point's moments are recomputed with
+// FP64 products over the same neighbour set and the solve is repeated in FP64.
 // CountShell: the chain reports shell points (some cloud asked for it); the
 // check costs a few instructions per candidate, so chains that do not want
 // it run the variant without it.

@@ -90,6 +90,17 @@ struct SortedView {
   __device__ __forceinline__ uint32_t val(uint32_t i) const {
     return packed ? uint32_t(keys[i] & ((1ull << idx_bits) - 1)) : vals[i];
   }
+  // key and value of item i with one load of a packed item
+  __device__ __forceinline__ void get(uint32_t i, uint64_t &k, uint32_t &v) const {
+    const uint64_t w = keys[i];
+    if (packed) {
+      k = w >> idx_bits;
+      v = uint32_t(w & ((1ull << idx_bits) - 1));
+    } else {
+      k = w;
+      v = vals[i];
+    }
+  }
 };
 
 __device__ __forceinline__ SortedView sorted_view(const SortBuffers &b, const SortState &s) {

@@ -1342,6 +1342,27 @@ srcu_status srcu_voxel_normals_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
   return SRCU_OK;
 }
 
+srcu_status srcu_voxel_centroid_enqueue(srcu_ctx *ctx, const srcu_cloud *cloud,
+                                        const srcu_voxel_params *vparams) {
+  if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
+  ST_TRY(check_cloud(ctx, cloud));
+  ST_TRY(check_voxel_params(ctx, vparams));
+  if (!cloud->on_device)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "enqueue needs a device-resident cloud");
+  const uint64_t n = cloud->n;
+  const uint32_t nc = 3 + cloud->n_attrs;
+  ST_TRY(reserve(ctx, n, nc, needs_staging(cloud), true, false));
+  ST_TRY(reserve_batch(ctx, 1));
+  const float *cols[MAX_COLS];
+  ST_TRY(stage_input(ctx, cloud, cols));
+  const Batch bt = make_batch(ctx, 1);
+  ST_TRY(begin_chain(ctx, n, bt, 1, vparams, nullptr));
+  if (n > 0) ST_TRY(enqueue_voxel(ctx, cols, nc, n, bt));
+  ctx->last_attrs = cloud->n_attrs;
+  CU_TRY(cudaGetLastError());
+  return SRCU_OK;
+}
+
 static srcu_status batch_enqueue(srcu_ctx *ctx, const srcu_cloud *points, const uint64_t *offsets,
                                  uint32_t count, const srcu_voxel_params *vparams,
                                  const srcu_normal_params *nparams, bool stage) {

@@ -108,8 +108,26 @@ __global__ void __launch_bounds__(BND_THREADS) k_bounds(const float *x, const fl
   if (bt.clouds == 1) {
     BoundsAcc acc;
     acc.reset();
-    for (uint64_t i = blockIdx.x * uint64_t(BND_THREADS) + threadIdx.x; i < n;
-         i += uint64_t(gridDim.x) * BND_THREADS) {
+    const uint64_t stride = uint64_t(gridDim.x) * BND_THREADS;
+    uint64_t i = blockIdx.x * uint64_t(BND_THREADS) + threadIdx.x;
+    // four points per thread in flight: all loads first, then the stores
+    for (; i + 3 * stride < n; i += 4 * stride) {
+      float px[4], py[4], pz[4], pa[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint64_t k = i + uint64_t(q) * stride;
+        px[q] = x[k];
+        py[q] = y[k];
+        pz[q] = z[k];
+        pa[q] = a0 ? a0[k] : 0.0f;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (aos) aos[i + uint64_t(q) * stride] = make_float4(px[q], py[q], pz[q], pa[q]);
+        acc.add(px[q], py[q], pz[q]);
+      }
+    }
+    for (; i < n; i += stride) {
       const float xi = x[i], yi = y[i], zi = z[i];
       if (aos) aos[i] = make_float4(xi, yi, zi, a0 ? a0[i] : 0.0f);
       acc.add(xi, yi, zi);
@@ -373,22 +391,42 @@ __global__ void __launch_bounds__(SEG_THREADS, 5) k_voxel_segments(Control *ctl,
     if (tile >= num_tiles) break;
     const uint32_t base = tile * SEG_TILE;
     const uint32_t tile_n = min(uint32_t(SEG_TILE), n - base);
-    for (uint32_t j = t; j < tile_n; j += SEG_THREADS) {
-      sm.keys[1 + j] = sv.key(base + j);
-      const uint32_t v = sv.val(base + j);
+    // The tile's sorted items, then their points: every thread issues all of
+    // its SEG_ITEMS item loads, then all of its random point gathers, before
+    // any of them is consumed, so the gathers' latencies overlap.
+    uint64_t ik[SEG_ITEMS];
+    uint32_t iv[SEG_ITEMS];
+#pragma unroll
+    for (int q = 0; q < SEG_ITEMS; ++q) {
+      const uint32_t j = t + uint32_t(q) * SEG_THREADS;
+      ik[q] = 0;
+      iv[q] = n;  // out of range: no gather
+      if (j < tile_n) sv.get(base + j, ik[q], iv[q]);
+    }
+    if (aos_in) {  // columns 0..3 from the AoS copy: one sector per point
+      float4 pt[SEG_ITEMS];
+#pragma unroll
+      for (int q = 0; q < SEG_ITEMS; ++q)
+        pt[q] = iv[q] < n ? aos_in[iv[q]] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int q = 0; q < SEG_ITEMS; ++q) {
+        const uint32_t j = t + uint32_t(q) * SEG_THREADS;
+        if (j >= tile_n) continue;
+        scol[0 * SEG_TILE + j] = pt[q].x;
+        scol[1 * SEG_TILE + j] = pt[q].y;
+        scol[2 * SEG_TILE + j] = pt[q].z;
+        if (NC > 3) scol[3 * SEG_TILE + j] = pt[q].w;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < SEG_ITEMS; ++q) {
+      const uint32_t j = t + uint32_t(q) * SEG_THREADS;
+      if (j >= tile_n) continue;
+      sm.keys[1 + j] = ik[q];
+      const uint32_t v = iv[q];
       if (v < n) {
-        if (aos_in) {  // columns 0..3 from the AoS copy: one sector per point
-          const float4 p = aos_in[v];
-          scol[0 * SEG_TILE + j] = p.x;
-          scol[1 * SEG_TILE + j] = p.y;
-          scol[2 * SEG_TILE + j] = p.z;
-          if (NC > 3) scol[3 * SEG_TILE + j] = p.w;
 #pragma unroll
-          for (int c = 4; c < NC; ++c) scol[c * SEG_TILE + j] = cols.in[c][v];
-        } else {
-#pragma unroll
-          for (int c = 0; c < NC; ++c) scol[c * SEG_TILE + j] = cols.in[c][v];
-        }
+        for (int c = aos_in ? 4 : 0; c < NC; ++c) scol[c * SEG_TILE + j] = cols.in[c][v];
       } else {  // a consistent sort never produces this; never read out of bounds
         atomicOr(&ctl->status, ST_INTERNAL);
 #pragma unroll

@@ -7,6 +7,7 @@ voxel keys and counts equal the oracle's."""
 import numpy as np
 import pytest
 
+import normal_parity
 import oracle
 import spatialrust_b200 as sr
 from spatialrust_b200 import _native, autotune, synthetic
@@ -78,7 +79,7 @@ def test_tuning_table_arguments(cuda_ctx):
 def test_autotuner_measures_every_shape():
     res = autotune.measure(sizes=(20_000, 150_000), reps=2, warmup=1)
     n_cfg = len(res["configs"])
-    assert len(res["runs"]) == 2 * n_cfg and len(res["staging"]) == 4
+    assert len(res["runs"]) == 2 * n_cfg and len(res["staging"]) == 2 * len(autotune.WALK_MODES)
     assert all(r["voxel_sort_ms"] > 0 and r["cell_sort_ms"] > 0 for r in res["runs"])
     for kind in ("voxel", "cell"):
         table = autotune.choose(res, kind)
@@ -151,11 +152,83 @@ def test_staged_gather_without_shell_count(cuda_ctx):
 
 def test_staging_switch_arguments(cuda_ctx):
     builtin = cuda_ctx.neighbor_staging()
-    assert builtin in (0, 1)
-    cuda_ctx.set_neighbor_staging(1 - builtin)
-    assert cuda_ctx.neighbor_staging() == 1 - builtin
-    for bad in (2, -2):
+    assert builtin in (0, 1, 2)
+    for mode in (0, 1, 2):
+        cuda_ctx.set_neighbor_staging(mode)
+        assert cuda_ctx.neighbor_staging() == mode
+    for bad in (3, -2):
         with pytest.raises(sr.InvalidArgument):
             cuda_ctx.set_neighbor_staging(bad)
     cuda_ctx.set_neighbor_staging(-1)
     assert cuda_ctx.neighbor_staging() == builtin
+
+
+# ---- the flat neighbour walk (each lane's ranges as one list, f32x2) ----------
+
+FLAT = 2
+
+
+@pytest.mark.parametrize("case", ["georef_centroids", "dense", "shapes", "include_self"])
+def test_flat_walk_against_fp64_oracle(cuda_ctx, case):
+    # Same neighbour sets as the other walks (exact counts, shell counts), and
+    # normals within the bar of the FP64 oracle; columns out of reach are
+    # skipped without losing a neighbour or a shell point.
+    inc = case == "include_self"
+    if case in ("georef_centroids", "include_self"):
+        c = synthetic.georef_scan(400_000, seed=11)
+        v = oracle.voxel_centroid(c.x, c.y, c.z, leaf=0.1)
+        x, y, z, r, vp = v.x, v.y, v.z, 0.5, (0, 0, 100)
+    elif case == "dense":  # ~2,000 neighbours per point, 3-D: every column in reach
+        p = np.random.default_rng(12).uniform(0, 2, (30_000, 3)).astype(np.float32)
+        x, y, z, r, vp = p[:, 0], p[:, 1], p[:, 2], 0.5, None
+    else:
+        c = synthetic.shapes_scene(300_000, seed=13)
+        x, y, z, r, vp = c.x, c.y, c.z, 0.3, (50, 50, 150)
+    a = normals_with(cuda_ctx, x, y, z, 0, radius=r, viewpoint=vp, include_self=inc)
+    b = normals_with(cuda_ctx, x, y, z, FLAT, radius=r, viewpoint=vp, include_self=inc)
+    assert np.array_equal(a[4], b[4])  # neighbour counts
+    assert a[5] == b[5] or all(a[5][k] == b[5][k] for k in ("valid_count", "invalid_count",
+                                                             "shell_points"))
+    ref = oracle.radius_normals_fp64(x, y, z, r, 3, vp, include_self=inc)
+    normal_parity.check_against_fp64(*b[:5], ref, x, y, z, vp, b[5], include_self=inc,
+                                     ill_max=5e-3, label=f"flat {case}")
+
+
+def test_flat_walk_batch_equals_alone(cuda_ctx):
+    import torch
+    rng = np.random.default_rng(78)
+    clouds = [synthetic.georef_scan(int(n), seed=200 + i, offset=rng.uniform(0, 1e6, 3))
+              for i, n in enumerate([30_000, 120_000, 7, 64_000])]
+    leaves = [0.1, 0.05, 0.1, 0.2]
+    radii = [5 * l for l in leaves]
+    cols = [np.concatenate([getattr(c, k) for c in clouds]) for k in ("x", "y", "z", "intensity")]
+    dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in cols]
+    offsets = np.concatenate([[0], np.cumsum([c.n for c in clouds])]).astype(np.int64)
+    keep = _native._Keep()
+    pts = _native.make_cloud(dev[0], dev[1], dev[2], [dev[3]], keep)
+    ctx = _native.Context(0)
+    ctx.set_neighbor_staging(FLAT)
+    ctx.batch_voxel_normals_enqueue(pts, offsets, leaves, radii, 3, [(0.0, 0.0, 100.0)] * 4)
+    voff = ctx.batch_voxel_offsets()
+    out = ctx.frame_fetch(int(offsets[-1]), n_attrs=1)
+    for b, c in enumerate(clouds):
+        ref = ctx.voxel_normals(c.x, c.y, c.z, [c.intensity], leaf=leaves[b], radius=radii[b],
+                                viewpoint=(0.0, 0.0, 100.0))
+        a_, e_ = int(voff[b]), int(voff[b + 1])
+        for k in ("nx", "ny", "nz", "curvature", "neighbor_counts"):
+            assert np.array_equal(out[k][a_:e_], ref[k], equal_nan=True), f"cloud {b}: {k}"
+    ctx.close()
+
+
+def test_flat_walk_plane_covariances(cuda_ctx):
+    c = synthetic.georef_scan(300_000, seed=16)
+    a = cuda_ctx.plane_covariances(c.x, c.y, c.z, 0.3, 1e-3)
+    cuda_ctx.set_neighbor_staging(FLAT)
+    try:
+        b = cuda_ctx.plane_covariances(c.x, c.y, c.z, 0.3, 1e-3)
+    finally:
+        cuda_ctx.set_neighbor_staging(-1)
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    fb = np.all(a[:, 3:] == 0, axis=1) & np.all(a[:, :3] == a[:, :1], axis=1)
+    assert np.array_equal(fb, np.all(b[:, 3:] == 0, axis=1) & np.all(b[:, :3] == b[:, :1], axis=1))
+    assert np.max(np.abs(a - b)) <= 2e-4

@@ -304,3 +304,20 @@ def test_approximate_first_xyzinormal():
     assert out.field("intensity").tolist() == [F(0.2), F(10.0)]
     assert out.field("normal_y").tolist() == [0.0, 1.0]
     assert out.field("normal_z").tolist() == [1.0, 0.0]
+
+
+def test_voxel_centroid_enqueue_matches_sync(cuda_ctx):
+    # the voxel stage alone, device-resident, against the synchronous call
+    import torch
+    c = synthetic.georef_scan(250_000, seed=14)
+    sync_cols, _, sync_counts = cuda_ctx.voxel_centroid(c.x, c.y, c.z, [c.intensity], leaf=0.1)
+    dev = [torch.from_numpy(a).cuda() for a in (c.x, c.y, c.z, c.intensity)]
+    keep = _native._Keep()
+    cloud = _native.make_cloud(dev[0], dev[1], dev[2], [dev[3]], keep)
+    cuda_ctx.voxel_centroid_enqueue(cloud, 0.1)
+    v, _ = cuda_ctx.frame_check()
+    assert v == len(sync_counts)
+    got = cuda_ctx.frame_fetch(c.n, n_attrs=1)
+    assert np.array_equal(got["counts"], sync_counts)
+    for a, b in zip(got["columns"], sync_cols):
+        assert np.array_equal(a, b)
