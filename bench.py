@@ -408,13 +408,28 @@ def run_gpu(args):
             c.voxel_normals_enqueue(dcloud, leaf, None, RADIUS, 3, VIEWPOINT, count_shell=False)
         torch.cuda.synchronize()
         passes.append([c.profile_read(reset=True) for c in ctxs])
+    # the voxel stage of each leaf alone (srcu_voxel_centroid_enqueue), one pair
+    # of CUDA events around the whole stage, L2 flushed before each, median of
+    # PROFILE_PASSES
+    voxel_chain_ms = []
+    for c, leaf in zip(ctxs, LEAVES):
+        c.profile_enable([])  # no events inside the timed stage
+        ms = []
+        for _ in range(PROFILE_PASSES + 1):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            c.voxel_centroid_enqueue(dcloud, leaf)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        voxel_chain_ms.append(statistics.median(ms[1:]))
+        c.frame_check()
+        c.profile_read(reset=True)
     for c, s in zip(ctxs, leaf_streams):
         c.set_stream(s.cuda_stream)
     group_ms = {g: statistics.median(sum(p[g]["total_ms"] for p in ps) for ps in passes)
                 for g in _native.KERNEL_IDS}  # ms per step (both leaves)
-    # the voxel chain of each leaf alone: kernel time of its groups, median over passes
-    voxel_chain_ms = [statistics.median(sum(ps[k][g]["total_ms"] for g in VOXEL_GROUPS)
-                                        for ps in passes) for k in range(len(LEAVES))]
     iso_group = {g: (group_ms[g], sum(p[g]["timed_regions"] for p in passes[0]))
                  for g in _native.KERNEL_IDS}  # (ms, launches) per step
     dominant = max(group_ms, key=group_ms.get)
@@ -501,8 +516,9 @@ def run_gpu(args):
                      split_ms={g: round(statistics.median(ps[k][g]["total_ms"] for ps in passes), 4)
                                for g in VOXEL_GROUPS})
                 for k, (leaf, i, b, ms) in enumerate(zip(LEAVES, infos, vox_bytes, voxel_chain_ms))],
-        timing=("each leaf's voxel chain alone (the isolated profile passes): CUDA events around "
-                "each of its kernel groups, summed, median over the passes"),
+        timing=("each leaf's voxel stage alone (srcu_voxel_centroid_enqueue: bounds, plan, sort, "
+                "segments): one pair of CUDA events around it, L2 flushed before, median of "
+                f"{PROFILE_PASSES}; split_ms: the isolated profile passes' per-group events"),
         byte_model="16 B/point read + 28 B/voxel written")
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
