@@ -87,6 +87,8 @@ def parse():
     ap.add_argument("--serving-rates", default="100,500,1000,2000",
                     help="offered request rates (req/s) of the serving measurement")
     ap.add_argument("--serving-seconds", type=float, default=2.0)
+    ap.add_argument("--neighbor-walk", type=int, default=-1, choices=[-1, 0, 1, 2],
+                    help="the normals kernel's neighbour walk (-1: the built-in choice)")
     return ap.parse_args()
 
 
@@ -314,6 +316,7 @@ def algorithmic_bytes(group: str, info: dict, n_attrs: int = 1) -> float:
 def summary(line: dict) -> dict:
     """The line's key figures, printed last (a reader of the line's tail sees them)."""
     out = dict(value=round(line["value"], 1), e2e=round(line["e2e"]["value"], 1),
+               e2e_one_step_in_flight=round(line["e2e_one_step_in_flight"]["value"], 1),
                e2e_pageable=round(line["e2e_pageable"]["value"], 1),
                roofline_frac=round(line["roofline"]["frac"], 4),
                roofline_voxel_frac=[round(x["frac"], 4) for x in line["roofline_voxel"]["leaves"]])
@@ -363,6 +366,7 @@ def run_gpu(args):
         [torch.cuda.Stream(dev) for _ in LEAVES]
     for c, s in zip(ctxs, leaf_streams):
         c.set_stream(s.cuda_stream)
+        c.set_neighbor_staging(args.neighbor_walk)
     cols = [torch.from_numpy(a).to(dev) for a in (cloud.x, cloud.y, cloud.z, cloud.intensity)]
     keep = _native._Keep()
     dcloud = _native.make_cloud(cols[0], cols[1], cols[2], [cols[3]], keep)
@@ -474,6 +478,7 @@ def run_gpu(args):
     # end to end through the C ABI with pinned host buffers, then with plain
     # (pageable) numpy buffers as a Rust caller's Vecs are
     e2e = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream)
+    e2e_one_step = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, inflight=1)
     e2e_pageable = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=False)
 
     peaks = {}
@@ -529,10 +534,12 @@ def run_gpu(args):
                      sort_passes=[[i["voxel_sort_passes"], i["cell_sort_passes"]] for i in infos],
                      normals=[{k: st[k] for k in ("valid_count", "invalid_count", "fp64_eigensolves")}
                               for st in nstats],
+                     neighbor_walk=ctxs[0].neighbor_staging(),
                      l2="flushed by a 256 MB write before every timed step (outside the events)",
                      leaf_chains=("one stream, one after the other" if args.serial_leaves else
                                   "two streams (one context each), forked and joined every step")),
-        e2e=e2e, e2e_pageable=e2e_pageable, roofline=roofline, roofline_voxel=roofline_voxel,
+        e2e=e2e, e2e_one_step_in_flight=e2e_one_step, e2e_pageable=e2e_pageable,
+        roofline=roofline, roofline_voxel=roofline_voxel,
         clocks=clock, gpu_launches=int(launches),
     )
     if not args.no_batched:
@@ -1140,22 +1147,37 @@ def run_serving(args, device):
     return out
 
 
-def run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=True):
+E2E_INFLIGHT = 2  # steps in flight in the e2e measurement
+
+
+def run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=True,
+            inflight=E2E_INFLIGHT):
     """Synchronous srcu_voxel_normals calls with host inputs and outputs, one
-    call per leaf: pinned buffers, or (pinned=False) plain numpy arrays in
-    pageable memory, as the reference's Rust arm passes its Vecs.  Unless
-    --serial-leaves, the two calls of a step are made from two host threads on
-    their own contexts and streams, so one call's transfers overlap the other's
-    kernels.  Device time: every leaf stream waits on the start event, and the
-    timing stream joins them all before the end event."""
+    call per leaf and step: pinned buffers, or (pinned=False) plain numpy arrays
+    in pageable memory, as the reference's Rust arm passes its Vecs.  `inflight`
+    steps run at once, as a caller with a stream of clouds would run them: one
+    host thread per (slot, leaf), each on its own context and stream with its
+    own output buffers, slot s taking steps s, s + inflight, ...; every call
+    copies its inputs to the device and its results back inside the timed
+    region (--serial-leaves: one thread, one step at a time).  Device time:
+    every stream waits on the start event, and the timing stream joins them all
+    before the end event."""
     import threading
 
     from spatialrust_b200 import _native
     lib = _native.load()
     serial = args.serial_leaves
-    streams = [stream] * len(LEAVES) if serial else leaf_streams
-    for c, s in zip(ctxs, streams):
-        c.set_stream(s.cuda_stream)
+    if serial:
+        inflight = 1
+    slots = max(1, inflight)
+    slot_ctxs = [list(ctxs)] + [[_native.Context(dev.index) for _ in LEAVES]
+                                for _ in range(slots - 1)]
+    slot_streams = [([stream] * len(LEAVES) if serial else list(leaf_streams))] + [
+        [torch.cuda.Stream(dev) for _ in LEAVES] for _ in range(slots - 1)]
+    for cs, ss in zip(slot_ctxs, slot_streams):
+        for c, st in zip(cs, ss):
+            c.set_stream(st.cuda_stream)
+            c.set_neighbor_staging(args.neighbor_walk)
     n = cloud.n
 
     def host(a):  # a torch CPU tensor: pinned, or a view of a pageable numpy array
@@ -1166,61 +1188,65 @@ def run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=True):
     attr_in = keep.add((ctypes.c_void_p * 1)(pin[3].data_ptr()))
     hcloud = _native.SrcuCloud(pin[0].data_ptr(), pin[1].data_ptr(), pin[2].data_ptr(),
                                ctypes.cast(attr_in, ctypes.c_void_p), 1, 0, n)
-    outs = []
-    for _ in LEAVES:
-        vcols = [host(torch.empty(n, dtype=torch.float32)) for _ in range(4)]
-        ncols = [host(torch.empty(n, dtype=torch.float32)) for _ in range(4)]
-        attr_out = keep.add((ctypes.c_void_p * 1)(vcols[3].data_ptr()))
-        # the reference's output schema: centroid columns and the four normal
-        # columns (no per-voxel or neighbour counts)
-        vout = _native.SrcuVoxelOut(vcols[0].data_ptr(), vcols[1].data_ptr(), vcols[2].data_ptr(),
-                                    ctypes.cast(attr_out, ctypes.c_void_p), 0, 0, 0)
-        nout = _native.SrcuNormalOut(*[c.data_ptr() for c in ncols], 0, 0)
-        outs.append((vcols, ncols, vout, nout))
+    outs = {}
+    for sl in range(slots):
+        for k in range(len(LEAVES)):
+            vcols = [host(torch.empty(n, dtype=torch.float32)) for _ in range(4)]
+            ncols = [host(torch.empty(n, dtype=torch.float32)) for _ in range(4)]
+            attr_out = keep.add((ctypes.c_void_p * 1)(vcols[3].data_ptr()))
+            # the reference's output schema: centroid columns and the four normal
+            # columns (no per-voxel or neighbour counts)
+            vout = _native.SrcuVoxelOut(vcols[0].data_ptr(), vcols[1].data_ptr(),
+                                        vcols[2].data_ptr(), ctypes.cast(attr_out, ctypes.c_void_p),
+                                        0, 0, 0)
+            nout = _native.SrcuNormalOut(*[c.data_ptr() for c in ncols], 0, 0)
+            outs[sl, k] = (vcols, ncols, vout, nout, ctypes.c_uint64(0), _native.SrcuNormalStats())
     params = [(_native._voxel_params(leaf, None),
                _native._normal_params(RADIUS, 3, VIEWPOINT, False, count_shell=False))
               for leaf in LEAVES]
-    nvs = [ctypes.c_uint64(0) for _ in LEAVES]
-    stats = [_native.SrcuNormalStats() for _ in LEAVES]
     voxels = [0] * len(LEAVES)
     errors = []
 
-    def call(k):
+    def call(sl, k):
         vp, np_ = params[k]
-        st = lib.srcu_voxel_normals(ctxs[k].handle, ctypes.byref(hcloud), ctypes.byref(vp),
-                                    ctypes.byref(np_), ctypes.byref(outs[k][2]),
-                                    ctypes.byref(outs[k][3]), ctypes.byref(nvs[k]),
-                                    ctypes.byref(stats[k]))
+        _, _, vout, nout, nv, stats = outs[sl, k]
+        st = lib.srcu_voxel_normals(slot_ctxs[sl][k].handle, ctypes.byref(hcloud),
+                                    ctypes.byref(vp), ctypes.byref(np_), ctypes.byref(vout),
+                                    ctypes.byref(nout), ctypes.byref(nv), ctypes.byref(stats))
         if st != 0:
-            errors.append((k, st))
-        voxels[k] = int(nvs[k].value)
+            errors.append((sl, k, st))
+        voxels[k] = int(nv.value)
 
-    def step():
+    def run(steps):
         if serial:
-            for k in range(len(LEAVES)):
-                call(k)
+            for _ in range(steps):
+                for k in range(len(LEAVES)):
+                    call(0, k)
         else:
-            ths = [threading.Thread(target=call, args=(k,)) for k in range(len(LEAVES))]
+            def worker(sl, k):
+                for _ in range(sl, steps, slots):
+                    call(sl, k)
+            ths = [threading.Thread(target=worker, args=(sl, k))
+                   for sl in range(slots) for k in range(len(LEAVES))]
             for t in ths:
                 t.start()
             for t in ths:
                 t.join()
         if errors:
-            k, st = errors[0]
-            ctxs[k]._check(st)
+            sl, k, st = errors[0]
+            slot_ctxs[sl][k]._check(st)
 
-    for _ in range(max(args.warmup, 3)):
-        step()
+    run(max(args.warmup, 3) * slots)
     torch.cuda.synchronize()
-    steps = max(args.steps // 2, 3)
+    steps = max(args.steps, 3 * slots)
+    all_streams = {s for ss in slot_streams for s in ss}
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
-    for s in set(streams):
+    for s in all_streams:
         if s is not stream:
             s.wait_event(start)
-    for _ in range(steps):
-        step()
-    for s in set(streams):
+    run(steps)
+    for s in all_streams:
         if s is not stream:
             done = torch.cuda.Event()
             done.record(s)
@@ -1228,13 +1254,20 @@ def run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=True):
     end.record(stream)
     torch.cuda.synchronize()
     ms = start.elapsed_time(end) / steps
+    for cs in slot_ctxs[1:]:
+        for c in cs:
+            c.close()
+    for c, st in zip(ctxs, leaf_streams):
+        c.set_stream(st.cuda_stream)
     h2d = len(LEAVES) * n * 16
     d2h = sum(v * (16 + 16) for v in voxels)
     return dict(value=N_POINTS / (ms / 1e3) / 1e6, unit=UNIT, ms_per_step=ms,
-                h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h,
+                h2d_bytes_per_step=h2d, d2h_bytes_per_step=d2h, steps_in_flight=slots,
                 api=("srcu_voxel_normals (include/srcuda.h), "
                      + ("pinned" if pinned else "pageable (plain numpy)") + " host buffers, one "
-                     "call per leaf" + ("" if serial else ", the two calls from two host threads")))
+                     "call per leaf and step" + ("" if serial else
+                                                 f", {slots} steps in flight from "
+                                                 f"{slots * len(LEAVES)} host threads")))
 
 
 def main():

@@ -8,9 +8,9 @@ large ones want long tiles that amortise the per-tile look-back.  This module
 measures every shape on the real chain -- voxel centroid (voxel-key sort over
 the input points) then radius normals (cell-key sort over the centroids) on a
 georeferenced scan -- at one input size per size class, and picks per class
-the shape with the least sort time.  Digit width stays at 8 bits: one digit
-bin per thread of a 256-thread block is what the ranking and the look-back
-are laid out for.  It also times the normals kernel's three neighbour walks
+the shape with the least sort time.  The shapes cover keys per thread, blocks
+per SM and threads per block (256 or 512: the first 256 threads own one digit
+each).  Digit width stays at 8 bits.  It also times the normals kernel's three neighbour walks
 (range by range through L1, range by range from shared memory filled by bulk
 copies, each lane's ranges as one list with packed f32x2 arithmetic) over the
 same sizes and keeps the fastest.
@@ -188,7 +188,8 @@ def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> s
         lines.append("// Measured sort ms (georeferenced scan, leaf "
                      f"{LEAF}, radius {RADIUS}; L2 flushed before every chain):")
         cfgs = result["configs"]
-        shapes = "  ".join(f"{c['items_per_thread']:>4}x{c['blocks_per_sm']}" for c in cfgs)
+        shapes = "  ".join(f"{c['items_per_thread']:>2}x{c['blocks_per_sm']}x{c.get('threads_per_block', 256)}"
+                           for c in cfgs)
         for kind in ("voxel", "cell"):
             lines.append(f"//   {kind}-key sort     points  {shapes}")
             for keys, ms in samples(result, kind):

@@ -43,19 +43,19 @@ struct OnesweepTileSmem {
   uint32_t vals[TILE];
 };
 
-// Shared memory of one sort block for tiles of TILE keys.
-template <int TILE>
+// Shared memory of one sort block of WARPS warps for tiles of TILE keys.
+template <int TILE, int WARPS = OS_WARPS>
 struct OnesweepSmemT {
   union {
     OnesweepTileSmem<TILE> tile;
     uint32_t hist[HIST_COPIES][MAX_DIGITS][RADIX_BINS];
   } u;
-  uint32_t whist[OS_WARPS][RADIX_BINS];
-  uint32_t match[OS_WARPS][RADIX_BINS];  // per-warp peer masks, zero between uses
+  uint32_t whist[WARPS][RADIX_BINS];
+  uint32_t match[WARPS][RADIX_BINS];  // per-warp peer masks, zero between uses
   uint32_t digit_start[RADIX_BINS];
   uint32_t tile_excl[RADIX_BINS];
   uint32_t gbase[RADIX_BINS];
-  uint32_t scratch[OS_WARPS];
+  uint32_t scratch[WARPS];
   uint32_t trivial[MAX_DIGITS];
   uint32_t active[MAX_DIGITS];
   uint32_t num_active;
@@ -63,13 +63,15 @@ struct OnesweepSmemT {
 };
 using OnesweepSmem = OnesweepSmemT<OS_TILE>;
 
-// The sort's launch shapes the library is built with: keys per thread and the
-// blocks per SM the registers are capped for (8-bit digits throughout).  The
-// autotuner picks among them per input size (srcu_set_sort_tuning).
-constexpr int SORT_CONFIGS = 4;
-constexpr int kSortItems[SORT_CONFIGS] = {16, 8, 12, 8};
-constexpr int kSortMinBlocks[SORT_CONFIGS] = {2, 3, 3, 4};
-constexpr int SORT_MIN_ITEMS = 8;  // the smallest tile sizes the look-back buffer
+// The sort's launch shapes the library is built with: keys per thread, the
+// blocks per SM the registers are capped for, and threads per block (8-bit
+// digits throughout: the first 256 threads of a block own one digit each).
+// The autotuner picks among them per input size (srcu_set_sort_tuning).
+constexpr int SORT_CONFIGS = 6;
+constexpr int kSortItems[SORT_CONFIGS] = {16, 8, 12, 8, 8, 12};
+constexpr int kSortMinBlocks[SORT_CONFIGS] = {2, 3, 3, 4, 2, 1};
+constexpr int kSortThreads[SORT_CONFIGS] = {256, 256, 256, 256, 512, 512};
+constexpr int SORT_MIN_TILE = 2048;  // the smallest tile (keys) the look-back buffer is sized for
 
 // Ping-pong buffers of one sort.
 struct SortBuffers {
@@ -139,14 +141,16 @@ __device__ __forceinline__ void grid_barrier(SortState *st, uint32_t *status) {
   __syncthreads();
 }
 
-template <class Src, int ITEMS = OS_ITEMS, int MINB = 2>
-__global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl, uint32_t *hist,
-                                                        SortBuffers buf, uint32_t epoch_off,
-                                                        int work_slot, SortState *st) {
-  constexpr int TILE = OS_THREADS * ITEMS;
+template <class Src, int ITEMS = OS_ITEMS, int MINB = 2, int THREADS = OS_THREADS>
+__global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, uint32_t *hist,
+                                                     SortBuffers buf, uint32_t epoch_off,
+                                                     int work_slot, SortState *st) {
+  static_assert(THREADS >= RADIX_BINS && THREADS % 32 == 0, "a thread per digit at least");
+  constexpr int WARPS = THREADS / 32;
+  constexpr int TILE = THREADS * ITEMS;
   constexpr int WARP_ITEMS = ITEMS * 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  OnesweepSmemT<TILE> &sm = *reinterpret_cast<OnesweepSmemT<TILE> *>(smem_raw);
+  OnesweepSmemT<TILE, WARPS> &sm = *reinterpret_cast<OnesweepSmemT<TILE, WARPS> *>(smem_raw);
   if (ld_relaxed_u32(&ctl->status)) return;  // before any barrier: every block agrees
   src.prepare(ctl);
   const uint32_t n = src.count(ctl);
@@ -156,11 +160,12 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
   const bool packed = kbits + idx_bits <= 64;
   const uint32_t shift0 = packed ? idx_bits : 0u;
   const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
+  const bool owner = t < RADIX_BINS;  // this thread owns digit t in the per-digit steps
 
   // ---- phase 1: digit histograms ----------------------------------------
-  for (uint32_t i = t; i < HIST_COPIES * MAX_DIGITS * RADIX_BINS; i += OS_THREADS)
+  for (uint32_t i = t; i < HIST_COPIES * MAX_DIGITS * RADIX_BINS; i += THREADS)
     (&sm.u.hist[0][0][0])[i] = 0;
-  for (uint32_t i = t; i < OS_WARPS * RADIX_BINS; i += OS_THREADS) (&sm.match[0][0])[i] = 0;
+  for (uint32_t i = t; i < WARPS * RADIX_BINS; i += THREADS) (&sm.match[0][0])[i] = 0;
   __syncthreads();
   {
     // The keys are computed once, here, and kept in the ping-pong buffer that
@@ -168,14 +173,14 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
     // them like any pass's output.
     uint32_t(*h)[RADIX_BINS] = sm.u.hist[warp & (HIST_COPIES - 1)];
     uint64_t *kcache = buf.keys[1];
-    for (uint32_t i = blockIdx.x * OS_THREADS + t; i < n; i += gridDim.x * OS_THREADS) {
+    for (uint32_t i = blockIdx.x * THREADS + t; i < n; i += gridDim.x * THREADS) {
       const uint64_t k = src.key(i);
       kcache[i] = k;
       for (uint32_t d = 0; d < nd; ++d) atomicAdd(&h[d][uint32_t(k >> (RADIX_BITS * d)) & 0xffu], 1u);
     }
   }
   __syncthreads();
-  for (uint32_t i = t; i < nd * RADIX_BINS; i += OS_THREADS) {
+  for (uint32_t i = t; i < nd * RADIX_BINS; i += THREADS) {
     uint32_t c = 0;
 #pragma unroll
     for (int cp = 0; cp < HIST_COPIES; ++cp) c += (&sm.u.hist[cp][0][0])[i];
@@ -187,8 +192,9 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
   // ---- which digits need a pass ----------------------------------------
   if (t < MAX_DIGITS) sm.trivial[t] = 0;
   __syncthreads();
-  for (uint32_t d = 0; d < nd; ++d)
-    if (ld_relaxed_u32(&hist[d * RADIX_BINS + t]) == n) sm.trivial[d] = 1;
+  if (owner)
+    for (uint32_t d = 0; d < nd; ++d)
+      if (ld_relaxed_u32(&hist[d * RADIX_BINS + t]) == n) sm.trivial[d] = 1;
   __syncthreads();
   if (t == 0) {
     uint32_t na = 0;
@@ -214,8 +220,9 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
     const uint32_t shift = shift0 + sm.active[p] * RADIX_BITS;
     {
       uint32_t total;
-      sm.digit_start[t] = block_exclusive_sum<OS_THREADS>(
-          ld_relaxed_u32(&hist[sm.active[p] * RADIX_BINS + t]), sm.scratch, &total);
+      const uint32_t ds = block_exclusive_sum<THREADS>(
+          owner ? ld_relaxed_u32(&hist[sm.active[p] * RADIX_BINS + t]) : 0u, sm.scratch, &total);
+      if (owner) sm.digit_start[t] = ds;
     }
     const bool from_src = p == 0;
     const uint64_t *kin = buf.keys[(p + 1) & 1];
@@ -227,7 +234,7 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
 
     for (;;) {
       if (t == 0) sm.tile = atomicAdd(ctr, 1u);
-      for (uint32_t i = t; i < OS_WARPS * RADIX_BINS; i += OS_THREADS) (&sm.whist[0][0])[i] = 0;
+      for (uint32_t i = t; i < WARPS * RADIX_BINS; i += THREADS) (&sm.whist[0][0])[i] = 0;
       __syncthreads();
       const uint32_t tile = sm.tile;
       if (tile >= num_tiles) break;
@@ -290,18 +297,20 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
       __syncthreads();
       // Thread t owns digit t: exclusive prefix over warps, tile count.
       uint32_t cnt = 0;
-#pragma unroll
-      for (int w = 0; w < OS_WARPS; ++w) {
-        const uint32_t c = sm.whist[w][t];
-        sm.whist[w][t] = cnt;
-        cnt += c;
-      }
-      // Publish the tile aggregate as early as possible.
       uint64_t *lb_mine = buf.lookback + size_t(tile) * RADIX_BINS + t;
-      st_relaxed(lb_mine, lb_pack(epoch, tile == 0 ? LB_INC : LB_AGG, cnt));
+      if (owner) {
+#pragma unroll
+        for (int w = 0; w < WARPS; ++w) {
+          const uint32_t c = sm.whist[w][t];
+          sm.whist[w][t] = cnt;
+          cnt += c;
+        }
+        // Publish the tile aggregate as early as possible.
+        st_relaxed(lb_mine, lb_pack(epoch, tile == 0 ? LB_INC : LB_AGG, cnt));
+      }
       uint32_t tile_total;
-      const uint32_t texcl = block_exclusive_sum<OS_THREADS>(cnt, sm.scratch, &tile_total);
-      sm.tile_excl[t] = texcl;
+      const uint32_t texcl = block_exclusive_sum<THREADS>(cnt, sm.scratch, &tile_total);
+      if (owner) sm.tile_excl[t] = texcl;
       __syncthreads();
       // Scatter to shared memory in digit order.
 #pragma unroll
@@ -316,7 +325,7 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
       // Resolve the look-back for digit t, LB_WIDTH predecessors per step
       // (independent loads, one latency), stopping at the first inclusive.
       uint32_t excl = 0;
-      if (tile > 0) {
+      if (owner && tile > 0) {
         int64_t j = int64_t(tile) - 1;
         uint32_t spins = 0;
         bool done = false;
@@ -347,10 +356,10 @@ __global__ void __launch_bounds__(OS_THREADS, MINB) k_sort(Src src, Control *ctl
         }
         st_relaxed(lb_mine, lb_pack(epoch, LB_INC, excl + cnt));
       }
-      sm.gbase[t] = sm.digit_start[t] + excl - texcl;
+      if (owner) sm.gbase[t] = sm.digit_start[t] + excl - texcl;
       __syncthreads();
       const uint32_t tile_n = min(uint32_t(TILE), n - base);
-      for (uint32_t j = t; j < tile_n; j += OS_THREADS) {
+      for (uint32_t j = t; j < tile_n; j += THREADS) {
         const uint64_t kk = sm.u.tile.keys[j];
         const uint32_t pos = sm.gbase[uint32_t(kk >> shift) & 0xffu] + j;
         if (pos < n) {

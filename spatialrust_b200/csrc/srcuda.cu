@@ -257,8 +257,7 @@ srcu_status reserve(srcu_ctx *ctx, uint64_t n, uint32_t cols, bool host_input, b
   ST_TRY(ensure(ctx, ctx->vals[0], m * 4));
   ST_TRY(ensure(ctx, ctx->vals[1], m * 4));
   // look-back words for the smallest tile any sort launch shape uses
-  ST_TRY(ensure(ctx, ctx->lb_sort,
-                size_t(ceil_div(m, OS_THREADS * SORT_MIN_ITEMS)) * RADIX_BINS * 8, true));
+  ST_TRY(ensure(ctx, ctx->lb_sort, size_t(ceil_div(m, SORT_MIN_TILE)) * RADIX_BINS * 8, true));
   ST_TRY(ensure(ctx, ctx->in_aos, m * 16));
   if (voxel) {
     ST_TRY(ensure(ctx, ctx->vaos, m * 16));
@@ -478,7 +477,9 @@ template <class Src, int C>
 cudaError_t launch_sort_config(cudaStream_t stream, uint32_t grid_cap, const Src &src,
                                Control *ctl, uint32_t *hist, const SortBuffers &sb,
                                uint32_t epoch_off, int work_slot, SortState *st, uint64_t n_max) {
-  constexpr int TILE = OS_THREADS * kSortItems[C];
+  constexpr int THREADS = kSortThreads[C];
+  constexpr int TILE = THREADS * kSortItems[C];
+  static_assert(TILE >= SORT_MIN_TILE, "the look-back buffer is sized for SORT_MIN_TILE");
   const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, TILE));
   const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(tiles, grid_cap));
   Src s = src;
@@ -490,30 +491,34 @@ cudaError_t launch_sort_config(cudaStream_t stream, uint32_t grid_cap, const Src
   SortState *ss = st;
   void *args[] = {&s, &c, &h, &b, &e, &w, &ss};
   return cudaLaunchCooperativeKernel(
-      reinterpret_cast<const void *>(&k_sort<Src, kSortItems[C], kSortMinBlocks[C]>), dim3(grid),
-      dim3(OS_THREADS), args, sizeof(OnesweepSmemT<TILE>), stream);
+      reinterpret_cast<const void *>(&k_sort<Src, kSortItems[C], kSortMinBlocks[C], THREADS>),
+      dim3(grid), dim3(THREADS), args, sizeof(OnesweepSmemT<TILE, THREADS / 32>), stream);
 }
 
 template <class Src, int C>
 cudaError_t sort_config_setup(int *occ) {
-  constexpr int TILE = OS_THREADS * kSortItems[C];
-  const void *kern = reinterpret_cast<const void *>(&k_sort<Src, kSortItems[C], kSortMinBlocks[C]>);
+  constexpr int THREADS = kSortThreads[C];
+  constexpr int TILE = THREADS * kSortItems[C];
+  using Smem = OnesweepSmemT<TILE, THREADS / 32>;
+  const void *kern =
+      reinterpret_cast<const void *>(&k_sort<Src, kSortItems[C], kSortMinBlocks[C], THREADS>);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(sizeof(OnesweepSmemT<TILE>)));
+                                       int(sizeof(Smem)));
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, OS_THREADS,
-                                                    sizeof(OnesweepSmemT<TILE>));
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, THREADS, sizeof(Smem));
   *occ = std::max(1, *occ);
   return e;
 }
 
 template <class Src>
 cudaError_t sort_setup(int (&occ)[SORT_CONFIGS]) {
-  static_assert(SORT_CONFIGS == 4, "one setup per launch shape");
+  static_assert(SORT_CONFIGS == 6, "one setup per launch shape");
   cudaError_t e = sort_config_setup<Src, 0>(&occ[0]);
   if (e == cudaSuccess) e = sort_config_setup<Src, 1>(&occ[1]);
   if (e == cudaSuccess) e = sort_config_setup<Src, 2>(&occ[2]);
   if (e == cudaSuccess) e = sort_config_setup<Src, 3>(&occ[3]);
+  if (e == cudaSuccess) e = sort_config_setup<Src, 4>(&occ[4]);
+  if (e == cudaSuccess) e = sort_config_setup<Src, 5>(&occ[5]);
   return e;
 }
 
@@ -555,6 +560,12 @@ srcu_status launch_sort_tuned(srcu_ctx *ctx, int kind, const Src &src, uint64_t 
       break;
     case 3:
       e = launch_sort_config<Src, 3>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
+      break;
+    case 4:
+      e = launch_sort_config<Src, 4>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
+      break;
+    case 5:
+      e = launch_sort_config<Src, 5>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
       break;
     default:
       e = launch_sort_config<Src, 0>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
@@ -1006,7 +1017,7 @@ int srcu_sort_configs(srcu_sort_config *out, int max_entries) {
     out[c].items_per_thread = uint32_t(kSortItems[c]);
     out[c].blocks_per_sm = uint32_t(kSortMinBlocks[c]);
     out[c].digit_bits = RADIX_BITS;
-    out[c].threads_per_block = OS_THREADS;
+    out[c].threads_per_block = uint32_t(kSortThreads[c]);
   }
   return SORT_CONFIGS;
 }
