@@ -499,7 +499,7 @@ __device__ __forceinline__ bool column_out_of_reach(int k, const double (&lo)[2]
 // Covariance from moments about the query (S: sx sy sz sxx syy szz sxy sxz syz
 // over n points) and its smallest eigenpair, FP64.
 __device__ __forceinline__ Eig3 eig_from_moments(const double (&S)[9], uint32_t n) {
-  const double inv = 1.0 / double(n);
+  const double inv = __drcp_rn(double(n));  // the correctly rounded 1 / n
   const double mx = S[0] * inv, my = S[1] * inv, mz = S[2] * inv;
   const double cxx = S[3] * inv - mx * mx, cyy = S[4] * inv - my * my;
   const double czz = S[5] * inv - mz * mz, cxy = S[6] * inv - mx * my;
@@ -512,7 +512,7 @@ __device__ __forceinline__ Eig3 eig_from_moments(const double (&S)[9], uint32_t 
 // is at least NM_REFINE_GAP of the trace the eigenvector is within ~1e-6 rad.
 // Smaller gaps go to the FP64 path.
 __device__ __forceinline__ Eig3 eig_from_moments_f32(const double (&S)[9], uint32_t n) {
-  const double inv = 1.0 / double(n);
+  const double inv = __drcp_rn(double(n));  // the correctly rounded 1 / n
   const double mx = S[0] * inv, my = S[1] * inv, mz = S[2] * inv;
   const double cxx = S[3] * inv - mx * mx, cyy = S[4] * inv - my * my;
   const double czz = S[5] * inv - mz * mz, cxy = S[6] * inv - mx * my;
@@ -916,24 +916,30 @@ __global__ void __launch_bounds__(NM_THREADS, Walk == WALK_FLAT ? NM_FLAT_MIN_BL
         e = eig_from_moments(S, n_eff);
         ++n_fp64;
       }
-      double v0 = e.v[0], v1 = e.v[1], v2 = e.v[2];
+      // Orientation and normalisation in f32, as the reference computes them
+      // (orient_normal_towards_viewpoint, normal.rs:408-421, with Vec3::dot
+      // and Vec3::normalize, vec.rs:66-100): the unit eigenvector rounded to
+      // f32 moves by ~1e-7 rad at most, and the sign test matches the
+      // reference's own f32 test.
+      float v0 = float(e.v[0]), v1 = float(e.v[1]), v2 = float(e.v[2]);
       if (!PlaneCov && prm.has_viewpoint) {
-        // orient_normal_towards_viewpoint, normal.rs:408-421
-        const double wx = double(prm.vp[0]) - double(qp.x);
-        const double wy = double(prm.vp[1]) - double(qp.y);
-        const double wz = double(prm.vp[2]) - double(qp.z);
-        if (v0 * wx + v1 * wy + v2 * wz < 0.0) {
+        const float wx = __fsub_rn(prm.vp[0], qp.x);
+        const float wy = __fsub_rn(prm.vp[1], qp.y);
+        const float wz = __fsub_rn(prm.vp[2], qp.z);
+        const float dot = __fadd_rn(__fadd_rn(__fmul_rn(v0, wx), __fmul_rn(v1, wy)), __fmul_rn(v2, wz));
+        if (dot < 0.0f) {
           v0 = -v0;
           v1 = -v1;
           v2 = -v2;
         }
       }
-      const double nn = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-      ox = float(v0 / nn);
-      oy = float(v1 / nn);
-      oz = float(v2 / nn);
-      const double sum = e.l0 + e.l1 + e.l2;
-      oc = sum > 0.0 ? float(e.l0 / sum) : 0.0f;
+      const float len =
+          sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(v0, v0), __fmul_rn(v1, v1)), __fmul_rn(v2, v2)));
+      ox = len != 0.0f ? v0 / len : v0;
+      oy = len != 0.0f ? v1 / len : v1;
+      oz = len != 0.0f ? v2 / len : v2;
+      const float sum = float(e.l0 + e.l1 + e.l2);
+      oc = sum > 0.0f ? float(e.l0) / sum : 0.0f;
       ++n_valid;
     } else {
       // include_self: (0, 0, 1) (normals_grid.rs:129-132), turned toward the
