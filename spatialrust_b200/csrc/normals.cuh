@@ -813,56 +813,61 @@ __global__ void __launch_bounds__(NM_THREADS, Walk == WALK_FLAT ? NM_FLAT_MIN_BL
         end = g0.y;
         c = __ldg(pts + cur);
       }
+      // Steps in chunks of NM_FLUSH (warp-uniform), each chunk's f32 partials
+      // then folded into FP64; within a chunk two steps per iteration, so the
+      // candidate prefetched for the next step needs no register moves.
 #pragma unroll 1
-      for (uint32_t t = 0; t < steps; ++t) {
-        if (t < total) {
-          uint32_t nxt = cur + 1;
-          if (nxt == end && li + 1 < nr) {  // on to the next range of the list
-            const uint2 gn = lst[++li][lane];
-            nxt = gn.x;
-            end = gn.y;
+      for (uint32_t t0 = 0; t0 < steps; t0 += NM_FLUSH) {
+        const uint32_t t1 = min(steps, t0 + NM_FLUSH);
+#pragma unroll 2
+        for (uint32_t t = t0; t < t1; ++t) {
+          if (t < total) {
+            uint32_t nxt = cur + 1;
+            if (nxt == end && li + 1 < nr) {  // on to the next range of the list
+              const uint2 gn = lst[++li][lane];
+              nxt = gn.x;
+              end = gn.y;
+            }
+            const float4 cn = t + 1 < total ? __ldg(pts + nxt) : c;  // one candidate ahead
+            // the reference predicate ((dx^2 + dy^2) + dz^2 <= r^2, kdtree.rs:544-549)
+            const uint64_t dxy = f2_sub(f2_pack(c.x, c.y), qxy);
+            const uint64_t pxy = f2_mul(dxy, dxy);
+            float dx, dy, xx, yy;
+            f2_unpack(dxy, dx, dy);
+            f2_unpack(pxy, xx, yy);
+            const float dz = __fsub_rn(c.z, qp.z);
+            const float zz = __fmul_rn(dz, dz);
+            const float d2 = __fadd_rn(__fadd_rn(xx, yy), zz);
+            if (d2 <= r2) {
+              hits += 1.f;
+              a01 = f2_add(a01, dxy);
+              a34 = f2_add(a34, pxy);
+              a78 = f2_fma(dxy, f2_pack(dz, dz), a78);
+              a2 += dz;
+              a5 += zz;
+              a6 = fmaf(dx, dy, a6);
+            }
+            if (CountShell && prm.count_shell && d2 != 0.f && fabsf(__fsub_rn(d2, r2)) <= shell_tol)
+              shell = 1;
+            c = cn;
+            cur = nxt;
           }
-          const float4 cn = t + 1 < total ? __ldg(pts + nxt) : c;  // one candidate ahead
-          // the reference predicate ((dx^2 + dy^2) + dz^2 <= r^2, kdtree.rs:544-549)
-          const uint64_t dxy = f2_sub(f2_pack(c.x, c.y), qxy);
-          const uint64_t pxy = f2_mul(dxy, dxy);
-          float dx, dy, xx, yy;
-          f2_unpack(dxy, dx, dy);
-          f2_unpack(pxy, xx, yy);
-          const float dz = __fsub_rn(c.z, qp.z);
-          const float zz = __fmul_rn(dz, dz);
-          const float d2 = __fadd_rn(__fadd_rn(xx, yy), zz);
-          if (d2 <= r2) {
-            hits += 1.f;
-            a01 = f2_add(a01, dxy);
-            a34 = f2_add(a34, pxy);
-            a78 = f2_fma(dxy, f2_pack(dz, dz), a78);
-            a2 += dz;
-            a5 += zz;
-            a6 = fmaf(dx, dy, a6);
-          }
-          if (CountShell && prm.count_shell && d2 != 0.f && fabsf(__fsub_rn(d2, r2)) <= shell_tol)
-            shell = 1;
-          c = cn;
-          cur = nxt;
         }
-        if ((t & (NM_FLUSH - 1)) == NM_FLUSH - 1 || t + 1 == steps) {  // warp-uniform
-          float v0, v1, v3, v4, v7, v8;
-          f2_unpack(a01, v0, v1);
-          f2_unpack(a34, v3, v4);
-          f2_unpack(a78, v7, v8);
-          S[0] += double(v0);
-          S[1] += double(v1);
-          S[2] += double(a2);
-          S[3] += double(v3);
-          S[4] += double(v4);
-          S[5] += double(a5);
-          S[6] += double(a6);
-          S[7] += double(v7);
-          S[8] += double(v8);
-          a01 = a34 = a78 = 0;
-          a2 = a5 = a6 = 0.f;
-        }
+        float v0, v1, v3, v4, v7, v8;
+        f2_unpack(a01, v0, v1);
+        f2_unpack(a34, v3, v4);
+        f2_unpack(a78, v7, v8);
+        S[0] += double(v0);
+        S[1] += double(v1);
+        S[2] += double(a2);
+        S[3] += double(v3);
+        S[4] += double(v4);
+        S[5] += double(a5);
+        S[6] += double(a6);
+        S[7] += double(v7);
+        S[8] += double(v8);
+        a01 = a34 = a78 = 0;
+        a2 = a5 = a6 = 0.f;
       }
       __syncwarp();  // the lists are rewritten by the next batch
     } else {
