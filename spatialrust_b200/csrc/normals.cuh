@@ -313,10 +313,14 @@ __device__ __forceinline__ int64_t column_lookup(const uint64_t *table, const ui
 // most three) cells are consecutive in key order, so each column is one
 // contiguous range: 9 ranges cover the 27-cell neighbourhood.  One thread per
 // cell: the key is unpacked once; the centre column holds the cell itself
-// (its z neighbours are its key-order neighbours); the other eight columns
-// are probed in the column hash with all eight slot loads in flight at once,
-// then searched from their first cell by galloping over the sorted keys.
-__global__ void __launch_bounds__(256) k_ranges(Control *ctl, const uint64_t *cell_key,
+// (its z neighbours are its key-order neighbours).  The other eight columns
+// are resolved in rounds of independent loads, all eight columns at once:
+// (1) their column-table slots, (2) the keys of each column's first three
+// cells, (3) the two cell starts that bound each range.  A column whose first
+// cell lies below the window (a column with cells under cz - 1) is searched
+// by galloping from its first cell instead; a window holds at most three
+// cells, so three keys from the first cell in the window decide its end.
+__global__ void __launch_bounds__(256, 3) k_ranges(Control *ctl, const uint64_t *cell_key,
                                                 const uint32_t *cell_start, const uint64_t *table,
                                                 uint32_t log2cap, uint2 *ranges, Batch bt) {
   if (ld_relaxed_u32(&ctl->status)) return;
@@ -346,8 +350,8 @@ __global__ void __launch_bounds__(256) k_ranges(Control *ctl, const uint64_t *ce
       if (cz + 1 < dims2 && u + 1 < u_count && cell_key[u + 1] == full + 1) last = u + 1;
       out[4] = make_uint2(cell_start[first], cell_start[last + 1]);
     }
-    // the other eight: column keys and first probes (a dense slot, or the
-    // first hash slot), all loads issued together
+    // round 1: column keys and first probes (a dense slot, or the first hash
+    // slot), all loads issued together
     uint64_t ckey[8];
     uint32_t slot[8];
     uint64_t word[8];
@@ -363,32 +367,54 @@ __global__ void __launch_bounds__(256) k_ranges(Control *ctl, const uint64_t *ce
       slot[k] = uint32_t(idx);
       word[k] = (inside && idx <= tmask) ? table[idx] : 0ull;
     }
+    // first cell of each column (or -1), resolving hash probe chains
+    int64_t f[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const int col = k < 4 ? k : k + 1;
-      uint2 rg = make_uint2(0, 0);
-      int64_t f = -1;
+      f[k] = -1;
       if (dense) {
-        if (ckey[k] != ~0ull && uint32_t(word[k] >> 32) == epoch) f = uint32_t(word[k]);
+        if (ckey[k] != ~0ull && uint32_t(word[k] >> 32) == epoch) f[k] = uint32_t(word[k]);
       } else if (ckey[k] != ~0ull) {
-        // resolve the probe chain from the slot already loaded
         uint32_t h = slot[k];
         uint64_t w = word[k];
         for (uint32_t probe = 0; probe <= tmask; ++probe) {
           if (uint32_t(w >> 32) != epoch) break;
           const uint32_t c = uint32_t(w);
           if ((cell_key[c] & cmask) == ckey[k]) {
-            f = c;
+            f[k] = c;
             break;
           }
           h = (h + 1) & tmask;
           w = table[h];
         }
       }
-      if (f >= 0) {
+    }
+    // rounds 2 and 3 for four columns at a time (half the keys live at once)
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      // round 2: the keys of each column's first three cells
+      uint64_t kk[4][3];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const int k = 4 * g + j;
+          const uint64_t c = uint64_t(f[k]) + q;
+          kk[j][q] = (f[k] >= 0 && c < u_count) ? cell_key[c] : ~0ull;
+        }
+      // the cells [c, last] of each window
+      uint64_t c0[4], c1[4];
+      bool has[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = 4 * g + j;
+        has[j] = false;
+        c0[j] = c1[j] = 0;
+        if (f[k] < 0) continue;
         const uint64_t lo_key = ckey[k] | zlo, hi_key = ckey[k] | zhi;
-        uint64_t c = uint64_t(f);
-        if (cell_key[c] < lo_key) {
+        uint64_t c = uint64_t(f[k]);
+        uint64_t key0 = kk[j][0], key1 = kk[j][1], key2 = kk[j][2];
+        if (key0 < lo_key) {  // the column reaches below the window: gallop to it
           uint64_t step = 1;
           while (c + step < u_count && cell_key[c + step] < lo_key) {
             c += step;
@@ -401,14 +427,28 @@ __global__ void __launch_bounds__(256) k_ranges(Control *ctl, const uint64_t *ce
             else hi = mid;
           }
           c = hi;
+          key0 = c < u_count ? cell_key[c] : ~0ull;
+          key1 = c + 1 < u_count ? cell_key[c + 1] : ~0ull;
+          key2 = c + 2 < u_count ? cell_key[c + 2] : ~0ull;
         }
-        if (c < u_count && cell_key[c] <= hi_key) {
+        if (c < u_count && key0 <= hi_key) {
           uint64_t last = c;
-          while (last + 1 < u_count && cell_key[last + 1] <= hi_key) ++last;
-          rg = make_uint2(cell_start[c], cell_start[last + 1]);
+          if (c + 1 < u_count && key1 <= hi_key) {
+            last = c + 1;
+            if (c + 2 < u_count && key2 <= hi_key) last = c + 2;
+          }
+          has[j] = true;
+          c0[j] = c;
+          c1[j] = last + 1;
         }
       }
-      out[col] = rg;
+      // round 3: the cell starts that bound each range
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = 4 * g + j;
+        const int col = k < 4 ? k : k + 1;
+        out[col] = has[j] ? make_uint2(cell_start[c0[j]], cell_start[c1[j]]) : make_uint2(0, 0);
+      }
     }
   }
 }
