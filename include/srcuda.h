@@ -236,8 +236,9 @@ srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float
 
 /* ---- sort launch shapes and their tuning ------------------------------------ */
 
-/* The onesweep radix sort is built in several launch shapes -- keys per thread
- * and the blocks per SM its registers are capped for; 8-bit digits throughout.
+/* The onesweep radix sort is built in several launch shapes -- keys per thread,
+ * the blocks per SM its registers are capped for, and threads per block (256 or
+ * 512); 8-bit digits throughout.
  * A context picks one per sort from a table of input sizes, one table per sort
  * kind (the voxel-key sort over the input points, the cell-key sort of the
  * radius grid).  The built-in tables were measured by spatialrust_b200.autotune
@@ -266,11 +267,15 @@ srcu_status srcu_set_sort_tuning(srcu_ctx *ctx, int32_t kind, const uint64_t *ma
 srcu_status srcu_get_sort_tuning(srcu_ctx *ctx, int32_t kind, uint64_t *max_points,
                                  int32_t *config, uint32_t *count);
 
-/* The normals kernel's neighbour gather: 1 stages each warp's candidate records
- * (the x-strips of its 3x3 column block) in shared memory by non-multicast
- * cp.async.bulk copies before the walk; 0 reads them through L1.  Both give
- * identical results.  -1 restores the built-in choice (measured by the
- * autotuner).  Plane covariances always read through L1. */
+/* The normals kernel's neighbour walk.  0: range by range through L1.  1: range
+ * by range, each warp's candidate records (the x-strips of its 3x3 column
+ * block) first staged in shared memory by non-multicast cp.async.bulk copies.
+ * 2: each lane's non-empty, reachable column ranges walked as one list (the
+ * warp runs to its longest list, not to its longest range nine times), with
+ * packed f32x2 arithmetic; columns that no point within the radius can lie in
+ * are skipped.  The neighbour sets and counts are the same in every walk; the
+ * normals agree to f32 rounding.  -1 restores the built-in choice (measured by
+ * the autotuner).  Plane covariances take walk 2 when it is chosen, else 0. */
 srcu_status srcu_set_neighbor_staging(srcu_ctx *ctx, int32_t mode);
 int32_t srcu_get_neighbor_staging(srcu_ctx *ctx);
 
