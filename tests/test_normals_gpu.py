@@ -21,7 +21,7 @@ angle_errors = normal_parity.angle_errors
 
 
 def check_normals(ctx, x, y, z, radius, min_neighbors=3, viewpoint=None, report=None,
-                  include_self=False, ill_max=1e-3):
+                  include_self=False, ill_max=normal_parity.ILL_MAX):
     nx, ny, nz, curv, counts, stats = ctx.radius_normals(x, y, z, radius, min_neighbors, viewpoint,
                                                          include_self)
     ref = oracle.radius_normals_fp64(x, y, z, radius, min_neighbors, viewpoint,

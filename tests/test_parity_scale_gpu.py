@@ -25,6 +25,11 @@ from spatialrust_b200 import _native, synthetic
 
 pytestmark = pytest.mark.gpu
 VIEWPOINT = (0.0, 0.0, 100.0)
+# Ill-conditioned points (relative eigengap < 1e-3) of each input, from the FP64
+# oracle's eigengaps on these seeded clouds: (count, solved points).
+ILL_C1 = {0.1: (4, 1_629_258), 0.5: (4, 57_353)}
+ILL_C3 = {74: (0, 0), 180: (6, 483), 156: (4415, 516_850), 186: (0, 4), 26: (185, 8228),
+          84: (151, 733_647), 225: (2, 217), 229: (292, 111_174), 21: (9, 616_665)}
 
 
 def check_voxels(cols, counts, vox, leaf, keys=None, label=""):
@@ -50,6 +55,7 @@ def test_georeferenced_2m_chain_full_size(leaf):
                                            out["neighbor_counts"], ref, gx, gy, gz, VIEWPOINT,
                                            out["stats"], label=f"C1 leaf {leaf}")
     assert rep["points"] == (1_820_918 if leaf == 0.1 else 417_439)
+    assert (rep["ill_conditioned"], rep["solved"]) == ILL_C1[leaf]
     print(f"C1 leaf {leaf}:", rep)
 
 
@@ -62,6 +68,7 @@ def test_shapes_5m_full_size():
     rep = normal_parity.check_against_fp64(nx, ny, nz, curv, counts, ref, c.x, c.y, c.z, None,
                                            stats, label="C2")
     assert counts.max() > 900  # the uncapped cylinder neighbourhoods are in the check
+    assert rep["ill_conditioned"] == 0 and rep["solved"] == 5_000_000
     print("C2 shapes 5M:", rep)
 
 
@@ -100,4 +107,5 @@ def test_batched_256_clouds_sliced():
                                                out["curvature"][a:e],
                                                out["neighbor_counts"][a:e], ref, gx, gy, gz,
                                                VIEWPOINT, label=label)
+        assert (rep["ill_conditioned"], rep["solved"]) == ILL_C3[b], label
         print(label, rep)
