@@ -270,12 +270,10 @@ srcu_status srcu_get_sort_tuning(srcu_ctx *ctx, int32_t kind, uint64_t *max_poin
 /* The normals kernel's neighbour walk.  0: range by range through L1.  1: range
  * by range, each warp's candidate records (the x-strips of its 3x3 column
  * block) first staged in shared memory by non-multicast cp.async.bulk copies.
- * 2: each lane's non-empty, reachable column ranges walked as one list (the
- * warp runs to its longest list, not to its longest range nine times), with
- * packed f32x2 arithmetic; columns that no point within the radius can lie in
- * are skipped.  The neighbour sets and counts are the same in every walk; the
- * normals agree to f32 rounding.  -1 restores the built-in choice (measured by
- * the autotuner).  Plane covariances take walk 2 when it is chosen, else 0. */
+ * 2: walk 0 with the predicate and the moments in packed f32x2 arithmetic.
+ * Every walk gives the same neighbour sets and counts, and walks 0 and 2 give
+ * bit-identical outputs.  -1 restores the built-in choice (measured by the
+ * autotuner).  Plane covariances take walk 2 when it is chosen, else 0. */
 srcu_status srcu_set_neighbor_staging(srcu_ctx *ctx, int32_t mode);
 int32_t srcu_get_neighbor_staging(srcu_ctx *ctx);
 

@@ -42,7 +42,7 @@ SAMPLE_POINTS = tuple(int(round(2 ** (16 + k / 2))) for k in range(19))
 LEAF = 0.1
 RADIUS = 0.5
 HYSTERESIS = 0.02  # keep the smaller size's shape unless another is this much faster
-WALK_MODES = (0, 1, 2)  # srcu_set_neighbor_staging: L1, staged, flat
+WALK_MODES = (0, 1, 2)  # srcu_set_neighbor_staging: L1, staged, packed
 TABLE_MAX = 32     # SRCU_SORT_TUNING_MAX
 BIG = (1 << 64) - 1
 L2_FLUSH_BYTES = 256 << 20  # written before every timed chain: inputs start outside L2
@@ -181,7 +181,7 @@ def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> s
         "// k*SortTuneConfig[k] indexes kSortItems / kSortMinBlocks in radix.cuh.",
         "// kNeighborStaging: the normals kernel's neighbour walk -- range by range",
         "// through L1 (0), range by range from shared memory filled by bulk copies (1),",
-        "// or each lane's ranges as one list with packed f32x2 arithmetic (2).",
+        "// or the L1 walk in packed f32x2 arithmetic (2).",
     ]
     if result is not None:
         lines.append("//")
@@ -195,7 +195,7 @@ def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> s
             for keys, ms in samples(result, kind):
                 lines.append(f"//   {'':14} {keys:>9}  " + "  ".join(f"{m:6.4f}" for m in ms))
         if result.get("staging"):
-            lines.append("// Normals kernel ms per chain, neighbour walk L1 / staged / flat:")
+            lines.append("// Normals kernel ms per chain, neighbour walk L1 / staged / packed:")
             by_n = {}
             for r in result["staging"]:
                 by_n.setdefault(r["points"], {})[r["staging"]] = r["normals_ms"]

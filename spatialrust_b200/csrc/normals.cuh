@@ -486,7 +486,7 @@ __device__ const uint2 nm_no_ranges[9] = {};  // the walk of a lane whose cell i
 // The neighbour walks of k_normals.
 constexpr int WALK_L1 = 0;      // range by range through L1, two candidates per step
 constexpr int WALK_STAGED = 1;  // range by range from shared memory filled by bulk copies
-constexpr int WALK_FLAT = 2;    // each lane's ranges as one list, packed f32x2 arithmetic
+constexpr int WALK_PACKED = 2;  // range by range through L1, packed f32x2 arithmetic
 
 // Packed f32x2 arithmetic (sm_100): two IEEE round-to-nearest f32 operations
 // per instruction, component by component -- the same results as
@@ -518,22 +518,6 @@ __device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
   uint64_t r;
   asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
   return r;
-}
-
-// Neighbour column k (dx = k / 3 - 1, dy = k % 3 - 1) of the query's cell is out
-// of reach when every point in it is farther than r from the query along x and
-// y alone.  lo[a] / hi[a]: the query's distance to its cell's lower / upper
-// face on axis a, in FP64 (a point of the column below lies below the face,
-// up to FP64 rounding of the cell arithmetic).  The margin of 1e-5 r^2 is far
-// above that rounding and above the f32 predicate's own (3 roundings of
-// 2^-24), and above the shell band (1e-6 r^2), so a pruned column holds no
-// neighbour and no shell point.
-__device__ __forceinline__ bool column_out_of_reach(int k, const double (&lo)[2],
-                                                    const double (&hi)[2], double r2_margin) {
-  const int dx = k / 3 - 1, dy = k % 3 - 1;
-  const double bx = dx < 0 ? lo[0] : (dx > 0 ? hi[0] : 0.0);
-  const double by = dy < 0 ? lo[1] : (dy > 0 ? hi[1] : 0.0);
-  return bx * bx + by * by > r2_margin;
 }
 
 // Covariance from moments about the query (S: sx sy sz sxx syy szz sxy sxz syz
@@ -627,12 +611,8 @@ __device__ __noinline__ void moments_fp64(const float4 *pts, const uint2 *rg, fl
 // NM_STAGE records is read from global memory as in the plain walk.  The plain
 // walk reads through L1 instead; which one a context runs is a tuning choice
 // (srcu_set_neighbor_staging).
-constexpr int NM_MIN_BLOCKS = 4;       // 64 registers: the range-by-range walks
-constexpr int NM_FLAT_MIN_BLOCKS = 3;  // 85 registers: the flat walk without spills
-
 template <bool CountShell, bool PlaneCov = false, int Walk = WALK_L1>
-__global__ void __launch_bounds__(NM_THREADS, Walk == WALK_FLAT ? NM_FLAT_MIN_BLOCKS
-                                                                : NM_MIN_BLOCKS) k_normals(Control *ctl, const float4 *pts,
+__global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const float4 *pts,
                                                            const uint32_t *pt_cell,
                                                            const uint2 *ranges,
                                                            const uint64_t *cell_key, Batch bt,
@@ -671,7 +651,7 @@ __global__ void __launch_bounds__(NM_THREADS, Walk == WALK_FLAT ? NM_FLAT_MIN_BL
     bool bad = false;
     if (u >= u_count) {  // cannot happen for a consistent cell table
       atomicOr(&ctl->status, ST_INTERNAL);
-      if constexpr (Staged || Walk == WALK_FLAT) {
+      if constexpr (Staged) {
         bad = true;  // the lane stays for the warp's collectives and walks nothing
       } else {
         continue;
@@ -807,92 +787,36 @@ __global__ void __launch_bounds__(NM_THREADS, Walk == WALK_FLAT ? NM_FLAT_MIN_BL
           walk([&](uint32_t j) { return __ldg(pts + j); }, range.x, range.y);
         }
       }
-    } else if constexpr (Walk == WALK_FLAT) {
-      // The lane's non-empty, reachable column ranges, in column order, as
-      // one list in this warp's shared memory; the walk then runs to the
-      // longest list of the warp instead of to the longest range nine times.
-      __shared__ uint2 nm_lists[NM_THREADS / 32][9][32];
-      uint2(*lst)[32] = nm_lists[threadIdx.x >> 5];
-      double lo[2] = {0.0, 0.0}, hi[2] = {0.0, 0.0};
-      const bool prune = !bad && isfinite(qp.x) && isfinite(qp.y) && isfinite(qp.z);
-      if (prune) {
-        const CellPlan &pl = bt.cplans[cb];
-        const float qa[2] = {qp.x, qp.y};
-#pragma unroll
-        for (int a = 0; a < 2; ++a) {
-          const double off = double(qa[a]) - pl.origin[a];
-          const double face = double(cell_axis(qa[a], pl.origin[a], pl.inv_h, pl.dims[a])) * pl.h;
-          lo[a] = off - face;
-          hi[a] = face + pl.h - off;
-        }
-      }
-      const double r2_margin = double(r2) * (1.0 + 1e-5);
-      uint2 g[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) g[k] = rg[k];  // nine independent loads
-      uint32_t nr = 0, total = 0;
-#pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        const bool keep = g[k].y > g[k].x && !(prune && column_out_of_reach(k, lo, hi, r2_margin));
-        if (keep) {
-          lst[nr][lane] = g[k];
-          ++nr;
-          total += g[k].y - g[k].x;
-        }
-      }
-      __syncwarp();
-      const uint32_t steps = __reduce_max_sync(FULL_MASK, total);
+    } else if constexpr (Walk == WALK_PACKED) {
+      // The L1 walk's candidate order and flush points, with the predicate and
+      // the moments in packed f32x2 arithmetic: the same IEEE operation on each
+      // half, so every result is bit-identical to WALK_L1's.
       const uint64_t qxy = f2_pack(qp.x, qp.y);
-      uint64_t a01 = 0, a34 = 0, a78 = 0;  // (sx, sy), (sxx, syy), (sxz, syz) as f32 pairs
+      uint64_t a01 = 0, a34 = 0, a78 = 0;  // (sx, sy), (sxx, syy), (sxz, syz)
       float a2 = 0.f, a5 = 0.f, a6 = 0.f;  // sz, szz, sxy
-      uint32_t li = 0, cur = 0, end = 0;
-      float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (total) {
-        const uint2 g0 = lst[0][lane];
-        cur = g0.x;
-        end = g0.y;
-        c = __ldg(pts + cur);
-      }
-      // Steps in chunks of NM_FLUSH (warp-uniform), each chunk's f32 partials
-      // then folded into FP64; within a chunk two steps per iteration, so the
-      // candidate prefetched for the next step needs no register moves.
-#pragma unroll 1
-      for (uint32_t t0 = 0; t0 < steps; t0 += NM_FLUSH) {
-        const uint32_t t1 = min(steps, t0 + NM_FLUSH);
-#pragma unroll 2
-        for (uint32_t t = t0; t < t1; ++t) {
-          if (t < total) {
-            uint32_t nxt = cur + 1;
-            if (nxt == end && li + 1 < nr) {  // on to the next range of the list
-              const uint2 gn = lst[++li][lane];
-              nxt = gn.x;
-              end = gn.y;
-            }
-            const float4 cn = t + 1 < total ? __ldg(pts + nxt) : c;  // one candidate ahead
-            // the reference predicate ((dx^2 + dy^2) + dz^2 <= r^2, kdtree.rs:544-549)
-            const uint64_t dxy = f2_sub(f2_pack(c.x, c.y), qxy);
-            const uint64_t pxy = f2_mul(dxy, dxy);
-            float dx, dy, xx, yy;
-            f2_unpack(dxy, dx, dy);
-            f2_unpack(pxy, xx, yy);
-            const float dz = __fsub_rn(c.z, qp.z);
-            const float zz = __fmul_rn(dz, dz);
-            const float d2 = __fadd_rn(__fadd_rn(xx, yy), zz);
-            if (d2 <= r2) {
-              hits += 1.f;
-              a01 = f2_add(a01, dxy);
-              a34 = f2_add(a34, pxy);
-              a78 = f2_fma(dxy, f2_pack(dz, dz), a78);
-              a2 += dz;
-              a5 += zz;
-              a6 = fmaf(dx, dy, a6);
-            }
-            if (CountShell && prm.count_shell && d2 != 0.f && fabsf(__fsub_rn(d2, r2)) <= shell_tol)
-              shell = 1;
-            c = cn;
-            cur = nxt;
-          }
+      auto pvisit = [&](const float4 c) {
+        // the reference predicate ((dx^2 + dy^2) + dz^2 <= r^2, kdtree.rs:544-549)
+        const uint64_t dxy = f2_sub(f2_pack(c.x, c.y), qxy);
+        const uint64_t pxy = f2_mul(dxy, dxy);
+        float dx, dy, xx, yy;
+        f2_unpack(dxy, dx, dy);
+        f2_unpack(pxy, xx, yy);
+        const float dz = __fsub_rn(c.z, qp.z);
+        const float zz = __fmul_rn(dz, dz);
+        const float d2 = __fadd_rn(__fadd_rn(xx, yy), zz);
+        if (d2 <= r2) {
+          hits += 1.f;
+          a01 = f2_add(a01, dxy);
+          a34 = f2_add(a34, pxy);
+          a78 = f2_fma(dxy, f2_pack(dz, dz), a78);
+          a2 += dz;
+          a5 += zz;
+          a6 = fmaf(dx, dy, a6);
         }
+        if (CountShell && prm.count_shell && d2 != 0.f && fabsf(__fsub_rn(d2, r2)) <= shell_tol)
+          shell = 1;
+      };
+      auto pflush = [&]() {
         float v0, v1, v3, v4, v7, v8;
         f2_unpack(a01, v0, v1);
         f2_unpack(a34, v3, v4);
@@ -908,8 +832,33 @@ __global__ void __launch_bounds__(NM_THREADS, Walk == WALK_FLAT ? NM_FLAT_MIN_BL
         S[8] += double(v8);
         a01 = a34 = a78 = 0;
         a2 = a5 = a6 = 0.f;
+      };
+      uint2 next = rg[0];
+#pragma unroll 1
+      for (int r = 0; r < 9; ++r) {
+        const uint2 range = next;
+        if (r < 8) next = rg[r + 1];  // the next column's range loads under this one
+        uint32_t j = range.x;
+        for (; j + 2 <= range.y; j += 2) {  // two independent candidate loads per step
+          const float4 c0 = __ldg(pts + j);
+          const float4 c1 = __ldg(pts + j + 1);
+          pvisit(c0);
+          pvisit(c1);
+          since += 2;
+          if (since >= NM_FLUSH) {
+            since = 0;
+            pflush();
+          }
+        }
+        if (j < range.y) {
+          pvisit(__ldg(pts + j));
+          if (++since >= NM_FLUSH) {
+            since = 0;
+            pflush();
+          }
+        }
       }
-      __syncwarp();  // the lists are rewritten by the next batch
+      pflush();
     } else {
       uint2 next = rg[0];
 #pragma unroll 1

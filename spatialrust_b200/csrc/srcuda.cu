@@ -49,8 +49,8 @@ struct srcu_ctx {
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_voxel = nullptr;
   unsigned char *head_host = nullptr;
-  int occ_normals = 1, occ_normals_staged = 1, occ_normals_flat = 1, occ_seg = 1, occ_cells = 1;
-  int neighbor_staging = 0;  // k_normals' neighbour walk: WALK_L1, WALK_STAGED or WALK_FLAT
+  int occ_normals = 1, occ_normals_staged = 1, occ_normals_packed = 1, occ_seg = 1, occ_cells = 1;
+  int neighbor_staging = 0;  // k_normals' neighbour walk: WALK_L1, WALK_STAGED or WALK_PACKED
   // co-resident blocks per SM of each sort launch shape, voxel-key and cell-key sorts
   int occ_sort_v[SORT_CONFIGS] = {}, occ_sort_c[SORT_CONFIGS] = {};
   // sort launch shape by input size, per sort kind (SRCU_SORT_VOXEL_KEYS /
@@ -732,12 +732,12 @@ srcu_status enqueue_normals(srcu_ctx *ctx, const float *x, const float *y, const
   auto kernel = walk == WALK_STAGED
                     ? (ctx->count_shell ? k_normals<true, false, WALK_STAGED>
                                         : k_normals<false, false, WALK_STAGED>)
-                : walk == WALK_FLAT
-                    ? (ctx->count_shell ? k_normals<true, false, WALK_FLAT>
-                                        : k_normals<false, false, WALK_FLAT>)
+                : walk == WALK_PACKED
+                    ? (ctx->count_shell ? k_normals<true, false, WALK_PACKED>
+                                        : k_normals<false, false, WALK_PACKED>)
                     : (ctx->count_shell ? k_normals<true> : k_normals<false>);
   const uint32_t grid = walk == WALK_STAGED ? uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals_staged)
-                        : walk == WALK_FLAT ? uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals_flat)
+                        : walk == WALK_PACKED ? uint32_t(ctx->num_sms) * uint32_t(ctx->occ_normals_packed)
                                             : grid_n;
   kernel<<<grid, NM_THREADS, 0, ctx->stream>>>(
       ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint2>(ctx->ranges),
@@ -947,8 +947,8 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals, k_normals<true>, NM_THREADS, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals_staged,
                                                 k_normals<true, false, WALK_STAGED>, NM_THREADS, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals_flat,
-                                                k_normals<true, false, WALK_FLAT>, NM_THREADS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals_packed,
+                                                k_normals<true, false, WALK_PACKED>, NM_THREADS, 0);
   ctx->neighbor_staging = kNeighborStaging;
   if (configure_segment_kernels() != cudaSuccess) return bail(SRCU_ERR_CUDA);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_seg, k_voxel_segments<4>, SEG_THREADS,
@@ -956,7 +956,7 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_cells, k_cells, CELL_THREADS, 0);
   ctx->occ_normals = std::max(1, ctx->occ_normals);
   ctx->occ_normals_staged = std::max(1, ctx->occ_normals_staged);
-  ctx->occ_normals_flat = std::max(1, ctx->occ_normals_flat);
+  ctx->occ_normals_packed = std::max(1, ctx->occ_normals_packed);
   ctx->occ_seg = std::max(1, ctx->occ_seg);
   ctx->occ_cells = std::max(1, ctx->occ_cells);
   if (cudaGetLastError() != cudaSuccess) return bail(SRCU_ERR_CUDA);
@@ -1065,7 +1065,7 @@ srcu_status srcu_get_sort_tuning(srcu_ctx *ctx, int32_t kind, uint64_t *max_poin
 
 srcu_status srcu_set_neighbor_staging(srcu_ctx *ctx, int32_t mode) {
   if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
-  if (mode < -1 || mode > WALK_FLAT)
+  if (mode < -1 || mode > WALK_PACKED)
     return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "the neighbour walk is -1 (built-in), 0, 1 or 2");
   ctx->neighbor_staging = mode < 0 ? kNeighborStaging : mode;
   return SRCU_OK;
@@ -1252,11 +1252,11 @@ srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float
   ST_TRY(enqueue_grid(ctx, cols[0], cols[1], cols[2], ptr<const float4>(ctx->in_aos), nullptr, n,
                       bt, nullptr));
   {
-    const bool flat = ctx->neighbor_staging == WALK_FLAT;
+    const bool flat = ctx->neighbor_staging == WALK_PACKED;
     const uint32_t grid_n =
-        uint32_t(ctx->num_sms) * uint32_t(flat ? ctx->occ_normals_flat : ctx->occ_normals);
+        uint32_t(ctx->num_sms) * uint32_t(flat ? ctx->occ_normals_packed : ctx->occ_normals);
     Launch l(ctx, SRCU_K_NORMALS);
-    (flat ? k_normals<false, true, WALK_FLAT> : k_normals<false, true>)<<<grid_n, NM_THREADS, 0, ctx->stream>>>(
+    (flat ? k_normals<false, true, WALK_PACKED> : k_normals<false, true>)<<<grid_n, NM_THREADS, 0, ctx->stream>>>(
         ctx->ctl, ptr<float4>(ctx->pts), ptr<uint32_t>(ctx->pt_cell), ptr<uint2>(ctx->ranges),
         ptr<uint64_t>(ctx->cell_key), bt, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
         dst, epsilon);

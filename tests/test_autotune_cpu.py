@@ -96,7 +96,7 @@ def test_choose_walk_among_three():
     def res(rows):
         return dict(staging=[dict(points=n, voxels=n, staging=m, normals_ms=ms)
                              for n, per in enumerate(rows) for m, ms in enumerate(per)])
-    # the flat walk wins on the geometric mean even where staging wins one size
+    # the packed walk wins on the geometric mean even where staging wins one size
     assert autotune.choose_staging(res([(1.0, 1.1, 0.7), (2.0, 1.8, 1.5), (4.0, 4.2, 3.0)])) == 2
     assert autotune.choose_staging(res([(1.0, 1.1, 1.2), (2.0, 2.1, 2.3)])) == 0
     assert "kNeighborStaging = 2;" in autotune.header_text({"voxel": [(BIG, 0)], "cell": [(BIG, 0)]},

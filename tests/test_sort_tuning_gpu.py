@@ -163,38 +163,38 @@ def test_staging_switch_arguments(cuda_ctx):
     assert cuda_ctx.neighbor_staging() == builtin
 
 
-# ---- the flat neighbour walk (each lane's ranges as one list, f32x2) ----------
+# ---- the packed neighbour walk (the L1 walk in f32x2 arithmetic) -------------
 
-FLAT = 2
+PACKED = 2
 
 
 @pytest.mark.parametrize("case", ["georef_centroids", "dense", "shapes", "include_self"])
-def test_flat_walk_against_fp64_oracle(cuda_ctx, case):
-    # Same neighbour sets as the other walks (exact counts, shell counts), and
-    # normals within the bar of the FP64 oracle; columns out of reach are
-    # skipped without losing a neighbour or a shell point.
+def test_packed_walk_is_bit_identical_and_meets_the_oracle(cuda_ctx, case):
+    # the same IEEE operations on each half of every packed instruction, in the
+    # L1 walk's order: every output bit-identical to walk 0, and the FP64
+    # oracle's bar met
     inc = case == "include_self"
     if case in ("georef_centroids", "include_self"):
         c = synthetic.georef_scan(400_000, seed=11)
         v = oracle.voxel_centroid(c.x, c.y, c.z, leaf=0.1)
         x, y, z, r, vp = v.x, v.y, v.z, 0.5, (0, 0, 100)
-    elif case == "dense":  # ~2,000 neighbours per point, 3-D: every column in reach
+    elif case == "dense":  # ~2,000 neighbours per point, 3-D
         p = np.random.default_rng(12).uniform(0, 2, (30_000, 3)).astype(np.float32)
         x, y, z, r, vp = p[:, 0], p[:, 1], p[:, 2], 0.5, None
     else:
         c = synthetic.shapes_scene(300_000, seed=13)
         x, y, z, r, vp = c.x, c.y, c.z, 0.3, (50, 50, 150)
     a = normals_with(cuda_ctx, x, y, z, 0, radius=r, viewpoint=vp, include_self=inc)
-    b = normals_with(cuda_ctx, x, y, z, FLAT, radius=r, viewpoint=vp, include_self=inc)
-    assert np.array_equal(a[4], b[4])  # neighbour counts
-    assert a[5] == b[5] or all(a[5][k] == b[5][k] for k in ("valid_count", "invalid_count",
-                                                             "shell_points"))
+    b = normals_with(cuda_ctx, x, y, z, PACKED, radius=r, viewpoint=vp, include_self=inc)
+    for u, w in zip(a[:5], b[:5]):
+        assert np.array_equal(np.asarray(u).view(np.uint32), np.asarray(w).view(np.uint32))
+    assert a[5] == b[5]
     ref = oracle.radius_normals_fp64(x, y, z, r, 3, vp, include_self=inc)
     normal_parity.check_against_fp64(*b[:5], ref, x, y, z, vp, b[5], include_self=inc,
-                                     ill_max=5e-3, label=f"flat {case}")
+                                     label=f"packed {case}")
 
 
-def test_flat_walk_batch_equals_alone(cuda_ctx):
+def test_packed_walk_batch_equals_alone(cuda_ctx):
     import torch
     rng = np.random.default_rng(78)
     clouds = [synthetic.georef_scan(int(n), seed=200 + i, offset=rng.uniform(0, 1e6, 3))
@@ -207,7 +207,7 @@ def test_flat_walk_batch_equals_alone(cuda_ctx):
     keep = _native._Keep()
     pts = _native.make_cloud(dev[0], dev[1], dev[2], [dev[3]], keep)
     ctx = _native.Context(0)
-    ctx.set_neighbor_staging(FLAT)
+    ctx.set_neighbor_staging(PACKED)
     ctx.batch_voxel_normals_enqueue(pts, offsets, leaves, radii, 3, [(0.0, 0.0, 100.0)] * 4)
     voff = ctx.batch_voxel_offsets()
     out = ctx.frame_fetch(int(offsets[-1]), n_attrs=1)
@@ -220,10 +220,10 @@ def test_flat_walk_batch_equals_alone(cuda_ctx):
     ctx.close()
 
 
-def test_flat_walk_plane_covariances(cuda_ctx):
+def test_packed_walk_plane_covariances(cuda_ctx):
     c = synthetic.georef_scan(300_000, seed=16)
     a = cuda_ctx.plane_covariances(c.x, c.y, c.z, 0.3, 1e-3)
-    cuda_ctx.set_neighbor_staging(FLAT)
+    cuda_ctx.set_neighbor_staging(PACKED)
     try:
         b = cuda_ctx.plane_covariances(c.x, c.y, c.z, 0.3, 1e-3)
     finally:
