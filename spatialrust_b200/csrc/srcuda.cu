@@ -11,6 +11,7 @@
 
 #include "../../include/srcuda.h"
 #include "cluster.cuh"
+#include "host_copy.h"
 #include "normals.cuh"
 #include "sort_tuning.h"
 #include "voxel.cuh"
@@ -43,6 +44,10 @@ struct srcu_ctx {
   bool capturing = false;
   // the counts behind the last SRCU_ERR_LENGTH_MISMATCH (srcu_last_length_mismatch)
   uint64_t mismatch_expected = 0, mismatch_found = 0;
+  // pinned staging ring for copies from and to pageable host memory (host_copy.h)
+  unsigned char *ring[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ring_ev[3] = {nullptr, nullptr, nullptr};
+  int ring_next = 0;
   // Side stream for read-backs that overlap later kernels of the same chain,
   // the event that releases them, and a pinned copy of the control-block head
   // (epoch, status, point and voxel counts) read once the voxel stage is done.
@@ -161,6 +166,81 @@ srcu_status ensure(srcu_ctx *ctx, DevBuf &b, size_t bytes, bool zero = false) {
   b.p = p;
   b.bytes = want;
   ctx->used += want;
+  return SRCU_OK;
+}
+
+// ---- host <-> device copies of pageable host memory ---------------------------
+// Chunks of kRingChunk bytes through the context's ring of pinned buffers: the
+// host-side copy of a chunk (split over HostCopyPool's threads) overlaps the
+// DMA of the previous chunk.  Pinned memory and small copies go straight to
+// cudaMemcpyAsync.
+constexpr size_t kRingChunk = size_t(4) << 20;
+constexpr int kRingSlots = 3;
+constexpr size_t kRingMin = size_t(1) << 20;
+
+srcu_status ring_ready(srcu_ctx *ctx) {
+  if (ctx->ring[0]) return SRCU_OK;
+  for (int k = 0; k < kRingSlots; ++k) {
+    CU_TRY(cudaMallocHost(reinterpret_cast<void **>(&ctx->ring[k]), kRingChunk));
+    CU_TRY(cudaEventCreateWithFlags(&ctx->ring_ev[k], cudaEventDisableTiming));
+  }
+  return SRCU_OK;
+}
+
+// Host -> device, ordered on `stream`; returns once the source has been read.
+srcu_status host_to_device(srcu_ctx *ctx, void *dst, const void *src, size_t bytes,
+                           cudaStream_t stream) {
+  if (bytes < kRingMin || !is_pageable(src)) {
+    CU_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+    return SRCU_OK;
+  }
+  ST_TRY(ring_ready(ctx));
+  for (size_t off = 0; off < bytes; off += kRingChunk) {
+    const size_t len = std::min(kRingChunk, bytes - off);
+    const int slot = ctx->ring_next;
+    ctx->ring_next = (slot + 1) % kRingSlots;
+    CU_TRY(cudaEventSynchronize(ctx->ring_ev[slot]));  // the slot's last DMA is done
+    HostCopyPool::get().copy(ctx->ring[slot], static_cast<const char *>(src) + off, len);
+    CU_TRY(cudaMemcpyAsync(static_cast<char *>(dst) + off, ctx->ring[slot], len,
+                           cudaMemcpyHostToDevice, stream));
+    CU_TRY(cudaEventRecord(ctx->ring_ev[slot], stream));
+  }
+  return SRCU_OK;
+}
+
+// Device -> host, ordered on `stream`.  Pageable destinations are complete on
+// return (as a driver-staged copy would be); pinned ones when the stream is.
+srcu_status device_to_host(srcu_ctx *ctx, void *dst, const void *src, size_t bytes,
+                           cudaStream_t stream) {
+  if (bytes < kRingMin || !is_pageable(dst)) {
+    CU_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream));
+    return SRCU_OK;
+  }
+  ST_TRY(ring_ready(ctx));
+  int pend = -1;
+  size_t pend_off = 0, pend_len = 0;
+  for (size_t off = 0;; off += kRingChunk) {
+    const bool more = off < bytes;
+    int slot = -1;
+    size_t len = 0;
+    if (more) {
+      len = std::min(kRingChunk, bytes - off);
+      slot = ctx->ring_next;
+      ctx->ring_next = (slot + 1) % kRingSlots;
+      CU_TRY(cudaEventSynchronize(ctx->ring_ev[slot]));
+      CU_TRY(cudaMemcpyAsync(ctx->ring[slot], static_cast<const char *>(src) + off, len,
+                             cudaMemcpyDeviceToHost, stream));
+      CU_TRY(cudaEventRecord(ctx->ring_ev[slot], stream));
+    }
+    if (pend >= 0) {  // the previous chunk, while this one's DMA runs
+      CU_TRY(cudaEventSynchronize(ctx->ring_ev[pend]));
+      HostCopyPool::get().copy(static_cast<char *>(dst) + pend_off, ctx->ring[pend], pend_len);
+    }
+    if (!more) break;
+    pend = slot;
+    pend_off = off;
+    pend_len = len;
+  }
   return SRCU_OK;
 }
 
@@ -314,8 +394,8 @@ srcu_status stage_input(srcu_ctx *ctx, const srcu_cloud *cloud, const float **co
       }
       const size_t floats = size_t(cloud->n - 1) * cloud->stride + (top - base) / 4 + 1;
       ST_TRY(ensure(ctx, ctx->stage_block, floats * 4));
-      CU_TRY(cudaMemcpyAsync(ctx->stage_block.p, reinterpret_cast<const void *>(base), floats * 4,
-                             cudaMemcpyHostToDevice, ctx->stream));
+      ST_TRY(host_to_device(ctx, ctx->stage_block.p, reinterpret_cast<const void *>(base),
+                            floats * 4, ctx->stream));
       for (uint32_t c = 0; c < nc; ++c)
         iv.src[c] = ptr<const float>(ctx->stage_block) +
                     (reinterpret_cast<uintptr_t>(src[c]) - base) / 4;
@@ -336,9 +416,7 @@ srcu_status stage_input(srcu_ctx *ctx, const srcu_cloud *cloud, const float **co
     if (cloud->on_device) {
       cols[c] = src[c];
     } else {
-      if (cloud->n)
-        CU_TRY(cudaMemcpyAsync(ctx->in[c].p, src[c], cloud->n * 4, cudaMemcpyHostToDevice,
-                               ctx->stream));
+      if (cloud->n) ST_TRY(host_to_device(ctx, ctx->in[c].p, src[c], cloud->n * 4, ctx->stream));
       cols[c] = ptr<const float>(ctx->in[c]);
     }
   }
@@ -817,9 +895,8 @@ srcu_status read_control(srcu_ctx *ctx) {
 srcu_status copy_out(srcu_ctx *ctx, void *dst, const void *src, size_t bytes, int on_device,
                      cudaStream_t stream = nullptr) {
   if (!dst || bytes == 0) return SRCU_OK;
-  CU_TRY(cudaMemcpyAsync(dst, src, bytes,
-                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                         stream ? stream : ctx->stream));
+  if (!on_device) return device_to_host(ctx, dst, src, bytes, stream ? stream : ctx->stream);
+  CU_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream ? stream : ctx->stream));
   return SRCU_OK;
 }
 
@@ -988,6 +1065,10 @@ void srcu_destroy(srcu_ctx *ctx) {
     if (ctx->h_stage[slot]) cudaFreeHost(ctx->h_stage[slot]);
   }
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+  for (int k = 0; k < 3; ++k) {
+    if (ctx->ring_ev[k]) cudaEventSynchronize(ctx->ring_ev[k]), cudaEventDestroy(ctx->ring_ev[k]);
+    if (ctx->ring[k]) cudaFreeHost(ctx->ring[k]);
+  }
   if (ctx->ctl) cudaFree(ctx->ctl);
   if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
   if (ctx->head_host) cudaFreeHost(ctx->head_host);

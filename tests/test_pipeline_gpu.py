@@ -72,3 +72,51 @@ def test_stages_match_the_oracle_on_a_scan():
     roots = oracle.euclidean_roots(ox, oy, oz, 0.5, sparse=True)
     sizes = np.bincount(np.unique(roots, return_inverse=True)[1])
     assert res.clusters.cluster_count == int((sizes >= 3).sum())
+
+
+def _voxel_normals_into(ctx, cloud, vcols, ncols, counts, ncounts):
+    """srcu_voxel_normals into caller buffers (numpy or pinned torch tensors)."""
+    import ctypes
+    from spatialrust_b200 import _native
+    keep = _native._Keep()
+    addr = _native._addr
+    attr_out = keep.add((ctypes.c_void_p * 1)(addr(vcols[3])))
+    vout = _native.SrcuVoxelOut(addr(vcols[0]), addr(vcols[1]), addr(vcols[2]),
+                                ctypes.cast(attr_out, ctypes.c_void_p), 0, addr(counts), 0)
+    nout = _native.SrcuNormalOut(*[addr(c) for c in ncols], addr(ncounts), 0)
+    vp = _native._voxel_params(0.1, None)
+    np_ = _native._normal_params(0.5, 3, (0.0, 0.0, 100.0), False)
+    nv = ctypes.c_uint64(0)
+    stats = _native.SrcuNormalStats()
+    ctx._check(ctx._lib.srcu_voxel_normals(ctx.handle, ctypes.byref(cloud), ctypes.byref(vp),
+                                           ctypes.byref(np_), ctypes.byref(vout),
+                                           ctypes.byref(nout), ctypes.byref(nv), ctypes.byref(stats)))
+    return int(nv.value)
+
+
+def test_pageable_host_buffers_match_pinned(cuda_ctx):
+    # Pageable host columns (numpy) are staged through the context's pinned ring
+    # in 4 MB chunks (3.2M points: 12.8 MB per column, four chunks) in both
+    # directions; every output must be bit-identical to pinned host buffers'.
+    import torch
+    from spatialrust_b200 import _native
+    c = synthetic.georef_scan(3_200_000, seed=61)
+    n = c.n
+    out = {}
+    for kind in ("pageable", "pinned"):
+        keep = _native._Keep()
+        if kind == "pinned":
+            cols = [torch.from_numpy(a.copy()).pin_memory() for a in (c.x, c.y, c.z, c.intensity)]
+            mk = lambda dt: torch.empty(n, dtype=dt).pin_memory()
+        else:
+            cols = [a.copy() for a in (c.x, c.y, c.z, c.intensity)]
+            mk = lambda dt: np.empty(n, {torch.float32: np.float32, torch.int32: np.uint32}[dt])
+        cloud = _native.make_cloud(cols[0], cols[1], cols[2], [cols[3]], keep)
+        vcols = [mk(torch.float32) for _ in range(4)]
+        ncols = [mk(torch.float32) for _ in range(4)]
+        counts, ncounts = mk(torch.int32), mk(torch.int32)
+        v = _voxel_normals_into(cuda_ctx, cloud, vcols, ncols, counts, ncounts)
+        out[kind] = [np.asarray(a)[:v].view(np.uint32).copy() for a in vcols + ncols + [counts, ncounts]]
+    assert len(out["pageable"][0]) > 2_000_000
+    for a, b in zip(out["pageable"], out["pinned"]):
+        assert np.array_equal(a, b)
