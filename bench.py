@@ -87,6 +87,8 @@ def parse():
     ap.add_argument("--serving-rates", default="100,500,1000,2000",
                     help="offered request rates (req/s) of the serving measurement")
     ap.add_argument("--serving-seconds", type=float, default=2.0)
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end (host buffers) measurements (profiling runs)")
     ap.add_argument("--neighbor-walk", type=int, default=-1, choices=[-1, 0, 1, 2],
                     help="the normals kernel's neighbour walk (-1: the built-in choice)")
     return ap.parse_args()
@@ -315,9 +317,10 @@ def algorithmic_bytes(group: str, info: dict, n_attrs: int = 1) -> float:
 
 def summary(line: dict) -> dict:
     """The line's key figures, printed last (a reader of the line's tail sees them)."""
-    out = dict(value=round(line["value"], 1), e2e=round(line["e2e"]["value"], 1),
-               e2e_one_step_in_flight=round(line["e2e_one_step_in_flight"]["value"], 1),
-               e2e_pageable=round(line["e2e_pageable"]["value"], 1),
+    r1 = lambda v: None if v is None else round(v, 1)  # noqa: E731
+    out = dict(value=round(line["value"], 1), e2e=r1(line["e2e"]["value"]),
+               e2e_one_step_in_flight=r1(line["e2e_one_step_in_flight"]["value"]),
+               e2e_pageable=r1(line["e2e_pageable"]["value"]),
                roofline_frac=round(line["roofline"]["frac"], 4),
                roofline_voxel_frac=[round(x["frac"], 4) for x in line["roofline_voxel"]["leaves"]])
     b = line.get("batched")
@@ -477,9 +480,13 @@ def run_gpu(args):
 
     # end to end through the C ABI with pinned host buffers, then with plain
     # (pageable) numpy buffers as a Rust caller's Vecs are
-    e2e = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream)
-    e2e_one_step = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, inflight=1)
-    e2e_pageable = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=False)
+    if args.no_e2e:
+        skipped = dict(value=None, unit=UNIT, skipped="--no-e2e")
+        e2e = e2e_one_step = e2e_pageable = skipped
+    else:
+        e2e = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream)
+        e2e_one_step = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, inflight=1)
+        e2e_pageable = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=False)
 
     peaks = {}
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
