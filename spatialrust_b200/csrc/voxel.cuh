@@ -396,6 +396,11 @@ __global__ void __launch_bounds__(SEG_THREADS, 5) k_voxel_segments(Control *ctl,
     // any of them is consumed, so the gathers' latencies overlap.
     uint64_t ik[SEG_ITEMS];
     uint32_t iv[SEG_ITEMS];
+    uint64_t k_before = 0, k_after = 0;  // the keys either side of the tile (thread 0)
+    if (t == 0) {
+      k_before = base > 0 ? sv.key(base - 1) : ~sv.key(0);
+      k_after = base + tile_n < n ? sv.key(base + tile_n) : ~sv.key(n - 1);
+    }
 #pragma unroll
     for (int q = 0; q < SEG_ITEMS; ++q) {
       const uint32_t j = t + uint32_t(q) * SEG_THREADS;
@@ -434,8 +439,8 @@ __global__ void __launch_bounds__(SEG_THREADS, 5) k_voxel_segments(Control *ctl,
       }
     }
     if (t == 0) {
-      sm.keys[0] = base > 0 ? sv.key(base - 1) : ~sv.key(0);
-      sm.keys[1 + tile_n] = base + tile_n < n ? sv.key(base + tile_n) : ~sv.key(n - 1);
+      sm.keys[0] = k_before;
+      sm.keys[1 + tile_n] = k_after;
     }
     __syncthreads();
 
