@@ -237,17 +237,24 @@ srcu_status srcu_plane_covariances(srcu_ctx *ctx, const srcu_cloud *cloud, float
 /* ---- sort launch shapes and their tuning ------------------------------------ */
 
 /* The onesweep radix sort is built in several launch shapes -- keys per thread,
- * the blocks per SM its registers are capped for, and threads per block (256 or
- * 512); 8-bit digits throughout.
+ * the blocks per SM its registers are capped for, threads per block (256 or
+ * 512) and digit width: 8 bits, or 9 bits in the 512-thread shapes built for
+ * them, which take 9-bit digits only where that saves a pass over the key
+ * width at hand (and 8-bit digits otherwise).
  * A context picks one per sort from a table of input sizes, one table per sort
- * kind (the voxel-key sort over the input points, the cell-key sort of the
- * radius grid).  The built-in tables were measured by spatialrust_b200.autotune
- * on a B200; srcu_set_sort_tuning installs others (the autotuner does so while
- * it measures).  No counterpart in the reference (its wgpu bitonic sort has
- * fixed workgroups). */
+ * kind: the voxel-key sort over the input points and the cell-key sort of the
+ * radius grid, each for one cloud and for a batch of clouds (whose keys carry
+ * the cloud id above the per-cloud key, so they are wider).  The built-in
+ * tables were measured by spatialrust_b200.autotune on a B200;
+ * srcu_set_sort_tuning installs others (the autotuner does so while it
+ * measures).  No counterpart in the reference (its wgpu bitonic sort has fixed
+ * workgroups). */
 #define SRCU_SORT_TUNING_MAX 32
 #define SRCU_SORT_VOXEL_KEYS 0
 #define SRCU_SORT_CELL_KEYS 1
+#define SRCU_SORT_BATCH_VOXEL_KEYS 2
+#define SRCU_SORT_BATCH_CELL_KEYS 3
+#define SRCU_SORT_KINDS 4
 
 typedef struct srcu_sort_config {
   uint32_t items_per_thread;

@@ -24,6 +24,9 @@ pub const SRCU_ATTRIBUTE_FIRST: c_int = 1;
 pub const SRCU_SORT_TUNING_MAX: c_int = 32;
 pub const SRCU_SORT_VOXEL_KEYS: c_int = 0;
 pub const SRCU_SORT_CELL_KEYS: c_int = 1;
+pub const SRCU_SORT_BATCH_VOXEL_KEYS: c_int = 2;
+pub const SRCU_SORT_BATCH_CELL_KEYS: c_int = 3;
+pub const SRCU_SORT_KINDS: c_int = 4;
 pub const SRCU_NOALLOC_MAX_POINTS: c_int = 131072;
 
 // ---- srcu_status and srcu_kernel_id values ----

@@ -307,7 +307,9 @@ SIGNATURES = {
 _lib = None
 
 SORT_TUNING_MAX = 32
-SORT_KINDS = {"voxel": 0, "cell": 1}  # SRCU_SORT_VOXEL_KEYS, SRCU_SORT_CELL_KEYS
+# SRCU_SORT_VOXEL_KEYS .. SRCU_SORT_BATCH_CELL_KEYS: one table per sort kind,
+# the batch kinds for chains of more than one cloud
+SORT_KINDS = {"voxel": 0, "cell": 1, "batch_voxel": 2, "batch_cell": 3}
 
 
 class SrcuSortConfig(ctypes.Structure):
@@ -562,7 +564,8 @@ class Context:
 
     def sort_tuning(self, kind: str | None = None):
         """[(max_points, launch shape index)] this context sorts `kind` keys
-        with ("voxel" or "cell"); both as a dict when kind is None."""
+        with ("voxel", "cell", "batch_voxel" or "batch_cell"); all of them as a
+        dict when kind is None."""
         if kind is None:
             return {k: self.sort_tuning(k) for k in SORT_KINDS}
         cap = SORT_TUNING_MAX
@@ -575,8 +578,9 @@ class Context:
 
     def set_sort_tuning(self, table, kind: str | None = None) -> None:
         """Installs [(max_points, launch shape index)], ascending sizes, for
-        the `kind` sort ("voxel" or "cell"; both when None); the last entry
-        also covers larger sorts.  An empty table restores the built-in one."""
+        the `kind` sort ("voxel", "cell", "batch_voxel" or "batch_cell"; all
+        four when None); the last entry also covers larger sorts.  An empty
+        table restores the built-in one."""
         if kind is None:
             for k in SORT_KINDS:
                 self.set_sort_tuning(table, k)

@@ -9,11 +9,18 @@ measures every shape on the real chain -- voxel centroid (voxel-key sort over
 the input points) then radius normals (cell-key sort over the centroids) on a
 georeferenced scan -- at one input size per size class, and picks per class
 the shape with the least sort time.  The shapes cover keys per thread, blocks
-per SM and threads per block (256 or 512: the first 256 threads own one digit
-each).  Digit width stays at 8 bits.  It also times the normals kernel's three neighbour walks
-(range by range through L1, range by range from shared memory filled by bulk
-copies, each lane's ranges as one list with packed f32x2 arithmetic) over the
-same sizes and keeps the fastest.
+per SM, threads per block (256 or 512) and digit width (8 bits, or 9 bits in
+512-thread shapes: a thread per digit bin).  It also times the normals
+kernel's three neighbour walks (range by range through L1, range by range from
+shared memory filled by bulk copies, and the L1 walk in packed f32x2
+arithmetic) over the same sizes and keeps the fastest.
+
+Shapes and digit width are tuned twice: on one georeferenced scan, and on
+batches of whole clouds from the uneven-cloud generator of the 256-cloud batch
+workload (leaves 0.05/0.1/0.2 m, radius 5 x leaf), cut to the same sizes.  A
+batch's keys carry the cloud id above each cloud's key, so they are wider,
+and the 9-bit-digit shapes save a pass on them where they save none on one
+scan; a context takes its batch tables for chains of more than one cloud.
 
     python -m spatialrust_b200.autotune                 # measure, print the table
     python -m spatialrust_b200.autotune --write         # ... and rewrite csrc/sort_tuning.h
@@ -50,39 +57,68 @@ L2_FLUSH_BYTES = 256 << 20  # written before every timed chain: inputs start out
 _HEADER = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "sort_tuning.h")
 
 
-def measure(sizes=SAMPLE_POINTS, reps: int = 10, warmup: int = 3, seed: int = 1,
-            device: int = 0) -> dict:
-    """Sort device time (ms per chain) of every launch shape at every size,
-    and the normals kernel's time with either neighbour gather.
+def batch_clouds(n: int, seed: int = 3):
+    """The first clouds of the uneven-cloud batch generator, the last one cut so
+    that they hold n points: (x, y, z, offsets, leaves, radii)."""
+    from . import synthetic
 
-    Returns {"configs": [...], "runs": [{"points", "voxels", "config",
-    "voxel_sort_ms", "cell_sort_ms"}], "staging": [{"points", "voxels",
-    "staging", "normals_ms"}]}."""
+    clouds, leaves, radii = synthetic.batched_uneven(256, seed=seed, max_points=n)
+    cols, offsets, total = ([], [], []), [0], 0
+    for c in clouds:
+        take = min(c.n, n - total)
+        for col, a in zip(cols, (c.x, c.y, c.z)):
+            col.append(a[:take])
+        total += take
+        offsets.append(total)
+    x, y, z = (np.concatenate(col) for col in cols)
+    k = len(offsets) - 1
+    return x, y, z, np.array(offsets, np.int64), leaves[:k], radii[:k]
+
+
+def measure(sizes=SAMPLE_POINTS, reps: int = 10, warmup: int = 3, seed: int = 1,
+            device: int = 0, batch: bool = True) -> dict:
+    """Sort device time (ms per chain) of every launch shape at every size,
+    on one scan and (batch) on a batch of clouds of that size, and the
+    normals kernel's time with each neighbour walk on the scan.
+
+    Returns {"configs": [...], "runs": [{"workload", "points", "voxels",
+    "clouds", "config", "voxel_sort_ms", "cell_sort_ms"}], "staging":
+    [{"points", "voxels", "staging", "normals_ms"}]}."""
     import torch
 
     from . import _native, synthetic
 
     configs = _native.sort_configs()
     scan = synthetic.georef_scan(max(sizes), seed=seed)
+    batch_src = batch_clouds(max(sizes)) if batch else None
     dev = torch.device("cuda", device)
     ctx = _native.Context(device)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     runs, staging = [], []
 
-    def timed(groups):
+    def timed(enqueue, groups):
         for _ in range(warmup):
-            ctx.voxel_normals_enqueue(cloud, LEAF, None, RADIUS, 3, None, count_shell=False)
+            enqueue()
         ctx.synchronize()
         ctx.profile_read(reset=True)
         ctx.profile_enable(groups)
         for _ in range(reps):
             flush.zero_()
             torch.cuda.synchronize(dev)
-            ctx.voxel_normals_enqueue(cloud, LEAF, None, RADIUS, 3, None, count_shell=False)
+            enqueue()
             ctx.synchronize()
         prof = ctx.profile_read(reset=True)
         ctx.profile_enable([])
         return {g: prof[g]["total_ms"] / reps for g in groups}
+
+    def shapes(workload, n, clouds, enqueue):
+        for c in range(len(configs)):
+            ctx.set_sort_tuning([(BIG, c)])
+            t = timed(enqueue, ["voxel_sort", "cell_sort"])
+            runs.append(dict(workload=workload, points=n, clouds=clouds,
+                             voxels=int(ctx.chain_info()["voxels"]), config=c,
+                             voxel_sort_ms=t["voxel_sort"], cell_sort_ms=t["cell_sort"]))
+        ctx.set_sort_tuning([])
 
     try:
         for n in sizes:
@@ -90,19 +126,37 @@ def measure(sizes=SAMPLE_POINTS, reps: int = 10, warmup: int = 3, seed: int = 1,
             cols = [keep.add(torch.from_numpy(np.ascontiguousarray(a[:n])).to(dev))
                     for a in (scan.x, scan.y, scan.z)]
             cloud = _native.make_cloud(*cols, (), keep)
-            for c in range(len(configs)):
-                ctx.set_sort_tuning([(BIG, c)])
-                t = timed(["voxel_sort", "cell_sort"])
-                runs.append(dict(points=n, voxels=int(ctx.chain_info()["voxels"]), config=c,
-                                 voxel_sort_ms=t["voxel_sort"], cell_sort_ms=t["cell_sort"]))
-            ctx.set_sort_tuning([])
+
+            def scan_chain():
+                ctx.voxel_normals_enqueue(cloud, LEAF, None, RADIUS, 3, None, count_shell=False)
+
+            shapes("scan", n, 1, scan_chain)
             for mode in WALK_MODES:
                 ctx.set_neighbor_staging(mode)
-                t = timed(["normals"])
+                t = timed(scan_chain, ["normals"])
                 staging.append(dict(points=n, voxels=int(ctx.chain_info()["voxels"]), staging=mode,
                                     normals_ms=t["normals"]))
             ctx.set_neighbor_staging(-1)
             del cols, cloud, keep
+            if batch_src is not None:
+                bx, by, bz, offsets, leaves, radii = batch_src
+                # clouds [0, k) hold >= n points; two clouds at least, so that
+                # the chain takes the batch tables
+                k = max(2, int(np.searchsorted(offsets, n, side="left")))
+                offs = np.minimum(offsets[:k + 1], n)
+                if offs[1] >= n:
+                    offs[1] = n // 2
+                keep = _native._Keep()
+                cols = [keep.add(torch.from_numpy(np.ascontiguousarray(a[:n])).to(dev))
+                        for a in (bx, by, bz)]
+                pts = _native.make_cloud(*cols, (), keep)
+
+                def batch_chain():
+                    ctx.batch_voxel_normals_enqueue(pts, offs, leaves[:k].tolist(),
+                                                    radii[:k].tolist(), 3, None, count_shell=False)
+
+                shapes("batch", n, k, batch_chain)
+                del cols, pts, keep
     finally:
         ctx.set_sort_tuning([])
         ctx.set_neighbor_staging(-1)
@@ -110,17 +164,23 @@ def measure(sizes=SAMPLE_POINTS, reps: int = 10, warmup: int = 3, seed: int = 1,
     return dict(configs=configs, runs=runs, staging=staging)
 
 
+KINDS = ("voxel", "cell", "batch_voxel", "batch_cell")
+
+
 def samples(result: dict, kind: str) -> list:
-    """[(size, [ms per shape])], ascending, for the voxel sorts (kind "voxel")
-    or the cell sorts ("cell").  The size is the chain's point count for both:
-    the library picks a cell sort's shape before the voxel count is known on
-    the host, from the same upper bound."""
+    """[(size, [ms per shape])], ascending, for one sort kind: the voxel sorts
+    ("voxel") or the cell sorts ("cell") of the scan chains, or the same of the
+    batch chains ("batch_voxel", "batch_cell").  The size is the chain's point
+    count for both sorts: the library picks a cell sort's shape before the
+    voxel count is known on the host, from the same upper bound."""
     n_cfg = len(result["configs"])
+    workload = "batch" if kind.startswith("batch_") else "scan"
+    field = "voxel_sort_ms" if kind.endswith("voxel") else "cell_sort_ms"
     by = {}
     for r in result["runs"]:
-        keys, ms = ((r["points"], r["voxel_sort_ms"]) if kind == "voxel"
-                    else (r["points"], r["cell_sort_ms"]))
-        by.setdefault(keys, [None] * n_cfg)[r["config"]] = ms
+        if r.get("workload", "scan") != workload:
+            continue
+        by.setdefault(r["points"], [None] * n_cfg)[r["config"]] = r[field]
     out = [(k, ms) for k, ms in by.items() if all(m is not None for m in ms)]
     return sorted(out, key=lambda t: t[0])
 
@@ -176,9 +236,11 @@ def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> s
         "// measurements; srcu_set_sort_tuning replaces it per context.",
         "//",
         "// One table per sort kind: the voxel-key sort over the input points and the",
-        "// cell-key sort over the radius-grid points.  Entry k applies to sorts of at",
-        "// most k*SortTuneMaxPoints[k] keys (the last entry to every larger sort);",
-        "// k*SortTuneConfig[k] indexes kSortItems / kSortMinBlocks in radix.cuh.",
+        "// cell-key sort over the radius-grid points, of one cloud and (Batch) of a",
+        "// batch of clouds.  Entry k applies to sorts of at most k*SortTuneMaxPoints[k]",
+        "// keys (the last entry to every larger sort); k*SortTuneConfig[k] indexes the",
+        "// launch shapes of radix.cuh (kSortItems, kSortMinBlocks, kSortThreads,",
+        "// kSortDigitBits).",
         "// kNeighborStaging: the normals kernel's neighbour walk -- range by range",
         "// through L1 (0), range by range from shared memory filled by bulk copies (1),",
         "// or the L1 walk in packed f32x2 arithmetic (2).",
@@ -186,14 +248,19 @@ def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> s
     if result is not None:
         lines.append("//")
         lines.append("// Measured sort ms (georeferenced scan, leaf "
-                     f"{LEAF}, radius {RADIUS}; L2 flushed before every chain):")
+                     f"{LEAF}, radius {RADIUS}; batches of uneven clouds, leaf 0.05-0.2,")
+        lines.append("// radius 5 x leaf; L2 flushed before every chain), per shape")
+        lines.append("// (keys per thread x blocks per SM x threads / digit bits):")
         cfgs = result["configs"]
-        shapes = "  ".join(f"{c['items_per_thread']:>2}x{c['blocks_per_sm']}x{c.get('threads_per_block', 256)}"
-                           for c in cfgs)
-        for kind in ("voxel", "cell"):
-            lines.append(f"//   {kind}-key sort     points  {shapes}")
-            for keys, ms in samples(result, kind):
-                lines.append(f"//   {'':14} {keys:>9}  " + "  ".join(f"{m:6.4f}" for m in ms))
+        shapes = "  ".join(f"{c['items_per_thread']}x{c['blocks_per_sm']}x{c.get('threads_per_block', 256)}"
+                           f"/{c.get('digit_bits', 8)}" for c in cfgs)
+        for kind in KINDS:
+            rows = samples(result, kind)
+            if not rows:
+                continue
+            lines.append(f"//   {kind} sort, points: {shapes}")
+            for keys, ms in rows:
+                lines.append(f"//   {keys:>9}  " + "  ".join(f"{m:6.4f}" for m in ms))
         if result.get("staging"):
             lines.append("// Normals kernel ms per chain, neighbour walk L1 / staged / packed:")
             by_n = {}
@@ -210,8 +277,10 @@ def header_text(tables: dict, result: dict | None = None, staging: int = 0) -> s
         "namespace srcu {",
         "",
     ]
-    for kind, name in (("voxel", "Voxel"), ("cell", "Cell")):
-        table = tables[kind]
+    for kind, name in (("voxel", "Voxel"), ("cell", "Cell"), ("batch_voxel", "BatchVoxel"),
+                       ("batch_cell", "BatchCell")):
+        # without batch measurements, a batch kind takes its scan kind's table
+        table = tables.get(kind) or tables[kind.replace("batch_", "")]
         lines += [
             f"constexpr uint32_t k{name}SortTuneCount = {len(table)};",
             f"constexpr uint64_t k{name}SortTuneMaxPoints[] = {{" + ", ".join(
@@ -233,6 +302,7 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--sizes", type=int, nargs="*", default=list(SAMPLE_POINTS))
     ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--no-batch", action="store_true", help="tune on the scan alone")
     ap.add_argument("--json", help="write the measurements and the chosen table here")
     ap.add_argument("--write", action="store_true", help="rewrite csrc/sort_tuning.h")
     ap.add_argument("--from-json", help="take the measurements from an earlier --json run")
@@ -241,19 +311,21 @@ def main(argv=None) -> int:
         with open(args.from_json) as f:
             result = json.load(f)
     else:
-        result = measure(args.sizes, reps=args.reps)
-    tables = {kind: choose(result, kind) for kind in ("voxel", "cell")}
+        result = measure(args.sizes, reps=args.reps, batch=not args.no_batch)
+    tables = {kind: choose(result, kind) for kind in KINDS
+              if kind in ("voxel", "cell") or samples(result, kind)}
     staging = choose_staging(result)
     result["tables"] = {k: [[m, c] for m, c in t] for k, t in tables.items()}
     result["neighbor_staging"] = staging
     for r in result["runs"]:
-        print(f"points {r['points']:>9} voxels {r['voxels']:>9} config {r['config']}: "
-              f"voxel sort {r['voxel_sort_ms']:.4f} ms  cell sort {r['cell_sort_ms']:.4f} ms")
+        print(f"{r.get('workload', 'scan'):5} points {r['points']:>9} voxels {r['voxels']:>9} "
+              f"config {r['config']}: voxel sort {r['voxel_sort_ms']:.4f} ms  "
+              f"cell sort {r['cell_sort_ms']:.4f} ms")
     for r in result.get("staging", []):
         print(f"points {r['points']:>9} voxels {r['voxels']:>9} staging {r['staging']}: "
               f"normals {r['normals_ms']:.4f} ms")
-    print("voxel-key sort table:", tables["voxel"])
-    print("cell-key sort table:", tables["cell"])
+    for kind, table in tables.items():
+        print(f"{kind} sort table:", table)
     print("neighbor staging:", staging)
     if args.json:
         with open(args.json, "w") as f:

@@ -16,9 +16,11 @@
 
 namespace srcu {
 
-constexpr int RADIX_BITS = 8;
+constexpr int RADIX_BITS = 8;        // the sort's narrow digit
 constexpr int RADIX_BINS = 256;
-constexpr int MAX_DIGITS = 8;  // 64-bit keys
+constexpr int WIDE_RADIX_BITS = 9;   // the wide digit of the 512-thread sort shapes
+constexpr int MAX_RADIX_BINS = 1 << WIDE_RADIX_BITS;
+constexpr int MAX_DIGITS = 8;        // 64-bit keys, at either width
 constexpr int MAX_COLS = 12;   // x, y, z + up to 9 attribute columns
 
 // Bounds over finite coordinates (ordered-uint encoded), with flags for
@@ -151,8 +153,8 @@ struct Control {
   NormalCounters ncount;
   SortState vsort;  // voxel-key sort
   SortState csort;  // cell-key sort
-  uint32_t hist_v[MAX_DIGITS * RADIX_BINS];  // voxel-key digit histograms
-  uint32_t hist_c[MAX_DIGITS * RADIX_BINS];  // cell-key digit histograms
+  uint32_t hist_v[MAX_DIGITS * MAX_RADIX_BINS];  // voxel-key digit histograms
+  uint32_t hist_c[MAX_DIGITS * MAX_RADIX_BINS];  // cell-key digit histograms
   unsigned long long col_total;  // sum over clouds of dims_x * dims_y
   uint32_t dense_cols;           // 1: the column table is dense (it fits the table buffer)
   uint32_t pad2;

@@ -2,8 +2,10 @@
 // one persistent cooperative kernel per sort.
 //
 // Phase 1 computes every key once (kept for the first pass) and histograms
-// its 8-bit digits (shared-memory atomics, which B200 executes at full rate
-// even when lanes collide).  After a grid
+// its digits (shared-memory atomics, which B200 executes at full rate even
+// when lanes collide).  Digits are 8 bits wide, or 9 bits in the shapes built
+// for them (512 threads) when that takes fewer passes over the key width at
+// hand -- 43-bit keys of a batch sort in 5 passes instead of 6.  After a grid
 // barrier, each digit pass that is not trivial (some key differs in that
 // digit) ranks 4096-key tiles with a warp-level multi-split, resolves the
 // tile's global digit offsets by decoupled look-back over earlier tiles, and
@@ -25,6 +27,8 @@
 // block resident for the barriers; every wait is bounded.
 #pragma once
 
+#include <type_traits>
+
 #include "plans.cuh"
 
 namespace srcu {
@@ -43,18 +47,24 @@ struct OnesweepTileSmem {
   uint32_t vals[TILE];
 };
 
-// Shared memory of one sort block of WARPS warps for tiles of TILE keys.
-template <int TILE, int WARPS = OS_WARPS>
+// Shared memory of one sort block of WARPS warps for tiles of TILE keys and
+// digits of up to DBITS bits.  The per-warp digit counters of the 9-bit shapes
+// are 16-bit (a tile holds fewer than 2^16 keys), which keeps two blocks of
+// 512 threads on an SM.
+template <int TILE, int WARPS = OS_WARPS, int DBITS = RADIX_BITS>
 struct OnesweepSmemT {
+  static constexpr int BINS = 1 << DBITS;
+  using WarpCount = typename std::conditional<(DBITS > RADIX_BITS), uint16_t, uint32_t>::type;
+  static_assert(TILE < 65536, "16-bit per-warp digit counters");
   union {
     OnesweepTileSmem<TILE> tile;
-    uint32_t hist[HIST_COPIES][MAX_DIGITS][RADIX_BINS];
+    uint32_t hist[HIST_COPIES][MAX_DIGITS][BINS];
   } u;
-  uint32_t whist[WARPS][RADIX_BINS];
-  uint32_t match[WARPS][RADIX_BINS];  // per-warp peer masks, zero between uses
-  uint32_t digit_start[RADIX_BINS];
-  uint32_t tile_excl[RADIX_BINS];
-  uint32_t gbase[RADIX_BINS];
+  WarpCount whist[WARPS][BINS];
+  uint32_t match[WARPS][BINS];  // per-warp peer masks, zero between uses
+  uint32_t digit_start[BINS];
+  uint32_t tile_excl[BINS];
+  uint32_t gbase[BINS];
   uint32_t scratch[WARPS];
   uint32_t trivial[MAX_DIGITS];
   uint32_t active[MAX_DIGITS];
@@ -64,14 +74,21 @@ struct OnesweepSmemT {
 using OnesweepSmem = OnesweepSmemT<OS_TILE>;
 
 // The sort's launch shapes the library is built with: keys per thread, the
-// blocks per SM the registers are capped for, and threads per block (8-bit
-// digits throughout: the first 256 threads of a block own one digit each).
-// The autotuner picks among them per input size (srcu_set_sort_tuning).
-constexpr int SORT_CONFIGS = 6;
-constexpr int kSortItems[SORT_CONFIGS] = {16, 8, 12, 8, 8, 12};
-constexpr int kSortMinBlocks[SORT_CONFIGS] = {2, 3, 3, 4, 2, 1};
-constexpr int kSortThreads[SORT_CONFIGS] = {256, 256, 256, 256, 512, 512};
+// blocks per SM the registers are capped for, threads per block, and the
+// widest digit (a thread per digit bin: 256 threads for 8-bit digits, 512
+// for 9-bit ones, which run 8-bit passes when 9 bits save none).  The
+// autotuner picks among them per input size (srcu_set_sort_tuning).
+constexpr int SORT_CONFIGS = 8;
+constexpr int kSortItems[SORT_CONFIGS] = {16, 8, 12, 8, 8, 12, 8, 12};
+constexpr int kSortMinBlocks[SORT_CONFIGS] = {2, 3, 3, 4, 2, 1, 2, 1};
+constexpr int kSortThreads[SORT_CONFIGS] = {256, 256, 256, 256, 512, 512, 512, 512};
+constexpr int kSortDigitBits[SORT_CONFIGS] = {8, 8, 8, 8, 8, 8, 9, 9};
 constexpr int SORT_MIN_TILE = 2048;  // the smallest tile (keys) the look-back buffer is sized for
+// Look-back words per key of a tile of TILE keys with BINS digit bins is
+// BINS / TILE; the buffer holds RADIX_BINS / SORT_MIN_TILE per key.
+constexpr bool lookback_fits(int tile, int bins) {
+  return int64_t(bins) * SORT_MIN_TILE <= int64_t(RADIX_BINS) * tile;
+}
 
 // Ping-pong buffers of one sort.
 struct SortBuffers {
@@ -141,46 +158,57 @@ __device__ __forceinline__ void grid_barrier(SortState *st, uint32_t *status) {
   __syncthreads();
 }
 
-template <class Src, int ITEMS = OS_ITEMS, int MINB = 2, int THREADS = OS_THREADS>
+template <class Src, int ITEMS = OS_ITEMS, int MINB = 2, int THREADS = OS_THREADS,
+          int DBITS = RADIX_BITS>
 __global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, uint32_t *hist,
                                                      SortBuffers buf, uint32_t epoch_off,
                                                      int work_slot, SortState *st) {
-  static_assert(THREADS >= RADIX_BINS && THREADS % 32 == 0, "a thread per digit at least");
   constexpr int WARPS = THREADS / 32;
   constexpr int TILE = THREADS * ITEMS;
   constexpr int WARP_ITEMS = ITEMS * 32;
+  constexpr uint32_t BINS = 1u << DBITS;  // digit bins of the widest digit; `hist` stride
+  static_assert(THREADS >= int(BINS) && THREADS % 32 == 0, "a thread per digit bin at least");
+  static_assert(DBITS >= RADIX_BITS && DBITS <= WIDE_RADIX_BITS, "digit width");
+  using Smem = OnesweepSmemT<TILE, WARPS, DBITS>;
+  using WarpCount = typename Smem::WarpCount;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  OnesweepSmemT<TILE, WARPS> &sm = *reinterpret_cast<OnesweepSmemT<TILE, WARPS> *>(smem_raw);
+  Smem &sm = *reinterpret_cast<Smem *>(smem_raw);
   if (ld_relaxed_u32(&ctl->status)) return;  // before any barrier: every block agrees
   src.prepare(ctl);
   const uint32_t n = src.count(ctl);
   const uint32_t kbits = src.key_bits();
-  const uint32_t nd = kbits == 0 ? 1u : (kbits + RADIX_BITS - 1) / RADIX_BITS;
+  // The digit width: DBITS where it takes fewer passes over kbits than 8-bit
+  // digits, else 8 (every block computes the same).
+  const uint32_t nd_narrow = kbits == 0 ? 1u : (kbits + RADIX_BITS - 1) / RADIX_BITS;
+  const uint32_t nd_wide = kbits == 0 ? 1u : (kbits + DBITS - 1) / DBITS;
+  const uint32_t dbits = nd_wide < nd_narrow ? uint32_t(DBITS) : uint32_t(RADIX_BITS);
+  const uint32_t nd = nd_wide < nd_narrow ? nd_wide : nd_narrow;
+  const uint32_t dmask = (1u << dbits) - 1u;
   const uint32_t idx_bits = n > 1 ? bit_width_u64(uint64_t(n) - 1) : 0u;
   const bool packed = kbits + idx_bits <= 64;
   const uint32_t shift0 = packed ? idx_bits : 0u;
   const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
-  const bool owner = t < RADIX_BINS;  // this thread owns digit t in the per-digit steps
+  const bool owner = t <= dmask;  // this thread owns digit t in the per-digit steps
 
   // ---- phase 1: digit histograms ----------------------------------------
-  for (uint32_t i = t; i < HIST_COPIES * MAX_DIGITS * RADIX_BINS; i += THREADS)
+  for (uint32_t i = t; i < HIST_COPIES * MAX_DIGITS * BINS; i += THREADS)
     (&sm.u.hist[0][0][0])[i] = 0;
-  for (uint32_t i = t; i < WARPS * RADIX_BINS; i += THREADS) (&sm.match[0][0])[i] = 0;
+  for (uint32_t i = t; i < WARPS * BINS; i += THREADS) (&sm.match[0][0])[i] = 0;
   __syncthreads();
   {
     // The keys are computed once, here, and kept in the ping-pong buffer that
     // the first digit pass reads (keys[1]); the grid barrier below publishes
     // them like any pass's output.
-    uint32_t(*h)[RADIX_BINS] = sm.u.hist[warp & (HIST_COPIES - 1)];
+    uint32_t(*h)[BINS] = sm.u.hist[warp & (HIST_COPIES - 1)];
     uint64_t *kcache = buf.keys[1];
     for (uint32_t i = blockIdx.x * THREADS + t; i < n; i += gridDim.x * THREADS) {
       const uint64_t k = src.key(i);
       kcache[i] = k;
-      for (uint32_t d = 0; d < nd; ++d) atomicAdd(&h[d][uint32_t(k >> (RADIX_BITS * d)) & 0xffu], 1u);
+      for (uint32_t d = 0; d < nd; ++d) atomicAdd(&h[d][uint32_t(k >> (dbits * d)) & dmask], 1u);
     }
   }
   __syncthreads();
-  for (uint32_t i = t; i < nd * RADIX_BINS; i += THREADS) {
+  for (uint32_t i = t; i < nd * BINS; i += THREADS) {
     uint32_t c = 0;
 #pragma unroll
     for (int cp = 0; cp < HIST_COPIES; ++cp) c += (&sm.u.hist[cp][0][0])[i];
@@ -194,7 +222,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, u
   __syncthreads();
   if (owner)
     for (uint32_t d = 0; d < nd; ++d)
-      if (ld_relaxed_u32(&hist[d * RADIX_BINS + t]) == n) sm.trivial[d] = 1;
+      if (ld_relaxed_u32(&hist[d * BINS + t]) == n) sm.trivial[d] = 1;
   __syncthreads();
   if (t == 0) {
     uint32_t na = 0;
@@ -217,11 +245,11 @@ __global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, u
 
   // ---- digit passes ------------------------------------------------------
   for (uint32_t p = 0; p < num_active; ++p) {
-    const uint32_t shift = shift0 + sm.active[p] * RADIX_BITS;
+    const uint32_t shift = shift0 + sm.active[p] * dbits;
     {
       uint32_t total;
       const uint32_t ds = block_exclusive_sum<THREADS>(
-          owner ? ld_relaxed_u32(&hist[sm.active[p] * RADIX_BINS + t]) : 0u, sm.scratch, &total);
+          owner ? ld_relaxed_u32(&hist[sm.active[p] * BINS + t]) : 0u, sm.scratch, &total);
       if (owner) sm.digit_start[t] = ds;
     }
     const bool from_src = p == 0;
@@ -234,7 +262,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, u
 
     for (;;) {
       if (t == 0) sm.tile = atomicAdd(ctr, 1u);
-      for (uint32_t i = t; i < WARPS * RADIX_BINS; i += THREADS) (&sm.whist[0][0])[i] = 0;
+      for (uint32_t i = t; i < WARPS * BINS; i += THREADS) (&sm.whist[0][0])[i] = 0;
       __syncthreads();
       const uint32_t tile = sm.tile;
       if (tile >= num_tiles) break;
@@ -269,7 +297,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, u
 #pragma unroll
       for (int i = 0; i < ITEMS; ++i) {
         const bool valid = (wbase + uint32_t(i) * 32u + lane) < n;
-        const uint32_t d = uint32_t(k[i] >> shift) & 0xffu;
+        const uint32_t d = uint32_t(k[i] >> shift) & dmask;
         const uint32_t vmask = __ballot_sync(FULL_MASK, valid);
         const uint32_t d0 = __shfl_sync(FULL_MASK, d, 0);
         const bool uniform = __all_sync(FULL_MASK, !valid || d == d0);
@@ -286,7 +314,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, u
           leader = 31u - __clz(peers);
           if (lane == leader) {
             prev = sm.whist[warp][d];
-            sm.whist[warp][d] = prev + uint32_t(__popc(peers));
+            sm.whist[warp][d] = WarpCount(prev + uint32_t(__popc(peers)));
             if (!uniform) sm.match[warp][d] = 0u;
           }
         }
@@ -297,12 +325,12 @@ __global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, u
       __syncthreads();
       // Thread t owns digit t: exclusive prefix over warps, tile count.
       uint32_t cnt = 0;
-      uint64_t *lb_mine = buf.lookback + size_t(tile) * RADIX_BINS + t;
+      uint64_t *lb_mine = buf.lookback + size_t(tile) * BINS + t;
       if (owner) {
 #pragma unroll
         for (int w = 0; w < WARPS; ++w) {
           const uint32_t c = sm.whist[w][t];
-          sm.whist[w][t] = cnt;
+          sm.whist[w][t] = WarpCount(cnt);
           cnt += c;
         }
         // Publish the tile aggregate as early as possible.
@@ -316,7 +344,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, u
 #pragma unroll
       for (int i = 0; i < ITEMS; ++i) {
         if ((wbase + uint32_t(i) * 32u + lane) < n) {
-          const uint32_t d = uint32_t(k[i] >> shift) & 0xffu;
+          const uint32_t d = uint32_t(k[i] >> shift) & dmask;
           const uint32_t pos = sm.tile_excl[d] + sm.whist[warp][d] + rank[i];
           sm.u.tile.keys[pos] = k[i];
           if (!packed) sm.u.tile.vals[pos] = v[i];
@@ -333,7 +361,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, u
           uint64_t w[LB_WIDTH];
 #pragma unroll
           for (int q = 0; q < LB_WIDTH; ++q)
-            w[q] = (j - q >= 0) ? ld_relaxed(buf.lookback + size_t(j - q) * RADIX_BINS + t)
+            w[q] = (j - q >= 0) ? ld_relaxed(buf.lookback + size_t(j - q) * BINS + t)
                                 : lb_pack(epoch, LB_INC, 0);
           uint32_t consumed = 0;
 #pragma unroll
@@ -361,7 +389,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_sort(Src src, Control *ctl, u
       const uint32_t tile_n = min(uint32_t(TILE), n - base);
       for (uint32_t j = t; j < tile_n; j += THREADS) {
         const uint64_t kk = sm.u.tile.keys[j];
-        const uint32_t pos = sm.gbase[uint32_t(kk >> shift) & 0xffu] + j;
+        const uint32_t pos = sm.gbase[uint32_t(kk >> shift) & dmask] + j;
         if (pos < n) {
           kout[pos] = kk;
           if (!packed) vout[pos] = sm.u.tile.vals[j];

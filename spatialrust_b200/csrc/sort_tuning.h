@@ -83,6 +83,12 @@ constexpr int32_t kVoxelSortTuneConfig[] = {1, 2, 0, 2};
 constexpr uint32_t kCellSortTuneCount = 3;
 constexpr uint64_t kCellSortTuneMaxPoints[] = {881743ull, 1246973ull, UINT64_MAX};
 constexpr int32_t kCellSortTuneConfig[] = {1, 0, 2};
+constexpr uint32_t kBatchVoxelSortTuneCount = 4;
+constexpr uint64_t kBatchVoxelSortTuneMaxPoints[] = {623486ull, 881743ull, 1246973ull, UINT64_MAX};
+constexpr int32_t kBatchVoxelSortTuneConfig[] = {1, 2, 0, 2};
+constexpr uint32_t kBatchCellSortTuneCount = 3;
+constexpr uint64_t kBatchCellSortTuneMaxPoints[] = {881743ull, 1246973ull, UINT64_MAX};
+constexpr int32_t kBatchCellSortTuneConfig[] = {1, 0, 2};
 // 1: the normals kernel gathers candidates through shared memory (bulk copies)
 constexpr int32_t kNeighborStaging = 0;
 

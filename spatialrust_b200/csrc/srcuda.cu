@@ -58,11 +58,11 @@ struct srcu_ctx {
   int neighbor_staging = 0;  // k_normals' neighbour walk: WALK_L1, WALK_STAGED or WALK_PACKED
   // co-resident blocks per SM of each sort launch shape, voxel-key and cell-key sorts
   int occ_sort_v[SORT_CONFIGS] = {}, occ_sort_c[SORT_CONFIGS] = {};
-  // sort launch shape by input size, per sort kind (SRCU_SORT_VOXEL_KEYS /
-  // SRCU_SORT_CELL_KEYS; sort_tuning.h, srcu_set_sort_tuning)
-  uint64_t tune_max_points[2][SRCU_SORT_TUNING_MAX] = {};
-  int32_t tune_config[2][SRCU_SORT_TUNING_MAX] = {};
-  uint32_t tune_count[2] = {};
+  // sort launch shape by input size, per sort kind (SRCU_SORT_VOXEL_KEYS ..
+  // SRCU_SORT_BATCH_CELL_KEYS; sort_tuning.h, srcu_set_sort_tuning)
+  uint64_t tune_max_points[SRCU_SORT_KINDS][SRCU_SORT_TUNING_MAX] = {};
+  int32_t tune_config[SRCU_SORT_KINDS][SRCU_SORT_TUNING_MAX] = {};
+  uint32_t tune_count[SRCU_SORT_KINDS] = {};
   // input staging (host inputs are copied here)
   DevBuf in[MAX_COLS];
   // sort
@@ -557,7 +557,8 @@ cudaError_t launch_sort_config(cudaStream_t stream, uint32_t grid_cap, const Src
                                uint32_t epoch_off, int work_slot, SortState *st, uint64_t n_max) {
   constexpr int THREADS = kSortThreads[C];
   constexpr int TILE = THREADS * kSortItems[C];
-  static_assert(TILE >= SORT_MIN_TILE, "the look-back buffer is sized for SORT_MIN_TILE");
+  constexpr int DBITS = kSortDigitBits[C];
+  static_assert(lookback_fits(TILE, 1 << DBITS), "the look-back buffer's words per key");
   const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, TILE));
   const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(tiles, grid_cap));
   Src s = src;
@@ -569,17 +570,18 @@ cudaError_t launch_sort_config(cudaStream_t stream, uint32_t grid_cap, const Src
   SortState *ss = st;
   void *args[] = {&s, &c, &h, &b, &e, &w, &ss};
   return cudaLaunchCooperativeKernel(
-      reinterpret_cast<const void *>(&k_sort<Src, kSortItems[C], kSortMinBlocks[C], THREADS>),
-      dim3(grid), dim3(THREADS), args, sizeof(OnesweepSmemT<TILE, THREADS / 32>), stream);
+      reinterpret_cast<const void *>(&k_sort<Src, kSortItems[C], kSortMinBlocks[C], THREADS, DBITS>),
+      dim3(grid), dim3(THREADS), args, sizeof(OnesweepSmemT<TILE, THREADS / 32, DBITS>), stream);
 }
 
 template <class Src, int C>
 cudaError_t sort_config_setup(int *occ) {
   constexpr int THREADS = kSortThreads[C];
   constexpr int TILE = THREADS * kSortItems[C];
-  using Smem = OnesweepSmemT<TILE, THREADS / 32>;
-  const void *kern =
-      reinterpret_cast<const void *>(&k_sort<Src, kSortItems[C], kSortMinBlocks[C], THREADS>);
+  constexpr int DBITS = kSortDigitBits[C];
+  using Smem = OnesweepSmemT<TILE, THREADS / 32, DBITS>;
+  const void *kern = reinterpret_cast<const void *>(
+      &k_sort<Src, kSortItems[C], kSortMinBlocks[C], THREADS, DBITS>);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(sizeof(Smem)));
   if (e != cudaSuccess) return e;
@@ -590,13 +592,15 @@ cudaError_t sort_config_setup(int *occ) {
 
 template <class Src>
 cudaError_t sort_setup(int (&occ)[SORT_CONFIGS]) {
-  static_assert(SORT_CONFIGS == 6, "one setup per launch shape");
+  static_assert(SORT_CONFIGS == 8, "one setup per launch shape");
   cudaError_t e = sort_config_setup<Src, 0>(&occ[0]);
   if (e == cudaSuccess) e = sort_config_setup<Src, 1>(&occ[1]);
   if (e == cudaSuccess) e = sort_config_setup<Src, 2>(&occ[2]);
   if (e == cudaSuccess) e = sort_config_setup<Src, 3>(&occ[3]);
   if (e == cudaSuccess) e = sort_config_setup<Src, 4>(&occ[4]);
   if (e == cudaSuccess) e = sort_config_setup<Src, 5>(&occ[5]);
+  if (e == cudaSuccess) e = sort_config_setup<Src, 6>(&occ[6]);
+  if (e == cudaSuccess) e = sort_config_setup<Src, 7>(&occ[7]);
   return e;
 }
 
@@ -608,9 +612,22 @@ int sort_config_for(const srcu_ctx *ctx, int kind, uint64_t n) {
 }
 
 void builtin_sort_tuning(srcu_ctx *ctx, int kind) {
-  const uint32_t cnt = kind == SRCU_SORT_VOXEL_KEYS ? kVoxelSortTuneCount : kCellSortTuneCount;
-  const uint64_t *mp = kind == SRCU_SORT_VOXEL_KEYS ? kVoxelSortTuneMaxPoints : kCellSortTuneMaxPoints;
-  const int32_t *cf = kind == SRCU_SORT_VOXEL_KEYS ? kVoxelSortTuneConfig : kCellSortTuneConfig;
+  uint32_t cnt;
+  const uint64_t *mp;
+  const int32_t *cf;
+  switch (kind) {
+    case SRCU_SORT_VOXEL_KEYS:
+      cnt = kVoxelSortTuneCount, mp = kVoxelSortTuneMaxPoints, cf = kVoxelSortTuneConfig;
+      break;
+    case SRCU_SORT_CELL_KEYS:
+      cnt = kCellSortTuneCount, mp = kCellSortTuneMaxPoints, cf = kCellSortTuneConfig;
+      break;
+    case SRCU_SORT_BATCH_VOXEL_KEYS:
+      cnt = kBatchVoxelSortTuneCount, mp = kBatchVoxelSortTuneMaxPoints, cf = kBatchVoxelSortTuneConfig;
+      break;
+    default:
+      cnt = kBatchCellSortTuneCount, mp = kBatchCellSortTuneMaxPoints, cf = kBatchCellSortTuneConfig;
+  }
   ctx->tune_count[kind] = cnt;
   for (uint32_t k = 0; k < cnt; ++k) {
     ctx->tune_max_points[kind][k] = mp[k];
@@ -644,6 +661,12 @@ srcu_status launch_sort_tuned(srcu_ctx *ctx, int kind, const Src &src, uint64_t 
       break;
     case 5:
       e = launch_sort_config<Src, 5>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
+      break;
+    case 6:
+      e = launch_sort_config<Src, 6>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
+      break;
+    case 7:
+      e = launch_sort_config<Src, 7>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
       break;
     default:
       e = launch_sort_config<Src, 0>(ctx->stream, cap, src, ctx->ctl, hist, sb, epoch_off, work_slot, st, n_max);
@@ -725,7 +748,9 @@ srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t
   src.y = in[1];
   src.z = in[2];
   src.bt = bt;
-  ST_TRY(launch_sort_tuned(ctx, SRCU_SORT_VOXEL_KEYS, src, n, ctx->ctl->hist_v, EP_VSORT, WK_VSORT, &ctx->ctl->vsort,
+  // a batch's keys carry the cloud id above the per-cloud key: tuned apart
+  ST_TRY(launch_sort_tuned(ctx, bt.clouds > 1 ? SRCU_SORT_BATCH_VOXEL_KEYS : SRCU_SORT_VOXEL_KEYS,
+                           src, n, ctx->ctl->hist_v, EP_VSORT, WK_VSORT, &ctx->ctl->vsort,
                            ctx->occ_sort_v, SRCU_K_VOXEL_SORT));
   const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n, SEG_TILE));
   const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(ctx->occ_seg));
@@ -769,8 +794,9 @@ srcu_status enqueue_grid(srcu_ctx *ctx, const float *x, const float *y, const fl
   src.count_dev = count_dev;
   src.voxel_keys = voxel_keys;
   src.bt = bt;
-  ST_TRY(launch_sort_tuned(ctx, SRCU_SORT_CELL_KEYS, src, n_max, ctx->ctl->hist_c, EP_CSORT, WK_CSORT,
-                           &ctx->ctl->csort, ctx->occ_sort_c, SRCU_K_CELL_SORT));
+  ST_TRY(launch_sort_tuned(ctx, bt.clouds > 1 ? SRCU_SORT_BATCH_CELL_KEYS : SRCU_SORT_CELL_KEYS,
+                           src, n_max, ctx->ctl->hist_c, EP_CSORT, WK_CSORT, &ctx->ctl->csort,
+                           ctx->occ_sort_c, SRCU_K_CELL_SORT));
   const uint32_t tiles = std::max<uint32_t>(1, ceil_div(n_max, CELL_TILE));
   const uint32_t grid_c = std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * uint32_t(ctx->occ_cells));
   {
@@ -1019,8 +1045,7 @@ srcu_status srcu_create(int device, uint64_t hbm_budget_bytes, srcu_ctx **out) {
       sort_setup<CellKeySrc>(ctx->occ_sort_c) != cudaSuccess ||
       sort_config_setup<FirstSeenSrc, 0>(&ctx->occ_sort_order) != cudaSuccess)
     return bail(SRCU_ERR_CUDA);
-  builtin_sort_tuning(ctx, SRCU_SORT_VOXEL_KEYS);
-  builtin_sort_tuning(ctx, SRCU_SORT_CELL_KEYS);
+  for (int kind = 0; kind < SRCU_SORT_KINDS; ++kind) builtin_sort_tuning(ctx, kind);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals, k_normals<true>, NM_THREADS, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->occ_normals_staged,
                                                 k_normals<true, false, WALK_STAGED>, NM_THREADS, 0);
@@ -1097,7 +1122,7 @@ int srcu_sort_configs(srcu_sort_config *out, int max_entries) {
   for (int c = 0; c < SORT_CONFIGS && c < max_entries && out; ++c) {
     out[c].items_per_thread = uint32_t(kSortItems[c]);
     out[c].blocks_per_sm = uint32_t(kSortMinBlocks[c]);
-    out[c].digit_bits = RADIX_BITS;
+    out[c].digit_bits = uint32_t(kSortDigitBits[c]);
     out[c].threads_per_block = uint32_t(kSortThreads[c]);
   }
   return SORT_CONFIGS;
@@ -1106,9 +1131,10 @@ int srcu_sort_configs(srcu_sort_config *out, int max_entries) {
 srcu_status srcu_set_sort_tuning(srcu_ctx *ctx, int32_t kind, const uint64_t *max_points,
                                  const int32_t *config, uint32_t count) {
   if (!ctx) return SRCU_ERR_INVALID_ARGUMENT;
-  if (kind != SRCU_SORT_VOXEL_KEYS && kind != SRCU_SORT_CELL_KEYS)
-    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT, "sort kind %d is not voxel keys (0) or cell keys (1)",
-                kind);
+  if (kind < 0 || kind >= SRCU_SORT_KINDS)
+    return fail(ctx, SRCU_ERR_INVALID_ARGUMENT,
+                "sort kind %d is not voxel keys (0), cell keys (1), batch voxel keys (2) or "
+                "batch cell keys (3)", kind);
   if (count == 0) {
     builtin_sort_tuning(ctx, kind);
     return SRCU_OK;
@@ -1133,8 +1159,7 @@ srcu_status srcu_set_sort_tuning(srcu_ctx *ctx, int32_t kind, const uint64_t *ma
 
 srcu_status srcu_get_sort_tuning(srcu_ctx *ctx, int32_t kind, uint64_t *max_points,
                                  int32_t *config, uint32_t *count) {
-  if (!ctx || !count || (kind != SRCU_SORT_VOXEL_KEYS && kind != SRCU_SORT_CELL_KEYS))
-    return SRCU_ERR_INVALID_ARGUMENT;
+  if (!ctx || !count || kind < 0 || kind >= SRCU_SORT_KINDS) return SRCU_ERR_INVALID_ARGUMENT;
   const uint32_t cap = *count;
   *count = ctx->tune_count[kind];
   for (uint32_t k = 0; k < ctx->tune_count[kind] && k < cap; ++k) {

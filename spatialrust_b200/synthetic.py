@@ -160,21 +160,27 @@ def shapes_scene(n: int = 5_000_000, seed: int = 2, noise: float = 0.005,
 
 
 def batched_uneven(count: int = 256, lo: int = 10_000, hi: int = 1_000_000, seed: int = 3,
-                   max_offset: float = 1e6, scale: float = 1.0):
+                   max_offset: float = 1e6, scale: float = 1.0, max_points: int | None = None):
     """Many uneven clouds: sizes log-uniform in [lo, hi], each the scan mixture with
     its own seed and a random FP64 origin offset up to max_offset m; per-cloud leaf
-    in {0.05, 0.1, 0.2} m and radius 5 x leaf.  `scale` shrinks every size (tests)."""
+    in {0.05, 0.1, 0.2} m and radius 5 x leaf.  `scale` shrinks every size (tests).
+    With max_points, generation stops once the clouds made (two at least) hold
+    max_points or more; they are the first clouds of the full batch."""
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(np.int64)
     sizes = np.maximum((sizes * scale).astype(np.int64), 16)
     leaves = rng.choice(np.array([0.05, 0.1, 0.2], np.float32), size=count)
-    clouds = []
+    clouds, total = [], 0
     for i in range(count):
         off = rng.uniform(0.0, max_offset, 3)
         off[2] = rng.uniform(0.0, 100.0)
         c = georef_scan(int(sizes[i]), seed=seed * 100_003 + i, offset=off)
         clouds.append(c)
-    return clouds, leaves, (leaves * np.float32(5.0)).astype(np.float32)
+        total += c.n
+        if max_points is not None and total >= max_points and len(clouds) >= 2:
+            break
+    k = len(clouds)
+    return clouds, leaves[:k], (leaves[:k] * np.float32(5.0)).astype(np.float32)
 
 
 def lidar_scene(seed: int = 4, n_boxes: int = 100, extent: float = 120.0):

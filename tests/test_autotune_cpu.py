@@ -62,16 +62,39 @@ def test_header_is_parseable():
 def test_library_shapes():
     cfgs = _native.sort_configs()
     assert len(cfgs) >= 2 and cfgs[0]["items_per_thread"] == 16
-    assert all(c["digit_bits"] == 8 and c["threads_per_block"] in (256, 512) for c in cfgs)
+    assert all(c["threads_per_block"] in (256, 512) for c in cfgs)
     assert {c["threads_per_block"] for c in cfgs} == {256, 512}  # block size is a tuned dimension
-    assert len({(c["items_per_thread"], c["blocks_per_sm"], c["threads_per_block"])
+    assert {c["digit_bits"] for c in cfgs} == {8, 9}  # and so is digit width
+    # a thread per digit bin of the widest digit
+    assert all(c["threads_per_block"] >= 1 << c["digit_bits"] for c in cfgs)
+    assert len({(c["items_per_thread"], c["blocks_per_sm"], c["threads_per_block"], c["digit_bits"])
                 for c in cfgs}) == len(cfgs)
+
+
+def test_batch_kinds_sample_their_own_runs():
+    def run(w, p, c, vms, cms):
+        return dict(workload=w, points=p, voxels=p // 2, config=c, voxel_sort_ms=vms, cell_sort_ms=cms)
+    res = dict(configs=[{}, {}], runs=[run("scan", 100_000, 0, 1.0, 0.5), run("scan", 100_000, 1, 2.0, 0.6),
+                                       run("batch", 100_000, 0, 3.0, 0.9), run("batch", 100_000, 1, 2.0, 0.7)])
+    assert autotune.samples(res, "voxel") == [(100_000, [1.0, 2.0])]
+    assert autotune.samples(res, "batch_voxel") == [(100_000, [3.0, 2.0])]
+    assert autotune.samples(res, "batch_cell") == [(100_000, [0.9, 0.7])]
+    assert autotune.choose(res, "voxel") == [(BIG, 0)] and autotune.choose(res, "batch_voxel") == [(BIG, 1)]
+    # runs from before the batch workload existed count as scan runs
+    old = dict(configs=[{}], runs=[dict(points=5, voxels=2, config=0, voxel_sort_ms=1.0, cell_sort_ms=1.0)])
+    assert autotune.samples(old, "voxel") == [(5, [1.0])] and autotune.samples(old, "batch_voxel") == []
+    # without batch tables the header repeats the scan tables for the batch kinds
+    text = autotune.header_text({"voxel": [(BIG, 3)], "cell": [(BIG, 2)]}, None)
+    assert "kBatchVoxelSortTuneConfig[] = {3};" in text and "kBatchCellSortTuneConfig[] = {2};" in text
+    text = autotune.header_text({"voxel": [(BIG, 3)], "cell": [(BIG, 2)], "batch_voxel": [(BIG, 6)],
+                                 "batch_cell": [(BIG, 7)]}, None)
+    assert "kBatchVoxelSortTuneConfig[] = {6};" in text and "kBatchCellSortTuneConfig[] = {7};" in text
 
 
 def test_committed_header_matches_library():
     import os
     h = open(os.path.join(os.path.dirname(autotune.__file__), "csrc", "sort_tuning.h")).read()
-    for name in ("Voxel", "Cell"):
+    for name in ("Voxel", "Cell", "BatchVoxel", "BatchCell"):
         n = int(re.search(rf"k{name}SortTuneCount = (\d+);", h).group(1))
         cfg = [int(v) for v in
                re.search(rf"k{name}SortTuneConfig\[\] = \{{([^}}]*)\}};", h).group(1).split(",")]
