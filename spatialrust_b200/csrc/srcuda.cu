@@ -336,8 +336,11 @@ srcu_status reserve(srcu_ctx *ctx, uint64_t n, uint32_t cols, bool host_input, b
   ST_TRY(ensure(ctx, ctx->keys[1], m * 8));
   ST_TRY(ensure(ctx, ctx->vals[0], m * 4));
   ST_TRY(ensure(ctx, ctx->vals[1], m * 4));
-  // look-back words for the smallest tile any sort launch shape uses
-  ST_TRY(ensure(ctx, ctx->lb_sort, size_t(ceil_div(m, SORT_MIN_TILE)) * RADIX_BINS * 8, true));
+  // Sort look-back words: a launch shape with tiles of T keys and B digit bins
+  // writes ceil(m / T) * B words, and B / T <= RADIX_BINS / SORT_MIN_TILE
+  // (lookback_fits), so this covers every shape up to one tile's rounding.
+  ST_TRY(ensure(ctx, ctx->lb_sort,
+                (size_t(ceil_div(m, SORT_MIN_TILE)) * RADIX_BINS + MAX_RADIX_BINS) * 8, true));
   ST_TRY(ensure(ctx, ctx->in_aos, m * 16));
   if (voxel) {
     ST_TRY(ensure(ctx, ctx->vaos, m * 16));
