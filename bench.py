@@ -89,6 +89,8 @@ def parse():
     ap.add_argument("--serving-seconds", type=float, default=2.0)
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end (host buffers) measurements (profiling runs)")
+    ap.add_argument("--e2e-inflight", type=int, default=E2E_INFLIGHT,
+                    help="steps in flight in the end-to-end measurement")
     ap.add_argument("--neighbor-walk", type=int, default=-1, choices=[-1, 0, 1, 2],
                     help="the normals kernel's neighbour walk (-1: the built-in choice)")
     return ap.parse_args()
@@ -484,9 +486,11 @@ def run_gpu(args):
         skipped = dict(value=None, unit=UNIT, skipped="--no-e2e")
         e2e = e2e_one_step = e2e_pageable = skipped
     else:
-        e2e = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream)
+        e2e = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream,
+                      inflight=args.e2e_inflight)
         e2e_one_step = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, inflight=1)
-        e2e_pageable = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=False)
+        e2e_pageable = run_e2e(ctxs, leaf_streams, cloud, args, torch, dev, stream, pinned=False,
+                               inflight=args.e2e_inflight)
 
     peaks = {}
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
