@@ -180,7 +180,7 @@ __device__ inline Eig3 smallest_eigenpair_t(T a00, T a11, T a22, T a01, T a02, T
   const T av2 = a02 * v0 + a12 * v1 + a22 * v2;
   const T vv = v0 * v0 + v1 * v1 + v2 * v2;
   const T rq = (v0 * av0 + v1 * av1 + v2 * av2) / vv;
-  if (rq >= T(0) && rq <= r.l1) {
+  if (rq <= r.l1) {  // false for NaN
     r.l1 = (a00 + a11 + a22) - rq - r.l2;
     r.l0 = rq;
   }
