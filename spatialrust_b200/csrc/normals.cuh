@@ -456,6 +456,7 @@ __global__ void __launch_bounds__(256, 3) k_ranges(Control *ctl, const uint64_t 
 constexpr int NM_THREADS = 256;
 constexpr int NM_FLUSH = 32;  // f32 partial moments are folded into FP64 every NM_FLUSH candidates
 constexpr double NM_REFINE_GAP = 0.05;  // (l1 - l0) / trace below this -> FP64 moments
+constexpr double NM_REFINE_MEAN = 0.75;  // |E[d]|^2 / E|d|^2 above this -> FP64 moments
 constexpr uint32_t NM_STAGE = 256;  // candidate records staged per warp (4 KB), staged gather
 
 // Staged gather: one mbarrier per warp, completed by the bulk copies' bytes.
@@ -898,14 +899,26 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
     const bool valid = prm.include_self ? (n_eff >= 3) : (cnt >= prm.min_neighbors && cnt > 0);
     float ox, oy, oz, oc;
     if (valid) {
-      Eig3 e = eig_from_moments_f32(S, n_eff);
-      // The f32 moments carry ~1e-7 r^2 of rounding and the FP32 solve ~6e-8
-      // of the trace; when the gap to the second eigenvalue is under
-      // NM_REFINE_GAP of the trace that rounding can tilt the normal by more
-      // than 1e-5 rad, so this point's moments are recomputed with FP64
-      // products (same neighbour set) and solved in FP64.
-      const double trace = e.l0 + e.l1 + e.l2;
-      if (!(e.l1 - e.l0 >= NM_REFINE_GAP * trace)) {
+      // The f32 moments carry ~1e-7 of E|d|^2 in rounding (d = p - q, about
+      // the query), and the covariance E[d d^T] - E[d] E[d]^T inherits it
+      // whole: where the neighbours' mean lies far from the query against
+      // their spread (|E[d]|^2 > NM_REFINE_MEAN E|d|^2, so the trace is under
+      // a quarter of E|d|^2) that is too much of the trace for the curvature,
+      // and the moments are recomputed with FP64 products.  The FP32 solve
+      // carries ~6e-8 of the trace; where the gap to the second eigenvalue is
+      // under NM_REFINE_GAP of the trace the normal can tilt by more than
+      // 1e-5 rad, and the same FP64 path is taken.  Both refinements use the
+      // same neighbour set and solve in FP64.
+      const double inv_n = __drcp_rn(double(n_eff));
+      const double e2 = (S[3] + S[4] + S[5]) * inv_n;
+      const double m2 = (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) * (inv_n * inv_n);
+      bool refine = !(m2 <= NM_REFINE_MEAN * e2);
+      Eig3 e;
+      if (!refine) {
+        e = eig_from_moments_f32(S, n_eff);
+        refine = !(e.l1 - e.l0 >= NM_REFINE_GAP * (e.l0 + e.l1 + e.l2));
+      }
+      if (refine) {
         moments_fp64(pts, rg, qp, r2, S);
         e = eig_from_moments(S, n_eff);
         ++n_fp64;
