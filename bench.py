@@ -47,7 +47,9 @@ PROFILE_PASSES = 5  # untimed per-group profile passes (median)
 # DRAM bytes (read + write) per launch of the dominant kernel group on this
 # workload, mean over the leaf-0.1 and leaf-0.5 chains, from one ncu capture
 # (profiles/k_normals_georef2M_leaf0.1.md); ncu cannot run inside the bench.
-MEASURED_TRAFFIC = {"normals": (97.0e6 + 42.4e6) / 2}
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of the normals launches of one step
+# (leaf 0.1, leaf 0.5), profiles/dram_per_kernel_georef2M.md
+MEASURED_TRAFFIC = {"normals": (93.1e6 + 42.7e6) / 2}
 
 
 def parse():
@@ -505,10 +507,10 @@ def run_gpu(args):
     roofline = dict(bound="hbm", kernel=dominant, achieved=achieved, peak=hbm, unit="GB/s",
                     frac=achieved / hbm, traffic=MEASURED_TRAFFIC.get(dominant),
                     traffic_source=("ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
-                                    "profiles/k_normals_georef2M_leaf0.1.md")
+                                    "profiles/dram_per_kernel_georef2M.md")
                     if dominant in MEASURED_TRAFFIC else None,
-                    note=("the normals kernel is bound by FP32 issue and L1 latency on its "
-                          "candidate walk (ncu: 64% issue active, 3% of DRAM peak), not by HBM")
+                    note=("the normals kernel is bound by issue and L1 latency on its "
+                          "candidate walk (ncu: 63% issue active, 3% of DRAM peak), not by HBM")
                     if dominant == "normals" else None,
                     peak_source="MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
                     else "fallback 6650 GB/s",
