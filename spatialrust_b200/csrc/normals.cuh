@@ -904,22 +904,19 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
       // whole: where the neighbours' mean lies far from the query against
       // their spread (|E[d]|^2 > NM_REFINE_MEAN E|d|^2, so the trace is under
       // a quarter of E|d|^2) that is too much of the trace for the curvature,
-      // and the moments are recomputed with FP64 products.  The FP32 solve
-      // carries ~6e-8 of the trace; where the gap to the second eigenvalue is
-      // under NM_REFINE_GAP of the trace the normal can tilt by more than
-      // 1e-5 rad, and the same FP64 path is taken.  Both refinements use the
-      // same neighbour set and solve in FP64.
+      // so the moments are recomputed with FP64 products (same neighbour set)
+      // before the FP32 solve.  That solve carries ~6e-8 of the trace; where
+      // the gap to the second eigenvalue is under NM_REFINE_GAP of the trace
+      // the normal can tilt by more than 1e-5 rad, and the point is solved
+      // again in FP64 from FP64 moments.
       const double inv_n = __drcp_rn(double(n_eff));
       const double e2 = (S[3] + S[4] + S[5]) * inv_n;
       const double m2 = (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) * (inv_n * inv_n);
-      bool refine = !(m2 <= NM_REFINE_MEAN * e2);
-      Eig3 e;
-      if (!refine) {
-        e = eig_from_moments_f32(S, n_eff);
-        refine = !(e.l1 - e.l0 >= NM_REFINE_GAP * (e.l0 + e.l1 + e.l2));
-      }
-      if (refine) {
-        moments_fp64(pts, rg, qp, r2, S);
+      const bool exact_moments = !(m2 <= NM_REFINE_MEAN * e2);
+      if (exact_moments) moments_fp64(pts, rg, qp, r2, S);
+      Eig3 e = eig_from_moments_f32(S, n_eff);
+      if (!(e.l1 - e.l0 >= NM_REFINE_GAP * (e.l0 + e.l1 + e.l2))) {
+        if (!exact_moments) moments_fp64(pts, rg, qp, r2, S);
         e = eig_from_moments(S, n_eff);
         ++n_fp64;
       }
