@@ -166,24 +166,9 @@ __device__ inline Eig3 smallest_eigenpair_t(T a00, T a11, T a22, T a01, T a02, T
     return r;
   }
   const T inv = Tr::rsqrt_(bn);
-  const T v0 = c[best][0] * inv, v1 = c[best][1] * inv, v2 = c[best][2] * inv;
-  r.v[0] = v0;
-  r.v[1] = v1;
-  r.v[2] = v2;
-  // l0 again, as the Rayleigh quotient v^T A v / v^T v, with l1 keeping the
-  // trace: the trigonometric l0 carries the acos's rounding, which grows where
-  // acos is steep (two eigenvalues close), while the quotient's error is a
-  // few ulps of |A| plus the square of the eigenvector's.  Curvature
-  // l0 / (l0 + l1 + l2) then holds ~1e-7 of the trace in either precision.
-  const T av0 = a00 * v0 + a01 * v1 + a02 * v2;
-  const T av1 = a01 * v0 + a11 * v1 + a12 * v2;
-  const T av2 = a02 * v0 + a12 * v1 + a22 * v2;
-  const T vv = v0 * v0 + v1 * v1 + v2 * v2;
-  const T rq = (v0 * av0 + v1 * av1 + v2 * av2) / vv;
-  if (rq <= r.l1) {  // false for NaN
-    r.l1 = (a00 + a11 + a22) - rq - r.l2;
-    r.l0 = rq;
-  }
+  r.v[0] = c[best][0] * inv;
+  r.v[1] = c[best][1] * inv;
+  r.v[2] = c[best][2] * inv;
   return r;
 }
 
