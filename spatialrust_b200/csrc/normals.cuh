@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(256, 3) k_ranges(Control *ctl, const uint64_t 
 constexpr int NM_THREADS = 256;
 constexpr int NM_FLUSH = 32;  // f32 partial moments are folded into FP64 every NM_FLUSH candidates
 constexpr double NM_REFINE_GAP = 0.05;  // (l1 - l0) / trace below this -> FP64 moments
-constexpr double NM_REFINE_MEAN = 0.75;  // |E[d]|^2 / E|d|^2 above this -> FP64 moments
+constexpr double NM_REFINE_MEAN = 0.875;  // |E[d]|^2 / E|d|^2 above this -> FP64 moments
 constexpr uint32_t NM_STAGE = 256;  // candidate records staged per warp (4 KB), staged gather
 
 // Staged gather: one mbarrier per warp, completed by the bulk copies' bytes.
@@ -903,22 +903,27 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
       // the query), and the covariance E[d d^T] - E[d] E[d]^T inherits it
       // whole: where the neighbours' mean lies far from the query against
       // their spread (|E[d]|^2 > NM_REFINE_MEAN E|d|^2, so the trace is under
-      // a quarter of E|d|^2) that is too much of the trace for the curvature,
-      // so the moments are recomputed with FP64 products (same neighbour set)
-      // before the FP32 solve.  That solve carries ~6e-8 of the trace; where
-      // the gap to the second eigenvalue is under NM_REFINE_GAP of the trace
-      // the normal can tilt by more than 1e-5 rad, and the point is solved
-      // again in FP64 from FP64 moments.
+      // an eighth of E|d|^2) that is too much of the trace for the curvature
+      // and, over a small gap, for the normal, so the moments are recomputed
+      // with FP64 products (same neighbour set) and solved again in FP32.
+      // The FP32 solve carries ~6e-8 of the trace; where the gap to the
+      // second eigenvalue is under NM_REFINE_GAP of the trace the normal can
+      // tilt by more than 1e-5 rad, and the point is solved in FP64 from FP64
+      // moments.  One call site for the FP64 walk keeps the common path lean.
       const double inv_n = __drcp_rn(double(n_eff));
       const double e2 = (S[3] + S[4] + S[5]) * inv_n;
       const double m2 = (S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) * (inv_n * inv_n);
       const bool exact_moments = !(m2 <= NM_REFINE_MEAN * e2);
-      if (exact_moments) moments_fp64(pts, rg, qp, r2, S);
       Eig3 e = eig_from_moments_f32(S, n_eff);
-      if (!(e.l1 - e.l0 >= NM_REFINE_GAP * (e.l0 + e.l1 + e.l2))) {
-        if (!exact_moments) moments_fp64(pts, rg, qp, r2, S);
-        e = eig_from_moments(S, n_eff);
-        ++n_fp64;
+      const bool small_gap = !(e.l1 - e.l0 >= NM_REFINE_GAP * (e.l0 + e.l1 + e.l2));
+      if (exact_moments || small_gap) {
+        moments_fp64(pts, rg, qp, r2, S);
+        if (small_gap) {
+          e = eig_from_moments(S, n_eff);
+          ++n_fp64;
+        } else {
+          e = eig_from_moments_f32(S, n_eff);
+        }
       }
       // Orientation and normalisation in f32, as the reference computes them
       // (orient_normal_towards_viewpoint, normal.rs:408-421, with Vec3::dot
