@@ -325,6 +325,7 @@ def summary(line: dict) -> dict:
     out = dict(value=round(line["value"], 1), e2e=r1(line["e2e"]["value"]),
                e2e_one_step_in_flight=r1(line["e2e_one_step_in_flight"]["value"]),
                e2e_pageable=r1(line["e2e_pageable"]["value"]),
+               graph=r1(line["graph"]["value"]) if "graph" in line else None,
                roofline_frac=round(line["roofline"]["frac"], 4),
                roofline_voxel_frac=[round(x["frac"], 4) for x in line["roofline_voxel"]["leaves"]])
     b = line.get("batched")
@@ -482,6 +483,46 @@ def run_gpu(args):
     ms_per_step = max_ms / args.steps
     value = job_mpts(world, N_POINTS, ms_per_step)
 
+    # the same step replayed from CUDA graphs: each leaf chain captured once
+    # (srcu_chain_graph_create) and launched on its stream every step
+    graphs = [c.chain_graph(dcloud, [leaf], [RADIUS], None, 3, [VIEWPOINT], False)
+              for c, leaf in zip(ctxs, LEAVES)]
+
+    def graph_step():
+        if not args.serial_leaves:
+            fork.record(stream)
+            for s in leaf_streams:
+                s.wait_event(fork)
+        for g in graphs:
+            g.launch()
+        if not args.serial_leaves:
+            for s, e in zip(leaf_streams, joins):
+                e.record(s)
+                stream.wait_event(e)
+
+    for _ in range(max(args.warmup, 3)):
+        flush.zero_()
+        graph_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    gev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for s in range(args.steps):
+        flush.zero_()
+        gev[s][0].record(stream)
+        graph_step()
+        gev[s][1].record(stream)
+    torch.cuda.synchronize()
+    graph_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in gev), dev) / args.steps
+    for g in graphs:
+        g.close()
+    for c in ctxs:
+        c.frame_check()
+    graph = dict(value=job_mpts(world, N_POINTS, graph_ms), unit=UNIT, ms_per_step=graph_ms,
+                 api="srcu_chain_graph_create once per leaf context, srcu_graph_launch of both "
+                     "on the two leaf streams every step (same fork, join and L2 flush)")
+
     # end to end through the C ABI with pinned host buffers, then with plain
     # (pageable) numpy buffers as a Rust caller's Vecs are
     if args.no_e2e:
@@ -552,7 +593,7 @@ def run_gpu(args):
                      leaf_chains=("one stream, one after the other" if args.serial_leaves else
                                   "two streams (one context each), forked and joined every step")),
         e2e=e2e, e2e_one_step_in_flight=e2e_one_step, e2e_pageable=e2e_pageable,
-        roofline=roofline, roofline_voxel=roofline_voxel,
+        graph=graph, roofline=roofline, roofline_voxel=roofline_voxel,
         clocks=clock, gpu_launches=int(launches),
     )
     if not args.no_batched:
