@@ -131,7 +131,10 @@ struct CellKeySrc {
 };
 
 constexpr int CELL_THREADS = 256;
-constexpr int CELL_ITEMS = 8;
+// 1024-point tiles: at 417k points (C1's leaf-0.5 centroids) twice the tiles of
+// 2048-point ones spread the look-back-bound tiles over every SM (45 -> 27 us),
+// with no loss at 1.8M; 512-point tiles lose at 1.8M.
+constexpr int CELL_ITEMS = 4;
 constexpr int CELL_TILE = CELL_THREADS * CELL_ITEMS;
 
 struct CellSmem {
