@@ -79,7 +79,7 @@ struct BoundsAcc {
   }
 };
 
-constexpr uint32_t BND_CHUNK = 16;  // points per lane of a warp span in the multi-cloud case
+constexpr uint32_t BND_CHUNK = 32;  // points per lane of a warp span in the multi-cloud case
 
 // Interleaved input records (srcu_cloud.stride > 1) -> packed columns.
 struct Interleaved {
@@ -182,7 +182,25 @@ __global__ void __launch_bounds__(BND_THREADS) k_bounds(const float *x, const fl
     BoundsAcc acc;
     acc.reset();
     if (b0 == b1) {
-      for (uint64_t i = s0 + lane; i < s1; i += 32) {
+      uint64_t i = s0 + lane;
+      // four points per lane in flight: all loads first, then the stores
+      for (; i + 96 < s1; i += 128) {
+        float px[4], py[4], pz[4], pa[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint64_t k = i + 32u * q;
+          px[q] = x[k];
+          py[q] = y[k];
+          pz[q] = z[k];
+          pa[q] = a0 ? a0[k] : 0.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (aos) aos[i + 32u * q] = make_float4(px[q], py[q], pz[q], pa[q]);
+          acc.add(px[q], py[q], pz[q]);
+        }
+      }
+      for (; i < s1; i += 32) {
         const float xi = x[i], yi = y[i], zi = z[i];
         if (aos) aos[i] = make_float4(xi, yi, zi, a0 ? a0[i] : 0.0f);
         acc.add(xi, yi, zi);
