@@ -735,7 +735,7 @@ srcu_status enqueue_first_seen(srcu_ctx *ctx, const float **in, uint64_t n) {
 srcu_status enqueue_voxel(srcu_ctx *ctx, const float **in, uint32_t nc, uint64_t n,
                           const Batch &bt) {
   const uint32_t grid_b = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(n, BND_THREADS * 4),
-                                                                    uint32_t(ctx->num_sms) * 8));
+                                                                    uint32_t(ctx->num_sms) * 16));
   {
     Launch l(ctx, SRCU_K_BOUNDS);
     k_bounds<<<grid_b, BND_THREADS, 0, ctx->stream>>>(in[0], in[1], in[2], ctx->ctl, nullptr,
