@@ -311,6 +311,154 @@ __device__ __forceinline__ int64_t column_lookup(const uint64_t *table, const ui
   return -1;
 }
 
+// Key arithmetic of k_ranges in K (uint32_t where the chain's cell keys with
+// their cloud bits fit 31 bits, uint64_t otherwise): a shift or a mask as wide
+// as K is defined here, where C++ leaves it undefined.
+template <class K>
+__device__ __forceinline__ K shl_k(K v, uint32_t s) {
+  return s >= 8 * sizeof(K) ? K(0) : K(v << s);
+}
+template <class K>
+__device__ __forceinline__ K shr_k(K v, uint32_t s) {
+  return s >= 8 * sizeof(K) ? K(0) : K(v >> s);
+}
+template <class K>
+__device__ __forceinline__ K low_mask_k(uint32_t bits) {
+  return bits >= 8 * sizeof(K) ? ~K(0) : K((K(1) << bits) - K(1));
+}
+
+// The 9 column ranges of cell u (see k_ranges), with cell keys held in K.
+template <class K>
+__device__ __forceinline__ void ranges_of_cell(uint32_t u, uint32_t u_count, const uint64_t *cell_key,
+                                               const uint32_t *cell_start, const uint64_t *table,
+                                               uint32_t log2cap, uint32_t tmask, bool dense,
+                                               uint32_t epoch, uint32_t lb, const Batch &bt,
+                                               uint2 *ranges) {
+  const K none = ~K(0);  // no column: above every key (keys have at most 31 bits in uint32_t)
+  const K full = K(cell_key[u]);
+  const uint32_t b = (bt.clouds == 1 || lb >= 8 * sizeof(K)) ? 0u : uint32_t(shr_k<K>(full, lb));
+  const CellPlan &pl = bt.cplans[b < bt.clouds ? b : 0];
+  const int32_t dims0 = int32_t(pl.dims[0]), dims1 = int32_t(pl.dims[1]);
+  const uint32_t dims2 = pl.dims[2];
+  const uint32_t sx = pl.shift_x, sy = pl.shift_y;
+  const K local = full & low_mask_k<K>(lb);
+  const uint32_t cz = uint32_t(local & low_mask_k<K>(pl.bits[2]));
+  const uint32_t cy = uint32_t(shr_k<K>(local, sy) & low_mask_k<K>(pl.bits[1]));
+  const uint32_t cx = uint32_t(shr_k<K>(local, sx));
+  const K cmask = ~low_mask_k<K>(pl.bits[2]);
+  const K cloud_part = (bt.clouds == 1) ? K(0) : shl_k<K>(K(b), lb);
+  const K zlo = cz > 0 ? K(cz - 1) : K(0);
+  const K zhi = cz + 1 < dims2 ? K(cz + 1) : K(cz);
+  uint2 *out = ranges + size_t(u) * 9;
+  // centre column
+  {
+    uint32_t first = u, last = u;
+    if (cz > 0 && u > 0 && K(cell_key[u - 1]) == full - K(1)) first = u - 1;
+    if (cz + 1 < dims2 && u + 1 < u_count && K(cell_key[u + 1]) == full + K(1)) last = u + 1;
+    out[4] = make_uint2(cell_start[first], cell_start[last + 1]);
+  }
+  // round 1: column keys and first probes (a dense slot, or the first hash
+  // slot), all loads issued together
+  K ckey[8];
+  uint32_t slot[8];
+  uint64_t word[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int col = k < 4 ? k : k + 1;
+    const int32_t nx = int32_t(cx) + col / 3 - 1;
+    const int32_t ny = int32_t(cy) + col % 3 - 1;
+    const bool inside = nx >= 0 && ny >= 0 && nx < dims0 && ny < dims1;
+    ckey[k] = inside ? K(shl_k<K>(K(nx), sx) | shl_k<K>(K(ny), sy) | cloud_part) : none;
+    uint64_t idx = cell_hash(uint64_t(ckey[k]), log2cap);
+    if (dense) idx = inside ? dense_column(pl, uint64_t(nx), uint64_t(ny)) : 0;
+    slot[k] = uint32_t(idx);
+    word[k] = (inside && idx <= tmask) ? table[idx] : 0ull;
+  }
+  // first cell of each column (or -1), resolving hash probe chains
+  int32_t f[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    f[k] = -1;
+    if (dense) {
+      if (ckey[k] != none && uint32_t(word[k] >> 32) == epoch) f[k] = int32_t(uint32_t(word[k]));
+    } else if (ckey[k] != none) {
+      uint32_t h = slot[k];
+      uint64_t w = word[k];
+      for (uint32_t probe = 0; probe <= tmask; ++probe) {
+        if (uint32_t(w >> 32) != epoch) break;
+        const uint32_t c = uint32_t(w);
+        if ((K(cell_key[c]) & cmask) == ckey[k]) {
+          f[k] = int32_t(c);
+          break;
+        }
+        h = (h + 1) & tmask;
+        w = table[h];
+      }
+    }
+  }
+  // rounds 2 and 3 for four columns at a time (half the keys live at once)
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    // round 2: the keys of each column's first three cells
+    K kk[4][3];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int k = 4 * g + j;
+        const uint32_t c = uint32_t(f[k]) + q;
+        kk[j][q] = (f[k] >= 0 && c < u_count) ? K(cell_key[c]) : none;
+      }
+    // the cells [c, last] of each window
+    uint32_t c0[4], c1[4];
+    bool has[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = 4 * g + j;
+      has[j] = false;
+      c0[j] = c1[j] = 0;
+      if (f[k] < 0) continue;
+      const K lo_key = ckey[k] | zlo, hi_key = ckey[k] | zhi;
+      uint32_t c = uint32_t(f[k]);
+      K key0 = kk[j][0], key1 = kk[j][1], key2 = kk[j][2];
+      if (key0 < lo_key) {  // the column reaches below the window: gallop to it
+        uint32_t step = 1;
+        while (c + step < u_count && K(cell_key[c + step]) < lo_key) {
+          c += step;
+          step <<= 1;
+        }
+        uint32_t hi = c + step < u_count ? c + step : u_count;
+        while (hi - c > 1) {
+          const uint32_t mid = c + ((hi - c) >> 1);
+          if (K(cell_key[mid]) < lo_key) c = mid;
+          else hi = mid;
+        }
+        c = hi;
+        key0 = c < u_count ? K(cell_key[c]) : none;
+        key1 = c + 1 < u_count ? K(cell_key[c + 1]) : none;
+        key2 = c + 2 < u_count ? K(cell_key[c + 2]) : none;
+      }
+      if (c < u_count && key0 <= hi_key) {
+        uint32_t last = c;
+        if (c + 1 < u_count && key1 <= hi_key) {
+          last = c + 1;
+          if (c + 2 < u_count && key2 <= hi_key) last = c + 2;
+        }
+        has[j] = true;
+        c0[j] = c;
+        c1[j] = last + 1;
+      }
+    }
+    // round 3: the cell starts that bound each range
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = 4 * g + j;
+      const int col = k < 4 ? k : k + 1;
+      out[col] = has[j] ? make_uint2(cell_start[c0[j]], cell_start[c1[j]]) : make_uint2(0, 0);
+    }
+  }
+}
+
 // For every occupied cell and each of the 3x3 neighbouring columns, the range
 // of cell-sorted points in cells (cx+dx, cy+dy, cz-1 .. cz+1).  Those (at
 // most three) cells are consecutive in key order, so each column is one
@@ -323,136 +471,28 @@ __device__ __forceinline__ int64_t column_lookup(const uint64_t *table, const ui
 // cell lies below the window (a column with cells under cz - 1) is searched
 // by galloping from its first cell instead; a window holds at most three
 // cells, so three keys from the first cell in the window decide its end.
+// The kernel is bound by its integer arithmetic, so keys that fit 31 bits
+// with their cloud bits (one scan at a 0.5 m radius: ~24 bits) are handled in
+// 32-bit arithmetic, the rest in 64-bit.
 __global__ void __launch_bounds__(256, 3) k_ranges(Control *ctl, const uint64_t *cell_key,
                                                 const uint32_t *cell_start, const uint64_t *table,
                                                 uint32_t log2cap, uint2 *ranges, Batch bt) {
   if (ld_relaxed_u32(&ctl->status)) return;
-  const uint64_t u_count = ctl->n_cells;
+  const uint32_t u_count = uint32_t(ctl->n_cells);  // < 2^30 (the look-back counters)
   const uint32_t epoch = ctl->epoch + EP_CELLS;
   const uint32_t lb = ctl->ckey_bits;
-  const uint64_t local_mask = lb >= 64 ? ~0ull : ((1ull << lb) - 1);
   const uint32_t tmask = (1u << log2cap) - 1u;
   const bool dense = ctl->dense_cols != 0;
-  for (uint64_t u = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; u < u_count;
-       u += uint64_t(gridDim.x) * blockDim.x) {
-    const uint64_t full = cell_key[u];
-    const uint32_t b = cloud_of_key(full, bt, lb);
-    const CellPlan &pl = bt.cplans[b < bt.clouds ? b : 0];
-    const uint32_t dims0 = pl.dims[0], dims1 = pl.dims[1], dims2 = pl.dims[2];
-    const uint32_t sx = pl.shift_x, sy = pl.shift_y;
-    uint32_t cx, cy, cz;
-    cell_unpack(pl, full & local_mask, cx, cy, cz);
-    const uint64_t cmask = ~((1ull << pl.bits[2]) - 1ull);
-    const uint64_t zlo = cz > 0 ? cz - 1 : 0;
-    const uint64_t zhi = cz + 1 < dims2 ? cz + 1 : cz;
-    uint2 *out = ranges + size_t(u) * 9;
-    // centre column
-    {
-      uint64_t first = u, last = u;
-      if (cz > 0 && u > 0 && cell_key[u - 1] == full - 1) first = u - 1;
-      if (cz + 1 < dims2 && u + 1 < u_count && cell_key[u + 1] == full + 1) last = u + 1;
-      out[4] = make_uint2(cell_start[first], cell_start[last + 1]);
-    }
-    // round 1: column keys and first probes (a dense slot, or the first hash
-    // slot), all loads issued together
-    uint64_t ckey[8];
-    uint32_t slot[8];
-    uint64_t word[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const int col = k < 4 ? k : k + 1;
-      const int64_t nx = int64_t(cx) + col / 3 - 1;
-      const int64_t ny = int64_t(cy) + col % 3 - 1;
-      const bool inside = nx >= 0 && ny >= 0 && nx < dims0 && ny < dims1;
-      ckey[k] = inside ? with_cloud((uint64_t(nx) << sx) | (uint64_t(ny) << sy), b, lb) : ~0ull;
-      uint64_t idx = cell_hash(ckey[k], log2cap);
-      if (dense) idx = inside ? dense_column(pl, uint64_t(nx), uint64_t(ny)) : 0;
-      slot[k] = uint32_t(idx);
-      word[k] = (inside && idx <= tmask) ? table[idx] : 0ull;
-    }
-    // first cell of each column (or -1), resolving hash probe chains
-    int64_t f[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      f[k] = -1;
-      if (dense) {
-        if (ckey[k] != ~0ull && uint32_t(word[k] >> 32) == epoch) f[k] = uint32_t(word[k]);
-      } else if (ckey[k] != ~0ull) {
-        uint32_t h = slot[k];
-        uint64_t w = word[k];
-        for (uint32_t probe = 0; probe <= tmask; ++probe) {
-          if (uint32_t(w >> 32) != epoch) break;
-          const uint32_t c = uint32_t(w);
-          if ((cell_key[c] & cmask) == ckey[k]) {
-            f[k] = c;
-            break;
-          }
-          h = (h + 1) & tmask;
-          w = table[h];
-        }
-      }
-    }
-    // rounds 2 and 3 for four columns at a time (half the keys live at once)
-#pragma unroll
-    for (int g = 0; g < 2; ++g) {
-      // round 2: the keys of each column's first three cells
-      uint64_t kk[4][3];
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          const int k = 4 * g + j;
-          const uint64_t c = uint64_t(f[k]) + q;
-          kk[j][q] = (f[k] >= 0 && c < u_count) ? cell_key[c] : ~0ull;
-        }
-      // the cells [c, last] of each window
-      uint64_t c0[4], c1[4];
-      bool has[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int k = 4 * g + j;
-        has[j] = false;
-        c0[j] = c1[j] = 0;
-        if (f[k] < 0) continue;
-        const uint64_t lo_key = ckey[k] | zlo, hi_key = ckey[k] | zhi;
-        uint64_t c = uint64_t(f[k]);
-        uint64_t key0 = kk[j][0], key1 = kk[j][1], key2 = kk[j][2];
-        if (key0 < lo_key) {  // the column reaches below the window: gallop to it
-          uint64_t step = 1;
-          while (c + step < u_count && cell_key[c + step] < lo_key) {
-            c += step;
-            step <<= 1;
-          }
-          uint64_t hi = c + step < u_count ? c + step : u_count;
-          while (hi - c > 1) {
-            const uint64_t mid = c + ((hi - c) >> 1);
-            if (cell_key[mid] < lo_key) c = mid;
-            else hi = mid;
-          }
-          c = hi;
-          key0 = c < u_count ? cell_key[c] : ~0ull;
-          key1 = c + 1 < u_count ? cell_key[c + 1] : ~0ull;
-          key2 = c + 2 < u_count ? cell_key[c + 2] : ~0ull;
-        }
-        if (c < u_count && key0 <= hi_key) {
-          uint64_t last = c;
-          if (c + 1 < u_count && key1 <= hi_key) {
-            last = c + 1;
-            if (c + 2 < u_count && key2 <= hi_key) last = c + 2;
-          }
-          has[j] = true;
-          c0[j] = c;
-          c1[j] = last + 1;
-        }
-      }
-      // round 3: the cell starts that bound each range
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int k = 4 * g + j;
-        const int col = k < 4 ? k : k + 1;
-        out[col] = has[j] ? make_uint2(cell_start[c0[j]], cell_start[c1[j]]) : make_uint2(0, 0);
-      }
-    }
+  const bool narrow = lb + ctl->cloud_bits <= 31;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  if (narrow) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < u_count; u += stride)
+      ranges_of_cell<uint32_t>(u, u_count, cell_key, cell_start, table, log2cap, tmask, dense,
+                               epoch, lb, bt, ranges);
+  } else {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < u_count; u += stride)
+      ranges_of_cell<uint64_t>(u, u_count, cell_key, cell_start, table, log2cap, tmask, dense,
+                               epoch, lb, bt, ranges);
   }
 }
 
