@@ -49,7 +49,7 @@ PROFILE_PASSES = 5  # untimed per-group profile passes (median)
 # (profiles/k_normals_georef2M_leaf0.1.md); ncu cannot run inside the bench.
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of the normals launches of one step
 # (leaf 0.1, leaf 0.5), profiles/dram_per_kernel_georef2M.md
-MEASURED_TRAFFIC = {"normals": (92.7e6 + 42.4e6) / 2}
+MEASURED_TRAFFIC = {"normals": (91.7e6 + 42.4e6) / 2}
 
 
 def parse():
