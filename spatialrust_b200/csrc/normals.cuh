@@ -357,7 +357,7 @@ __device__ __forceinline__ void ranges_of_cell(uint32_t u, uint32_t u_count, con
     if (cz + 1 < dims2 && u + 1 < u_count && K(cell_key[u + 1]) == full + K(1)) last = u + 1;
     out[4] = make_uint2(cell_start[first], cell_start[last + 1]);
   }
-  // round 1: column keys and first probes (a dense slot, or the first hash
+  // (1) column keys and first probes (a dense slot, or the first hash
   // slot), all loads issued together
   K ckey[8];
   uint32_t slot[8];
@@ -396,10 +396,10 @@ __device__ __forceinline__ void ranges_of_cell(uint32_t u, uint32_t u_count, con
       }
     }
   }
-  // rounds 2 and 3 for four columns at a time (half the keys live at once)
+  // steps (2) and (3) for four columns at a time (half the keys live at once)
 #pragma unroll
   for (int g = 0; g < 2; ++g) {
-    // round 2: the keys of each column's first three cells
+    // (2) the keys of each column's first three cells
     K kk[4][3];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
@@ -449,7 +449,7 @@ __device__ __forceinline__ void ranges_of_cell(uint32_t u, uint32_t u_count, con
         c1[j] = last + 1;
       }
     }
-    // round 3: the cell starts that bound each range
+    // (3) the cell starts that bound each range
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int k = 4 * g + j;
