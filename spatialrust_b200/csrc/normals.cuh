@@ -619,7 +619,7 @@ __device__ __noinline__ void moments_fp64(const float4 *pts, const uint2 *rg, fl
 }
 
 // Radius normals.  One warp per 32 consecutive cell-sorted points, one query
-// per lane.  Each lane walks the 9 column ranges of its own cell (the 27-cell
+// per lane; the persistent warps claim these batches from a counter.  Each lane walks the 9 column ranges of its own cell (the 27-cell
 // neighbourhood) and reads candidates through L1: lanes of the same cell read
 // the same record at the same step, so loads are broadcasts, and the
 // eigensolve runs on all 32 lanes.
@@ -670,7 +670,6 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
   const uint64_t u_count = ctl->n_cells;
   const uint32_t lb = ctl->ckey_bits;
   const uint32_t batches = (n + 31) / 32;
-  const uint32_t warps = gridDim.x * (NM_THREADS / 32);
   unsigned long long n_valid = 0, n_invalid = 0, n_shell = 0, n_fp64 = 0;
   float4 *sbuf = nullptr;  // this warp's staging buffer (Staged)
   uint64_t *sbar = nullptr;
@@ -686,7 +685,15 @@ __global__ void __launch_bounds__(NM_THREADS, 4) k_normals(Control *ctl, const f
     __syncwarp();
   }
 
-  for (uint32_t b = blockIdx.x * (NM_THREADS / 32) + (threadIdx.x >> 5); b < batches; b += warps) {
+  // Each warp claims its next batch of 32 queries from the chain's counter:
+  // batches differ in cost (dense and sparse parts of a cloud), so claiming
+  // keeps every warp busy to the end instead of a fixed share each.
+  auto claim = [&]() {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(&ctl->work[WK_NORMALS], 1u);
+    return __shfl_sync(FULL_MASK, c, 0);
+  };
+  for (uint32_t b = claim(); b < batches; b = claim()) {
     const uint32_t i = b * 32 + lane;
     const bool active = i < n;
     const uint32_t ii = active ? i : n - 1;
