@@ -173,6 +173,7 @@ constexpr int WK_VSEG = 8;
 constexpr int WK_CSORT = 16;  // 8 slots
 constexpr int WK_CELLS = 24;
 constexpr int WK_NORMALS = 25;
+constexpr int WK_RANGES = 26;
 constexpr int WK_ORDER = 32;  // 4 slots
 
 __device__ __forceinline__ int64_t rs_sat_i64(float t) {
