@@ -49,7 +49,7 @@ PROFILE_PASSES = 5  # untimed per-group profile passes (median)
 # (profiles/k_normals_georef2M_leaf0.1.md); ncu cannot run inside the bench.
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of the normals launches of one step
 # (leaf 0.1, leaf 0.5), profiles/dram_per_kernel_georef2M.md
-MEASURED_TRAFFIC = {"normals": (91.7e6 + 42.4e6) / 2}
+MEASURED_TRAFFIC = {"normals": (88.3e6 + 41.3e6) / 2}
 
 
 def parse():
@@ -551,7 +551,7 @@ def run_gpu(args):
                                     "profiles/dram_per_kernel_georef2M.md")
                     if dominant in MEASURED_TRAFFIC else None,
                     note=("the normals kernel is bound by issue and L1 latency on its "
-                          "candidate walk (ncu: 63% issue active, 3% of DRAM peak), not by HBM")
+                          "candidate walk (ncu: 65% issue active, 3% of DRAM peak), not by HBM")
                     if dominant == "normals" else None,
                     peak_source="MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
                     else "fallback 6650 GB/s",
