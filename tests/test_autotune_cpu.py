@@ -124,3 +124,20 @@ def test_choose_walk_among_three():
     assert autotune.choose_staging(res([(1.0, 1.1, 1.2), (2.0, 2.1, 2.3)])) == 0
     assert "kNeighborStaging = 2;" in autotune.header_text({"voxel": [(BIG, 0)], "cell": [(BIG, 0)]},
                                                              None, 2)
+
+
+def test_batch_workload_holds_exactly_n_points_in_two_clouds_or_more():
+    import numpy as np
+    from spatialrust_b200 import synthetic
+    for n in (20_000, 150_000):
+        x, y, z, offsets, leaves, radii = autotune.batch_clouds(n)
+        assert len(x) == len(y) == len(z) == n
+        assert offsets[0] == 0 and offsets[-1] == n and np.all(np.diff(offsets) > 0)
+        assert len(offsets) - 1 == len(leaves) == len(radii) >= 2
+        assert np.allclose(radii, 5.0 * leaves)
+    # the clouds are the first clouds of the full batch generator
+    few, lv, _ = synthetic.batched_uneven(256, seed=3, max_points=50_000)
+    assert len(few) >= 2 and sum(c.n for c in few) >= 50_000
+    assert sum(c.n for c in few[:-1]) < 50_000 or len(few) == 2
+    head, lv_all, _ = synthetic.batched_uneven(256, seed=3, scale=0.01)
+    assert np.array_equal(lv, lv_all[:len(few)])
